@@ -1,0 +1,257 @@
+"""Plain description of one Mjolnir system and seeded synthetic builders.
+
+A :class:`SystemDesc` carries exactly what the reference reads from its TOML
+input for the per-step hot path (``[[systems]]`` particles and attributes,
+``[[forcefields.global]]`` ExcludedVolume / DebyeHuckel / LennardJones with
+their ``ignore`` rules and ``spatial_partition``, ``[[forcefields.local]]``
+BondLength / BondAngle / DihedralAngle, and the BAOAB ``[simulator]``
+settings; input/read_system.hpp:93-290, input/read_global_potential.hpp,
+input/read_local_interaction.hpp, input/read_integrator.hpp:120-187).
+
+Units are kcal/mol and angstrom throughout (input/read_units.hpp:32-91).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional
+
+import numpy as np
+
+KB_KCAL = 1.38064852e-23 * (1.0 / 4.184 / 1000.0) * 6.022140857e23  # kB in kcal/mol/K
+
+
+@dataclasses.dataclass
+class PairTerm:
+    """One ``[[forcefields.global]]`` pair interaction."""
+    kind: str                          # "ExcludedVolume" | "DebyeHuckel" | "LennardJones"
+    idx: np.ndarray                    # participant particle indices (input order)
+    param0: np.ndarray                 # radius | charge | sigma
+    param1: Optional[np.ndarray] = None  # LJ epsilon
+    cutoff: float = 2.0                # relative cutoff (potential default)
+    margin: float = 0.5                # relative Verlet skin of the cell list
+    epsilon: float = 0.2               # ExcludedVolume epsilon
+
+
+@dataclasses.dataclass
+class SystemDesc:
+    pos: np.ndarray                    # (n, 3) float64
+    vel: np.ndarray                    # (n, 3) float64
+    mass: np.ndarray                   # (n,)
+    boundary: str = "Unlimited"        # "Unlimited" | "PeriodicCuboid"
+    lower: tuple = (0.0, 0.0, 0.0)
+    upper: tuple = (0.0, 0.0, 0.0)
+    temperature: float = 300.0
+    ionic_strength: float = 0.1
+    exv: Optional[PairTerm] = None
+    dh: Optional[PairTerm] = None
+    lj: Optional[PairTerm] = None
+    ignore_molecule: str = "Nothing"   # "Nothing" | "Self" | "Others"
+    ignore_bond_within: int = 0        # ignore.particles_within.bond
+    single_molecule: bool = False      # fluids: one "bond"-chain molecule
+    bonds: Optional[tuple] = None      # (idx (m,2) int64, k (m,), v0 (m,))
+    angles: Optional[tuple] = None     # (idx (m,3), k, v0)
+    dihedrals: Optional[tuple] = None  # (idx (m,4), k, n int32, v0)
+    integrator: str = "BAOAB"          # "BAOAB" | "VelocityVerlet"
+    dt: float = 0.01
+    gamma: Optional[np.ndarray] = None
+    seed: int = 12345
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+    @property
+    def periodic(self) -> bool:
+        return self.boundary == "PeriodicCuboid"
+
+    def pair_terms(self):
+        return [t for t in (self.exv, self.dh, self.lj) if t is not None]
+
+    def copy(self) -> "SystemDesc":
+        return dataclasses.replace(self, pos=self.pos.copy(), vel=self.vel.copy())
+
+
+# --------------------------------------------------------------------------
+# seeded synthetic systems (the named workloads are synthetic: no dataset)
+# --------------------------------------------------------------------------
+
+def maxwell_boltzmann(rng: np.random.Generator, mass: np.ndarray, kT: float) -> np.ndarray:
+    return rng.standard_normal((mass.shape[0], 3)) * np.sqrt(kT / mass)[:, None]
+
+
+def lj_fluid(n: int = 4096, density: float = 0.8, jitter: float = 0.05,
+             cutoff: float = 2.5, margin: float = 0.5, dt: float = 0.005,
+             gamma: float = 1.0, seed: int = 1) -> SystemDesc:
+    """Lennard-Jones fluid on a jittered simple-cubic lattice (sigma = eps = 1),
+    cubic periodic box L = (n/density)^(1/3), kT = 1 (temperature 1/kB)."""
+    rng = np.random.default_rng(seed)
+    m = round(n ** (1.0 / 3.0))
+    if m ** 3 != n:
+        raise ValueError("lj_fluid needs a cubic particle count")
+    L = (n / density) ** (1.0 / 3.0)
+    a = L / m
+    g = np.arange(m, dtype=np.float64)
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    pos = (np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1) + 0.5) * a
+    pos += rng.uniform(-jitter, jitter, size=pos.shape)
+    mass = np.ones(n)
+    T = 1.0 / KB_KCAL
+    vel = maxwell_boltzmann(rng, mass, 1.0)
+    idx = np.arange(n, dtype=np.int64)
+    return SystemDesc(pos=pos, vel=vel, mass=mass, boundary="PeriodicCuboid",
+                      lower=(0.0, 0.0, 0.0), upper=(L, L, L), temperature=T,
+                      ionic_strength=0.1,
+                      lj=PairTerm("LennardJones", idx, np.ones(n), np.ones(n),
+                                  cutoff=cutoff, margin=margin),
+                      single_molecule=True, dt=dt, gamma=np.full(n, gamma), seed=seed)
+
+
+def _random_walk_chains(rng, nchains, nbeads, bond, min_dist, radius, max_tries=200):
+    """Random-walk chains with `bond`-long steps from seed-drawn directions,
+    rejecting any bead closer than `min_dist` to an existing bead other than
+    the one it is bonded to, or outside the sphere of `radius` (grid hash of
+    `min_dist` cells)."""
+    cell = min_dist
+    grid = {}
+    out = np.empty((nchains * nbeads, 3))
+    k = 0
+
+    def ok(p, skip=-1):
+        if p @ p > radius * radius:
+            return False
+        c = np.floor(p / cell).astype(np.int64)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for q in grid.get((c[0] + dx, c[1] + dy, c[2] + dz), ()):
+                        if q == skip:
+                            continue
+                        d = p - out[q]
+                        if d @ d < min_dist * min_dist:
+                            return False
+        return True
+
+    def add(p):
+        nonlocal k
+        out[k] = p
+        c = np.floor(p / cell).astype(np.int64)
+        grid.setdefault((c[0], c[1], c[2]), []).append(k)
+        k += 1
+
+    for _c in range(nchains):
+        while True:
+            u = rng.uniform(-1, 1, 3) * radius
+            if ok(u):
+                add(u)
+                break
+        for _b in range(1, nbeads):
+            prev = out[k - 1]
+            for _t in range(max_tries):
+                d = rng.standard_normal(3)
+                p = prev + bond * d / np.linalg.norm(d)
+                if ok(p, k - 1):
+                    add(p)
+                    break
+            else:
+                raise RuntimeError("random walk got stuck; lower the density")
+    return out
+
+
+def polymer_melt(nchains: int = 50, nbeads: int = 200, radius: float = 300.0,
+                 charged_fraction: float = 0.2, temperature: float = 300.0,
+                 ionic_strength: float = 0.1, dt: float = 0.01, gamma: float = 1.0,
+                 margin: float = 0.5, seed: int = 2, mass: float = 1.0) -> SystemDesc:
+    """Coarse-grained polymer melt in unbounded space: harmonic bonds (k=100,
+    r0=3.8), harmonic angles (k=10, 110 deg), cosine dihedrals (k=0.5, n=3,
+    v0=0), ExcludedVolume (radius 2, eps 0.2, cutoff 2), DebyeHuckel on a
+    random `charged_fraction` of beads with charges +-1 and zero net charge."""
+    rng = np.random.default_rng(seed)
+    pos = _random_walk_chains(rng, nchains, nbeads, 3.8, 4.0, radius)
+    n = pos.shape[0]
+    m = np.full(n, mass)
+    vel = maxwell_boltzmann(rng, m, KB_KCAL * temperature)
+    base = (np.arange(nchains, dtype=np.int64) * nbeads)[:, None]
+    b = np.arange(nbeads - 1, dtype=np.int64)[None, :]
+    bonds = np.stack([(base + b).ravel(), (base + b + 1).ravel()], axis=1)
+    a = np.arange(nbeads - 2, dtype=np.int64)[None, :]
+    angles = np.stack([(base + a).ravel(), (base + a + 1).ravel(), (base + a + 2).ravel()], axis=1)
+    d = np.arange(nbeads - 3, dtype=np.int64)[None, :]
+    dihd = np.stack([(base + d).ravel(), (base + d + 1).ravel(),
+                     (base + d + 2).ravel(), (base + d + 3).ravel()], axis=1)
+    nch = int(round(charged_fraction * n)) // 2 * 2
+    charged = np.sort(rng.choice(n, size=nch, replace=False)).astype(np.int64)
+    q = np.ones(nch)
+    q[rng.permutation(nch)[: nch // 2]] = -1.0
+    all_idx = np.arange(n, dtype=np.int64)
+    return SystemDesc(
+        pos=pos, vel=vel, mass=m, boundary="Unlimited", temperature=temperature,
+        ionic_strength=ionic_strength,
+        exv=PairTerm("ExcludedVolume", all_idx, np.full(n, 2.0), cutoff=2.0,
+                     margin=margin, epsilon=0.2),
+        dh=PairTerm("DebyeHuckel", charged, q, cutoff=5.5, margin=margin),
+        ignore_molecule="Nothing", ignore_bond_within=3,
+        bonds=(bonds, np.full(len(bonds), 100.0), np.full(len(bonds), 3.8)),
+        angles=(angles, np.full(len(angles), 10.0), np.full(len(angles), math.radians(110.0))),
+        dihedrals=(dihd, np.full(len(dihd), 0.5), np.full(len(dihd), 3, dtype=np.int32),
+                   np.zeros(len(dihd))),
+        dt=dt, gamma=np.full(n, gamma), seed=seed)
+
+
+def bead_fluid(n: int = 1 << 20, density: float = 0.003, charged_fraction: float = 0.3,
+               temperature: float = 300.0, ionic_strength: float = 0.15,
+               dt: float = 0.3, gamma: float = 1.0, margin: float = 0.5,
+               min_dist: float = 4.0, mass: float = 100.0, seed: int = 3) -> SystemDesc:
+    """Periodic EXV + Debye-Hueckel bead fluid: cubic box at number density
+    `density`, uniform positions with overlaps below `min_dist` redrawn, charges
+    +-1 on `charged_fraction` of the beads with zero net charge."""
+    rng = np.random.default_rng(seed)
+    L = (n / density) ** (1.0 / 3.0)
+    pos = rng.uniform(0.0, L, size=(n, 3))
+    # redraw overlapping beads until none is closer than min_dist (grid check)
+    for _ in range(64):
+        bad = _overlaps_periodic(pos, L, min_dist)
+        if bad.size == 0:
+            break
+        pos[bad] = rng.uniform(0.0, L, size=(bad.size, 3))
+    m = np.full(n, mass)
+    vel = maxwell_boltzmann(rng, m, KB_KCAL * temperature)
+    nch = int(round(charged_fraction * n)) // 2 * 2
+    charged = np.sort(rng.choice(n, size=nch, replace=False)).astype(np.int64)
+    q = np.ones(nch)
+    q[rng.permutation(nch)[: nch // 2]] = -1.0
+    all_idx = np.arange(n, dtype=np.int64)
+    return SystemDesc(
+        pos=pos, vel=vel, mass=m, boundary="PeriodicCuboid", lower=(0.0, 0.0, 0.0),
+        upper=(L, L, L), temperature=temperature, ionic_strength=ionic_strength,
+        exv=PairTerm("ExcludedVolume", all_idx, np.full(n, 2.0), cutoff=2.0,
+                     margin=margin, epsilon=0.2),
+        dh=PairTerm("DebyeHuckel", charged, q, cutoff=5.5, margin=margin),
+        single_molecule=True, dt=dt, gamma=np.full(n, gamma), seed=seed)
+
+
+def _overlaps_periodic(pos: np.ndarray, L: float, dmin: float) -> np.ndarray:
+    """Indices of the higher-indexed bead of every pair closer than dmin."""
+    nc = max(1, int(L // dmin))
+    w = L / nc
+    c = np.floor(pos / w).astype(np.int64) % nc
+    key = (c[:, 0] * nc + c[:, 1]) * nc + c[:, 2]
+    order = np.argsort(key, kind="stable")
+    skey = key[order]
+    starts = np.searchsorted(skey, np.arange(nc ** 3))
+    ends = np.searchsorted(skey, np.arange(nc ** 3), side="right")
+    bad = set()
+    for dx in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dz in (-1, 0, 1):
+                nb = ((((c[:, 0] + dx) % nc) * nc + (c[:, 1] + dy) % nc) * nc + (c[:, 2] + dz) % nc)
+                cnt = ends[nb] - starts[nb]
+                mx = cnt.max() if cnt.size else 0
+                for r in range(mx):
+                    sel = np.nonzero(cnt > r)[0]
+                    j = order[starts[nb[sel]] + r]
+                    d = pos[j] - pos[sel]
+                    d -= L * np.round(d / L)
+                    close = (np.einsum("ij,ij->i", d, d) < dmin * dmin) & (j > sel)
+                    bad.update(j[close].tolist())
+    return np.array(sorted(bad), dtype=np.int64)
