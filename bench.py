@@ -1,0 +1,383 @@
+"""Benchmark of the B200 Mjolnir hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload (the batching configuration the headline metric is quoted on): 256
+independent coarse-grained polymer melts, sizes log-uniform in [500, 20000]
+beads (chains of ~200 beads, 10,000 beads per 300 A sphere density), per-system
+temperature U[280, 360] K and ionic strength U[0.05, 0.3] M; harmonic bonds and
+angles, cosine dihedrals, ExcludedVolume and DebyeHuckel with cell lists
+(margin 0.5), BAOAB at dt = 0.01.  All systems are packed into one arena and
+advanced by the same CUDA-graph step.  Synthetic, seeded inputs: there is no
+dataset.
+
+One bench step = CHUNK (100) MD steps of every system.  `value` is aggregate
+particle-steps/s with the state resident in HBM, timed with CUDA events on the
+library's stream; `e2e` is the same metric through the public C ABI with the
+positions and velocities uploaded from pinned host memory before and
+downloaded after every bench step.  Under torchrun every rank runs its own
+replica of the batch (replicas only: no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CHUNK = 100
+NSYS = 256
+SEED = 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nsys", type=int, default=NSYS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(x, pg):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_batch(nsys):
+    from mjolnir_b200 import systems as S
+    return S.polymer_batch(nsys=nsys, seed=SEED)
+
+
+# ---------------------------------------------------------------- reference
+def cpu_reference_rate(descs, budget_s=15.0, threads=None):
+    """The reference's own OpenMP path (oracle/_ref, OpenMPSimulatorTraits)
+    stepping the batch's systems one after another, as the reference would
+    run 256 separate simulations; returns (particle-steps/s, sample text,
+    threads).  Only the integrator steps are timed."""
+    import oracle
+    if not oracle.reference_available():
+        return None
+    sims, total_n, t_run, steps_done = [], 0, 0.0, 0
+    for d in descs:
+        r = oracle.Reference(d, parallel=True)
+        r.initialize()
+        sims.append(r)
+    nthreads = oracle.Reference.max_threads()
+    rounds = 0
+    while t_run < budget_s:
+        for r, d in zip(sims, descs):
+            t_run += r.run(1)
+            total_n += d.n
+        rounds += 1
+    for r in sims:
+        r.close()
+    sample = (f"{len(descs)} of the {NSYS} systems ({sum(d.n for d in descs)} beads), "
+              f"{rounds} MD steps each through OpenMPSimulatorTraits BAOAB")
+    return total_n / t_run, sample, nthreads
+
+
+def run_reference_arm(args, ws, rank, pg):
+    """--impl reference: the reference's own CPU implementation on this
+    workload; each bench step = one MD step of every system of the batch."""
+    if rank != 0:
+        return
+    import oracle
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    descs = build_batch(args.nsys)
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference driver oracle/_ref was not built (reference tree absent at build time)"}))
+        return
+    sims = []
+    for d in descs:
+        r = oracle.Reference(d, parallel=True)
+        r.initialize()
+        sims.append(r)
+    ntot = sum(d.n for d in descs)
+    for _ in range(args.warmup):
+        for r in sims:
+            r.run(1)
+    t = 0.0
+    for _ in range(args.steps):
+        for r in sims:
+            t += r.run(1)
+    value = ntot * args.steps / t
+    threads = oracle.Reference.max_threads()
+    line = {
+        "metric": "particle-steps/s (batched polymer systems)", "value": value, "unit": "particle-steps/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(descs, precision="fp64 (reference CPU)", chunk=1),
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                         "sample": f"all {len(descs)} systems, 1 MD step per bench step, OpenMPSimulatorTraits"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    for r in sims:
+        r.close()
+    print(json.dumps(line))
+
+
+def workload_config(descs, precision, chunk):
+    return {
+        "workload": "configs[3]: batch of independent polymer melts (config-2 composition), "
+                    "log-uniform 500-20000 beads, T U[280,360] K, I U[0.05,0.3] M",
+        "systems": len(descs), "particles": int(sum(d.n for d in descs)),
+        "md_steps_per_bench_step": chunk, "precision": precision,
+        "integrator": "BAOAB dt=0.01 gamma=1", "partition": "cell lists, margin 0.5",
+        "l2": "inputs larger than L2 (resident arena of several hundred MB)",
+    }
+
+
+# ---------------------------------------------------------------- B200 arm
+def run_b200(args, ws, rank, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    from mjolnir_b200.engine import Engine
+
+    descs = build_batch(args.nsys)
+    ntot = sum(d.n for d in descs)
+    eng = Engine("mixed", device=local)
+    for d in descs:
+        eng.add_system(d)
+    eng.commit()
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
+
+    # ---- device-resident throughput
+    for _ in range(args.warmup):
+        eng.step(CHUNK)
+    eng.synchronize()
+    barrier(pg)
+    l0 = eng.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            eng.step(CHUNK)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+    launches = eng.launch_count() - l0
+    t_dev = e0.elapsed_time(e1) / 1e3
+    t_dev = max_over_ranks(t_dev, pg)
+    barrier(pg)
+    value = ws * ntot * CHUNK * args.steps / t_dev
+
+    # ---- end to end through the C ABI with pinned host buffers
+    pos = torch.empty((ntot, 3), dtype=torch.float64, pin_memory=True).numpy()
+    vel = torch.empty((ntot, 3), dtype=torch.float64, pin_memory=True).numpy()
+    eng.get_state_all(pos, vel)
+    e2e_steps = max(2, args.steps // 2)
+    eng.set_state_all(pos, vel)
+    eng.step(CHUNK)
+    eng.get_state_all(pos, vel)
+    barrier(pg)
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        eng.set_state_all(pos, vel)        # H2D of the step's inputs
+        eng.step(CHUNK)
+        eng.get_state_all(pos, vel)        # D2H of the step's result
+    f1.record(stream)
+    f1.synchronize()
+    t_e2e = max_over_ranks(f0.elapsed_time(f1) / 1e3, pg)
+    e2e = ws * ntot * CHUNK * e2e_steps / t_e2e
+    h2d = 2 * pos.nbytes
+    d2h = 2 * pos.nbytes
+
+    # ---- roofline of the dominant kernel (the pair kernels)
+    peak, peak_kind = measured_peaks()
+    kern = {}
+    for term in ("exv", "dh"):
+        ms = eng.time_kernel(term, reps=20)
+        pcut = eng.pair_count(-1, term)
+        nslots = sum(len(getattr(d, term).idx) for d in descs)
+        # algorithmic bytes per launch: own position+parameter (32 B) and the
+        # fixed-point force written (24 B) per participant, one 4-byte index
+        # per interacting pair (margin-free P_cut)
+        bytes_alg = nslots * (32 + 24) + 4 * pcut
+        kern[term] = {"ms": ms, "pcut": pcut, "slots": nslots, "bytes": bytes_alg,
+                      "gbs": bytes_alg / (ms * 1e-3) / 1e9}
+    dom = max(kern, key=lambda k: kern[k]["ms"])
+    k = kern[dom]
+    roofline = {"bound": "hbm", "kernel": f"k_pair<{dom}> (+ its slot gather)", "achieved": k["gbs"],
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": k["gbs"] / peak,
+                "traffic": None, "ms_per_launch": k["ms"], "pairs_in_cutoff": k["pcut"],
+                "algorithmic_bytes": k["bytes"], "other": {t: kern[t] for t in kern if t != dom}}
+
+    # ---- plain single-system FP64 path on a sample of the same systems
+    plain = None
+    if not args.no_plain and rank == 0:
+        sample = descs[: min(16, len(descs))]
+        tot_ps, tot_t = 0, 0.0
+        for d in sample:
+            pe = Engine("fp64", device=local)
+            pe.add_system(d)
+            pe.commit()
+            pe.step(5)
+            pe.synchronize()
+            ps = torch.cuda.ExternalStream(pe.stream_handle(), device=local)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(ps)
+            pe.step(CHUNK)
+            b.record(ps)
+            b.synchronize()
+            tot_t += a.elapsed_time(b) / 1e3
+            tot_ps += d.n * CHUNK
+            pe.close()
+        plain = {"value": tot_ps / tot_t, "unit": "particle-steps/s",
+                 "sample": f"{len(sample)} systems run one at a time, FP64, {CHUNK} steps each",
+                 "batched_over_plain": value / ws / (tot_ps / tot_t)}
+
+    # ---- CPU baseline: the reference's OpenMP path on a bounded sample
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and ws == 1:
+        try:
+            res = cpu_reference_rate(descs[:32], budget_s=12.0)
+            if res:
+                rate, sample, threads = res
+                cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                       "sample": sample}
+        except Exception as ex:  # the baseline must not sink the GPU line
+            cpu = {"value": None, "error": str(ex)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s (batched polymer systems)", "value": value, "unit": "particle-steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 pair math, f64 state, i64 fixed-point forces",
+            "data": "synthetic",
+            "config": workload_config(descs, precision="mixed", chunk=CHUNK),
+            "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "plain_fp64_single_system": plain,
+        }
+        print(json.dumps(line))
+    eng.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, ws, rank, pg)
+        else:
+            run_b200(args, ws, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,224 @@
+/*
+ * mjolnir_b200 -- C ABI of the B200 implementation of Mjolnir's per-step hot
+ * path: cell-list / Verlet-list rebuild, ExcludedVolume, DebyeHuckel and
+ * LennardJones pair forces and energies, harmonic bonds and angles, cosine
+ * dihedrals, and the BAOAB Langevin (or velocity Verlet) update.
+ *
+ * Plain pointers and sizes only.  Every call returns MJG_OK (0) or a negative
+ * MJG_E* code, and mjg_last_error() then describes the failure; no C++
+ * exception crosses this boundary.  Host arrays are owned by the caller and
+ * are only read (or written) during the call.  Device memory is owned by the
+ * context.  A context is used by one host thread at a time.
+ *
+ * Mjolnir has no C ABI and no plugin loader: the GPU path replaces the C++
+ * virtual interfaces named beside each entry point.  Citations are
+ * path:line inside the Mjolnir source tree (v1.31.0).
+ *
+ * Indices are 0-based particle indices local to their system.  Units are
+ * those of the caller's input (the reference's kcal/mol + angstrom by
+ * default: input/read_units.hpp:32-91).
+ */
+#ifndef MJOLNIR_B200_H
+#define MJOLNIR_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MJG_API __attribute__((visibility("default")))
+#else
+#define MJG_API
+#endif
+
+typedef struct mjg_context mjg_context;
+
+enum {
+    MJG_OK = 0,
+    MJG_EINVAL = -1,      /* bad argument                                   */
+    MJG_ECUDA = -2,       /* a CUDA call failed                             */
+    MJG_ESTATE = -3,      /* call not allowed in the current state          */
+    MJG_ENOMEM = -4,      /* device memory exhausted                        */
+    MJG_EOVERFLOW = -5,   /* a force left the fixed-point range             */
+    MJG_ENONFINITE = -6   /* non-finite positions or forces (blown up)      */
+};
+enum { MJG_PRECISION_FP64 = 0, MJG_PRECISION_MIXED = 1 };
+enum { MJG_UNLIMITED = 0, MJG_PERIODIC_CUBOID = 1 };
+enum { MJG_TERM_BOND = 0, MJG_TERM_ANGLE = 1, MJG_TERM_DIHEDRAL = 2,
+       MJG_TERM_EXV = 3, MJG_TERM_DH = 4, MJG_TERM_LJ = 5 };
+enum { MJG_IGNORE_NOTHING = 0, MJG_IGNORE_SELF = 1, MJG_IGNORE_OTHERS = 2 };
+enum { MJG_BAOAB = 0, MJG_VELOCITY_VERLET = 1 };
+
+/* ---------------------------------------------------------------- context */
+
+/* A context owns one arena on one device: every committed system lives in
+ * it, and mjg_step advances all of them in the same kernels.
+ * precision: MJG_PRECISION_FP64 (the reference's arithmetic) or
+ * MJG_PRECISION_MIXED (FP32 pair potentials, FP64 state, forces summed in
+ * 64-bit fixed point).  No counterpart in the reference (its parallelism is
+ * OpenMP inside one process, mjolnir/omp/*). */
+MJG_API int  mjg_context_create(int device, int precision, mjg_context** out);
+MJG_API void mjg_context_destroy(mjg_context* ctx);
+MJG_API const char* mjg_last_error(const mjg_context* ctx);
+/* 1: capture one MD step as a CUDA graph and replay it (default 1). */
+MJG_API int  mjg_context_set_graphs(mjg_context* ctx, int enable);
+/* Options: the per-step work of mjg_step is also checked for list overflow
+ * and rolled back when it happens (default 1). */
+MJG_API int  mjg_context_set_rollback(mjg_context* ctx, int enable);
+
+/* ---------------------------------------------------------------- systems */
+
+/* System<traits>(num_particles, boundary) with its particles
+ * (core/System.hpp:41-52; input/read_system.hpp:93-290).  lower/upper are
+ * the periodic box (ignored for MJG_UNLIMITED).  pos/vel/mass: [3n], [3n], [n].
+ * Positions are wrapped into the box (System::initialize, core/System.hpp:58-67).
+ * Returns the system id through *sys_id. */
+MJG_API int mjg_system_create(mjg_context* ctx, int64_t n, int boundary,
+                      const double* lower, const double* upper,
+                      const double* pos, const double* vel, const double* mass,
+                      int* sys_id);
+/* system.attributes temperature [K] and ionic_strength [mol/L]
+ * (core/System.hpp:151-156). */
+MJG_API int mjg_system_set_attributes(mjg_context* ctx, int sys, double temperature,
+                              double ionic_strength);
+/* Topology::add_connection for m pairs of the connection kind `kind`
+ * (core/Topology.hpp:165-195), e.g. a force-free "bond" chain
+ * (forcefield/local/DummyInteraction.hpp). */
+MJG_API int mjg_system_add_connections(mjg_context* ctx, int sys, const char* kind,
+                               int64_t m, const int64_t* pairs);
+/* Removes a system; its device state is freed at the next mjg_commit. */
+MJG_API int mjg_system_remove(mjg_context* ctx, int sys);
+
+/* ------------------------------------------------- global pair interactions
+ * GlobalPairInteraction<traits, Potential> (core/GlobalInteractionBase.hpp
+ * :20-36; forcefield/global/GlobalPairInteraction.hpp:26-136) with a
+ * CellList spatial partition of relative margin `margin`
+ * (input/read_spatial_partition.hpp:62-76; core/PeriodicGridCellList.hpp,
+ * core/UnlimitedGridCellList.hpp).  idx[np] lists the participants in input
+ * order; the last one leads no list (ParameterList leading_participants). */
+
+/* ExcludedVolumePotential(cutoff_ratio, epsilon) + ExcludedVolumeParameterList
+ * (forcefield/global/ExcludedVolumePotential.hpp:26-133,139-282). */
+MJG_API int mjg_exv_set(mjg_context* ctx, int sys, double epsilon, double cutoff_ratio,
+                double margin, int64_t np, const int64_t* idx, const double* radius);
+/* DebyeHuckelPotential(cutoff_ratio) + DebyeHuckelParameterList
+ * (forcefield/global/DebyeHuckelPotential.hpp:17-186,196-353); uses the
+ * system's temperature and ionic_strength. */
+MJG_API int mjg_dh_set(mjg_context* ctx, int sys, double cutoff_ratio, double margin,
+               int64_t np, const int64_t* idx, const double* charge);
+/* LennardJonesPotential(cutoff_ratio) + LorentzBerthelotRule
+ * (forcefield/global/LennardJonesPotential.hpp:15-110, ParameterList.hpp:185-329). */
+MJG_API int mjg_lj_set(mjg_context* ctx, int sys, double cutoff_ratio, double margin,
+               int64_t np, const int64_t* idx, const double* sigma, const double* epsilon);
+/* The ignore rules of one global term: ignore.molecule and
+ * ignore.particles_within (input/read_global_potential.hpp:29-90,168-190;
+ * core/ExclusionList.hpp:56-234).  kinds[k] / within[k] for nk connection
+ * kinds.  Default: ignore nothing. */
+MJG_API int mjg_ignore_set(mjg_context* ctx, int sys, int term, int ignore_molecule,
+                   int nk, const char* const* kinds, const int32_t* within);
+
+/* ------------------------------------------------------ local interactions
+ * LocalInteractionBase<traits> (core/LocalInteractionBase.hpp:24-40);
+ * `topology` is the connection kind written to the topology
+ * (write_topology), "none" for no edges. */
+
+/* BondLengthInteraction<HarmonicPotential> (BondLengthInteraction.hpp:126-148,
+ * HarmonicPotential.hpp:11-52; V = k (r - v0)^2). idx[2m]. */
+MJG_API int mjg_bonds_set(mjg_context* ctx, int sys, const char* topology, int64_t m,
+                  const int64_t* idx, const double* k, const double* v0);
+/* BondAngleInteraction<HarmonicPotential> (BondAngleInteraction.hpp:129-188). idx[3m]. */
+MJG_API int mjg_angles_set(mjg_context* ctx, int sys, const char* topology, int64_t m,
+                   const int64_t* idx, const double* k, const double* v0);
+/* DihedralAngleInteraction<CosinePotential> (DihedralAngleInteraction.hpp
+ * :157-227, CosinePotential.hpp:13-58; V = k (1 + cos(n (phi - v0)))). idx[4m]. */
+MJG_API int mjg_dihedrals_set(mjg_context* ctx, int sys, const char* topology, int64_t m,
+                      const int64_t* idx, const double* k, const int32_t* n,
+                      const double* v0);
+
+/* -------------------------------------------------------------- integrator
+ * BAOABLangevinIntegrator(dt, gammas) (core/BAOABLangevinIntegrator.hpp:34-99;
+ * input/read_integrator.hpp:120-187) or VelocityVerletIntegrator(dt)
+ * (core/VelocityVerletIntegrator.hpp).  gamma[n] (ignored for Verlet).  The
+ * Langevin noise is Philox4x32-10 keyed by `seed` and counted by
+ * (particle, step), in place of the reference's mt19937 stream
+ * (core/RandomNumberGenerator.hpp:13-86). */
+MJG_API int mjg_integrator_set(mjg_context* ctx, int sys, int kind, double dt,
+                       const double* gamma, uint64_t seed);
+
+/* ------------------------------------------------------------- execution */
+
+/* Packs every live system into device memory, builds the topology,
+ * exclusion lists, cell lists and Verlet lists, and evaluates the first
+ * forces (ForceField::initialize, core/ForceField.hpp:47-63, and
+ * Integrator::initialize, core/BAOABLangevinIntegrator.hpp:135-168).
+ * Systems already resident keep their positions, velocities, forces and
+ * noise counters.  Call again after adding or removing systems. */
+MJG_API int mjg_commit(mjg_context* ctx);
+/* nsteps integrator steps of every committed system
+ * (BAOABLangevinIntegrator::step, core/BAOABLangevinIntegrator.hpp:170-240,
+ * called by MolecularDynamicsSimulator::step, core/MolecularDynamicsSimulator.hpp:83-102). */
+MJG_API int mjg_step(mjg_context* ctx, int64_t nsteps);
+/* Waits for the context's stream. */
+MJG_API int mjg_synchronize(mjg_context* ctx);
+/* Rebuilds every Verlet list at the current positions. */
+MJG_API int mjg_rebuild(mjg_context* ctx);
+
+/* State of one system in host layout [3n] (NULL to skip an array).
+ * mjg_set_state replaces positions and/or velocities (wrapped into the box)
+ * and marks the lists for a rebuild. */
+MJG_API int mjg_get_state(mjg_context* ctx, int sys, double* pos, double* vel, double* force);
+MJG_API int mjg_set_state(mjg_context* ctx, int sys, const double* pos, const double* vel);
+/* Same for all committed systems at once, concatenated in commit order. */
+MJG_API int mjg_get_state_all(mjg_context* ctx, double* pos, double* vel);
+MJG_API int mjg_set_state_all(mjg_context* ctx, const double* pos, const double* vel);
+
+/* Energies of every term at the current positions, out[6] indexed by
+ * MJG_TERM_* (ForceField::calc_energy / format_energy, core/ForceField.hpp:123-160). */
+MJG_API int mjg_energies(mjg_context* ctx, int sys, double* out);
+/* Forces [3n] and energy of a single term at the current positions, without
+ * disturbing the integrator's force array (GlobalInteractionBase /
+ * LocalInteractionBase::calc_force_and_energy). */
+MJG_API int mjg_term_force(mjg_context* ctx, int sys, int term, double* force, double* energy);
+/* The half Verlet list of a global term as it was last built, as (i, j)
+ * pairs with i < j sorted by i then j -- the content of
+ * SpatialPartition::neighbors() (core/NeighborList.hpp:151-266).  Writes at
+ * most cap pairs to pairs[2 cap] and the total to *count. */
+MJG_API int mjg_neighbors(mjg_context* ctx, int sys, int term, int64_t* pairs,
+                  int64_t cap, int64_t* count);
+/* Number of interacting pairs (i < j inside the potential's own cutoff) of a
+ * global term at the current positions, for one system or all (sys = -1):
+ * the margin-free pair count P_cut of the pair kernel's roofline.  No
+ * counterpart in the reference. */
+MJG_API int mjg_pair_count(mjg_context* ctx, int sys, int term, int64_t* count);
+/* The CUDA stream (cudaStream_t) all of the context's work is enqueued on,
+ * for callers that record events or order their own work against it. */
+MJG_API int mjg_context_get_stream(mjg_context* ctx, void** stream);
+/* Average duration in milliseconds of one launch of a term's force kernel
+ * (pair kernel for MJG_TERM_EXV/DH/LJ, bonded kernel otherwise) over `reps`
+ * back-to-back launches on the current lists, timed with CUDA events on the
+ * context's stream; the integrator's forces are not touched. */
+MJG_API int mjg_time_kernel(mjg_context* ctx, int term, int reps, double* ms_per_launch);
+/* Sets the per-particle neighbour capacity of a global term's lists.  A
+ * capacity below what a later rebuild needs is detected on the device, the
+ * current mjg_step chunk is rolled back, the lists grow and the chunk runs
+ * again (with rollback enabled); used to test that path.  No counterpart in
+ * the reference, whose lists are growable std::vectors. */
+MJG_API int mjg_set_list_capacity(mjg_context* ctx, int term, int cap);
+/* Number of list rebuilds of a term since commit (reduce_margin rebuilds). */
+MJG_API int mjg_rebuild_count(mjg_context* ctx, int sys, int term, int64_t* count);
+/* Number of integrator steps taken by a system since it was created. */
+MJG_API int mjg_step_count(mjg_context* ctx, int sys, int64_t* steps);
+
+/* Number of particles of all committed systems, and of one system. */
+MJG_API int mjg_particle_count(mjg_context* ctx, int sys, int64_t* n);
+/* Bytes of device memory the context holds. */
+MJG_API int mjg_device_bytes(mjg_context* ctx, int64_t* bytes);
+/* Kernel launches issued since the context was created (graph replays count
+ * each kernel node). */
+MJG_API int mjg_launch_count(mjg_context* ctx, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

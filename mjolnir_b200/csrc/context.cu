@@ -1,0 +1,1429 @@
+// The context behind the C ABI: host-side system descriptions, packing of all
+// live systems into one device arena, and the per-step schedule
+//   integrate_first -> margin -> [rebuild per term] -> local forces ->
+//   pair forces per term -> integrate_last
+// captured once as a CUDA graph and replayed.  This is the work of
+// MolecularDynamicsSimulator::step + BAOABLangevinIntegrator::step +
+// ForceField::calc_force (core/MolecularDynamicsSimulator.hpp:83-102,
+// core/BAOABLangevinIntegrator.hpp:170-240, core/ForceField.hpp:101-109)
+// for every system of the arena at once.
+#include "../../include/mjolnir_b200.h"
+#include "kernels.cuh"
+#include "model.hpp"
+
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace mjg {
+
+std::atomic<long long> g_launches{0};
+void note_launches(int k) {g_launches.fetch_add(k, std::memory_order_relaxed);}
+
+
+namespace {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        const cudaError_t e_ = (call);                                                   \
+        if(e_ != cudaSuccess)                                                            \
+        {                                                                                \
+            throw Error(e_ == cudaErrorMemoryAllocation ? MJG_ENOMEM : MJG_ECUDA,        \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));             \
+        }                                                                                \
+    } while(0)
+
+// device buffer with byte accounting
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {release();}
+    void release() {if(p) {cudaFree(p); p = nullptr; bytes = 0;}}
+    void alloc(size_t b)
+    {
+        release();
+        if(b == 0) {return;}
+        CK(cudaMalloc(&p, b));
+        bytes = b;
+    }
+    template<typename T> T* as() const {return static_cast<T*>(p);}
+};
+
+struct HostGlobal {
+    bool on = false;
+    double eps = 0.0, cutoff_ratio = 0.0, margin = 0.5;
+    std::vector<int64_t> idx;
+    std::vector<double> p0, p1;
+    int ignore_mol = IGN_NOTHING;
+    std::vector<std::pair<std::string, int>> within;
+};
+struct HostLocal {
+    std::string kind = "none";
+    std::vector<int64_t> idx;
+    std::vector<double> k, v0;
+    std::vector<int32_t> n;
+    int64_t m() const {return (int64_t)k.size();}
+};
+struct HostSystem {
+    bool alive = true;
+    bool resident = false;       // part of the current arena
+    int arena_slot = -1;
+    int64_t n = 0;
+    int boundary = B_UNLIMITED;
+    double lower[3] = {0, 0, 0}, upper[3] = {0, 0, 0};
+    std::vector<double> pos, vel, mass, force;
+    bool force_valid = false;
+    double T = 300.0, I = 0.1;
+    std::vector<std::pair<std::string, std::pair<int64_t, int64_t>>> connections;
+    HostGlobal g[NGLOBAL];
+    HostLocal bond, angle, dihd;
+    int integrator = I_BAOAB;
+    double dt = 0.01;
+    std::vector<double> gamma;
+    uint64_t seed = 0;
+    uint64_t step = 0;
+    int rebuilds[NGLOBAL] = {0, 0, 0};
+    int64_t off = 0;             // particle offset in the arena
+};
+
+struct TermDev {
+    DevBuf part_particle, part_p0, part_p1, part_lead, part_sys, part_cell;
+    DevBuf cell_count, cell_start, cell_fill, block_sums;
+    DevBuf slot_part, slot_particle, slot_lead, slot_sys, slot_pd, slot_p1;
+    DevBuf nnb, nbr, max_count, any_rebuild;
+    DevBuf ex_start, ex_idx;
+    int cap_alloc = 0;           // capacity the nbr buffer was sized for
+    TermArrays t{};
+};
+
+}  // namespace
+}  // namespace mjg
+
+struct mjg_context {
+    int device = 0;
+    int precision = mjg::P_FP64;
+    bool graphs = true;
+    bool rollback = true;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::vector<mjg::HostSystem> sys;
+
+    // arena
+    bool committed = false;
+    std::vector<int> arena_ids;            // arena slot -> system id
+    long long n_tot = 0;
+    mjg::DevBuf d_sys, d_pos, d_vel, d_force, d_coef, d_psys, d_staging, d_mol;
+    mjg::DevBuf b_sys, b_pos, b_vel, b_force;   // rollback copies
+    mjg::DevBuf d_force_scratch;
+    mjg::TermDev term[mjg::NGLOBAL];
+    mjg::DevBuf l_bond_idx, l_bond_k, l_bond_v0, l_bond_sys;
+    mjg::DevBuf l_angle_idx, l_angle_k, l_angle_v0, l_angle_sys;
+    mjg::DevBuf l_dihd_idx, l_dihd_k, l_dihd_n, l_dihd_v0, l_dihd_sys;
+    mjg::Arena arena{};
+    mjg::LocalArrays local{};
+    std::vector<mjg::SysDev> h_sys;
+
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    long long graph_nodes = 0;
+    bool graph_dirty = true;
+};
+
+namespace mjg {
+namespace {
+
+int64_t device_bytes(const mjg_context* c)
+{
+    int64_t b = 0;
+    const DevBuf* bufs[] = {&c->d_sys, &c->d_pos, &c->d_vel, &c->d_force, &c->d_coef, &c->d_psys,
+                            &c->d_staging, &c->d_mol, &c->b_sys, &c->b_pos, &c->b_vel, &c->b_force,
+                            &c->d_force_scratch, &c->l_bond_idx, &c->l_bond_k, &c->l_bond_v0,
+                            &c->l_bond_sys, &c->l_angle_idx, &c->l_angle_k, &c->l_angle_v0,
+                            &c->l_angle_sys, &c->l_dihd_idx, &c->l_dihd_k, &c->l_dihd_n,
+                            &c->l_dihd_v0, &c->l_dihd_sys};
+    for(auto* x : bufs) {b += (int64_t)x->bytes;}
+    for(const auto& t : c->term)
+    {
+        const DevBuf* tb[] = {&t.part_particle, &t.part_p0, &t.part_p1, &t.part_lead, &t.part_sys,
+                              &t.part_cell, &t.cell_count, &t.cell_start, &t.cell_fill,
+                              &t.block_sums, &t.slot_part, &t.slot_particle, &t.slot_lead,
+                              &t.slot_sys, &t.slot_pd, &t.slot_p1, &t.nnb, &t.nbr, &t.max_count,
+                              &t.any_rebuild, &t.ex_start, &t.ex_idx};
+        for(auto* x : tb) {b += (int64_t)x->bytes;}
+    }
+    return b;
+}
+
+template<typename T>
+void upload(DevBuf& d, const std::vector<T>& h, cudaStream_t s)
+{
+    d.alloc(sizeof(T) * h.size());
+    if(!h.empty()) {CK(cudaMemcpyAsync(d.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));}
+}
+
+HostSystem& get_sys(mjg_context* c, int id)
+{
+    if(id < 0 || id >= (int)c->sys.size() || !c->sys[id].alive)
+    {
+        throw Error(MJG_EINVAL, "no such system: " + std::to_string(id));
+    }
+    return c->sys[id];
+}
+
+HostSystem& get_resident(mjg_context* c, int id)
+{
+    HostSystem& s = get_sys(c, id);
+    if(!c->committed || !s.resident) {throw Error(MJG_ESTATE, "system " + std::to_string(id) + " is not committed");}
+    return s;
+}
+
+void release_graph(mjg_context* c)
+{
+    if(c->graph_exec) {cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr;}
+    if(c->graph) {cudaGraphDestroy(c->graph); c->graph = nullptr;}
+    c->graph_dirty = true;
+}
+
+// ------------------------------------------------------------ schedule
+
+void enqueue_forces(mjg_context* c, const Arena& a, bool nf, bool ne)
+{
+    launch_local(a, c->local, 7, nf, ne, 0, c->stream);
+    for(int g = 0; g < NGLOBAL; ++g) {launch_pair(a, g, c->term[g].t, nf, ne, 0, c->stream);}
+}
+
+void enqueue_step(mjg_context* c)
+{
+    const Arena& a = c->arena;
+    TermArrays ts[NGLOBAL] = {c->term[0].t, c->term[1].t, c->term[2].t};
+    launch_integrate_first(a, c->stream);
+    launch_margin(a, ts, c->stream);
+    for(int g = 0; g < NGLOBAL; ++g) {launch_rebuild(a, g, c->term[g].t, 0, c->stream);}
+    enqueue_forces(c, a, true, false);
+    launch_integrate_last(a, c->stream);
+}
+
+void capture_graph(mjg_context* c)
+{
+    release_graph(c);
+    const long long before = g_launches.load();
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c);
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamEndCapture(c->stream, &g));
+    c->graph = g;
+    CK(cudaGraphInstantiate(&c->graph_exec, g, 0));
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    c->graph_nodes = (long long)nn;
+    // capture counted the launches once; graph replays add them per replay
+    g_launches.fetch_sub(g_launches.load() - before);
+    c->graph_dirty = false;
+}
+
+void download_sys(mjg_context* c)
+{
+    c->h_sys.resize(c->arena_ids.size());
+    if(!c->h_sys.empty())
+    {
+        CK(cudaMemcpyAsync(c->h_sys.data(), c->d_sys.p, sizeof(SysDev) * c->h_sys.size(),
+                           cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+void upload_sys(mjg_context* c)
+{
+    if(!c->h_sys.empty())
+    {
+        CK(cudaMemcpyAsync(c->d_sys.p, c->h_sys.data(), sizeof(SysDev) * c->h_sys.size(),
+                           cudaMemcpyHostToDevice, c->stream));
+    }
+}
+
+int list_capacity(int max_count) {return max_count + max_count / 4 + 16;}
+
+// (re)allocates the neighbour arrays of term g for capacity cap
+void alloc_lists(mjg_context* c, int g, int cap)
+{
+    TermDev& T = c->term[g];
+    T.nbr.alloc(sizeof(int) * (size_t)cap * (size_t)(T.t.np > 0 ? T.t.np : 1));
+    T.t.nbr = T.nbr.as<int>();
+    T.t.cap = cap;
+    T.cap_alloc = cap;
+    release_graph(c);
+}
+
+// forced rebuild of every list; grows capacities until nothing overflows
+void rebuild_all(mjg_context* c)
+{
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        TermDev& T = c->term[g];
+        if(!T.t.on || T.t.np == 0) {continue;}
+        for(int attempt = 0; attempt < 4; ++attempt)
+        {
+            CK(cudaMemsetAsync(T.t.max_count, 0, sizeof(int), c->stream));
+            launch_rebuild(c->arena, g, T.t, 1, c->stream);
+            int mx = 0;
+            CK(cudaMemcpyAsync(&mx, T.t.max_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            if(mx <= T.t.cap) {break;}
+            alloc_lists(c, g, list_capacity(mx));
+        }
+    }
+    // rebuild_all may have raised ST_LIST_OVERFLOW on the way; clear it
+    download_sys(c);
+    for(auto& s : c->h_sys) {s.status &= ~ST_LIST_OVERFLOW;}
+    upload_sys(c);
+}
+
+void compute_initial_forces(mjg_context* c)
+{
+    launch_zero_force(c->arena, c->stream);
+    enqueue_forces(c, c->arena, true, false);
+}
+
+// ------------------------------------------------------------- commit
+
+void save_resident_state(mjg_context* c)
+{
+    if(!c->committed) {return;}
+    CK(cudaStreamSynchronize(c->stream));
+    download_sys(c);
+    for(size_t k = 0; k < c->arena_ids.size(); ++k)
+    {
+        HostSystem& s = c->sys[c->arena_ids[k]];
+        const SysDev& d = c->h_sys[k];
+        s.step = d.step;
+        for(int g = 0; g < NGLOBAL; ++g) {s.rebuilds[g] = d.g[g].rebuilds;}
+        if(!s.alive) {continue;}
+        s.pos.resize(3 * s.n); s.vel.resize(3 * s.n); s.force.resize(3 * s.n);
+        double* st = c->d_staging.as<double>();
+        launch_pack_state(c->arena, st, 0, s.off, s.n, c->stream);
+        CK(cudaMemcpyAsync(s.pos.data(), st, sizeof(double) * 3 * s.n, cudaMemcpyDeviceToHost, c->stream));
+        launch_pack_state(c->arena, st, 1, s.off, s.n, c->stream);
+        CK(cudaMemcpyAsync(s.vel.data(), st, sizeof(double) * 3 * s.n, cudaMemcpyDeviceToHost, c->stream));
+        launch_pack_state(c->arena, st, 2, s.off, s.n, c->stream);
+        CK(cudaMemcpyAsync(s.force.data(), st, sizeof(double) * 3 * s.n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        s.force_valid = true;
+    }
+}
+
+int kind_id(std::map<std::string, int>& kinds, const std::string& k)
+{
+    auto it = kinds.find(k);
+    if(it != kinds.end()) {return it->second;}
+    const int id = (int)kinds.size();
+    kinds[k] = id;
+    return id;
+}
+
+void commit(mjg_context* c)
+{
+    CK(cudaSetDevice(c->device));
+    save_resident_state(c);
+    release_graph(c);
+    for(auto& s : c->sys) {s.resident = false; s.arena_slot = -1;}
+
+    // ---- host packing
+    std::vector<int> ids;
+    for(int i = 0; i < (int)c->sys.size(); ++i)
+    {
+        HostSystem& s = c->sys[i];
+        if(!s.alive) {continue;}
+        if(s.integrator == I_BAOAB && (int64_t)s.gamma.size() != s.n)
+        {
+            throw Error(MJG_ESTATE, "system " + std::to_string(i) + " has no integrator set");
+        }
+        ids.push_back(i);
+    }
+    const Units u;
+    long long n_tot = 0;
+    for(int id : ids) {c->sys[id].off = n_tot; n_tot += c->sys[id].n;}
+    const int nsys = (int)ids.size();
+
+    std::vector<double4> pos(n_tot), vel(n_tot), coef(n_tot);
+    std::vector<int> psys(n_tot), mol(n_tot);
+    std::vector<SysDev> hs(nsys);
+    std::vector<long long> ex_start[NGLOBAL];
+    std::vector<int> ex_idx[NGLOBAL];
+    for(int g = 0; g < NGLOBAL; ++g) {ex_start[g].push_back(0);}
+
+    // per term participant data
+    std::vector<int> part_particle[NGLOBAL], part_sys[NGLOBAL], cell_sys[NGLOBAL];
+    std::vector<double> part_p0[NGLOBAL], part_p1[NGLOBAL];
+    std::vector<unsigned char> part_lead[NGLOBAL];
+    int ncell[NGLOBAL] = {0, 0, 0};
+
+    // local terms
+    std::vector<int> b_idx, b_sys, a_idx, a_sys, d_idx, d_sys, d_n;
+    std::vector<double> b_k, b_v0, a_k, a_v0, d_k, d_v0;
+
+    long long mol_base = 0;
+    for(int k = 0; k < nsys; ++k)
+    {
+        HostSystem& s = c->sys[ids[k]];
+        s.resident = true;
+        s.arena_slot = k;
+        SysDev& d = hs[k];
+        std::memset(&d, 0, sizeof(SysDev));
+        d.off = s.off; d.n = s.n;
+        d.boundary = s.boundary;
+        d.integrator = s.integrator;
+        for(int x = 0; x < 3; ++x)
+        {
+            d.lower[x] = s.lower[x]; d.upper[x] = s.upper[x];
+            d.width[x] = s.upper[x] - s.lower[x];
+            d.halfw[x] = d.width[x] / 2;
+        }
+        d.seed = s.seed;
+        d.step = s.step;
+
+        // particles
+        const double halfdt = s.dt / 2;
+        const double kBT = u.kB * s.T;
+        for(int64_t i = 0; i < s.n; ++i)
+        {
+            double p[3] = {s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2]};
+            if(s.boundary == B_PERIODIC)          // adjust_position
+            {
+                for(int x = 0; x < 3; ++x)
+                {
+                    if(p[x] < d.lower[x]) {p[x] += d.width[x];}
+                    else if(p[x] >= d.upper[x]) {p[x] -= d.width[x];}
+                }
+            }
+            const long long gi = s.off + i;
+            pos[gi] = make_double4(p[0], p[1], p[2], 0.0);
+            vel[gi] = make_double4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], 0.0);
+            const double rmass = 1.0 / s.mass[i];
+            if(s.integrator == I_BAOAB)        // reset_parameters (:73-99)
+            {
+                const double gamma_dt = -1 * s.gamma[i] * s.dt;
+                coef[gi] = make_double4(halfdt * rmass, std::exp(gamma_dt),
+                                        std::sqrt(kBT * (1 - std::exp(2 * gamma_dt)) * rmass), halfdt);
+            }
+            else
+            {
+                coef[gi] = make_double4(halfdt * rmass, 1.0, 0.0, s.dt);
+            }
+            psys[gi] = k;
+        }
+
+        // topology: edges in the order the reference's local force field
+        // writes them (bond, angle, dihedral), then explicit connections
+        std::map<std::string, int> kinds;
+        const int bond_kind = kind_id(kinds, "bond");
+        TopologyGraph topo(s.n);
+        auto add_edges = [&](const HostLocal& L, int arity) {
+            if(L.kind.empty() || L.kind == "none") {return;}
+            const int kd = kind_id(kinds, L.kind);
+            for(int64_t t = 0; t < L.m(); ++t)
+            {
+                const int64_t* q = &L.idx[arity * t];
+                for(int x = 0; x < arity; ++x)
+                    for(int y = x + 1; y < arity; ++y) {topo.add(q[x], q[y], kd);}
+            }
+        };
+        add_edges(s.bond, 2);
+        add_edges(s.angle, 3);
+        add_edges(s.dihd, 4);
+        for(const auto& e : s.connections) {topo.add(e.second.first, e.second.second, kind_id(kinds, e.first));}
+        const std::vector<int64_t> m = topo.molecules(bond_kind);
+        int64_t nmol = 0;
+        for(int64_t i = 0; i < s.n; ++i)
+        {
+            mol[s.off + i] = (int)(mol_base + m[i]);
+            nmol = std::max(nmol, m[i] + 1);
+        }
+        mol_base += nmol;
+
+        // global terms
+        for(int g = 0; g < NGLOBAL; ++g)
+        {
+            const HostGlobal& H = s.g[g];
+            GlobalParams& G = d.g[g];
+            std::vector<std::pair<int, int>> kw;
+            for(const auto& w : H.within) {kw.emplace_back(kind_id(kinds, w.first), w.second);}
+            exclusion_csr(topo, s.n, kw, s.off, ex_start[g], ex_idx[g]);
+            if(!H.on) {continue;}
+            G.on = 1;
+            G.margin = H.margin;
+            G.cutoff_ratio = H.cutoff_ratio;
+            G.cutoff_ratio_sq = H.cutoff_ratio * H.cutoff_ratio;
+            G.ignore_mol = H.ignore_mol;
+            G.eps = H.eps;
+            const int64_t np = (int64_t)H.idx.size();
+            if(g == G_EXV)             // ExcludedVolumePotential.hpp:44-48,92-106
+            {
+                G.coef_at_cutoff = std::pow(1.0 / H.cutoff_ratio, 12);
+                double mr = 0;
+                for(double r : H.p0) {mr = std::max(mr, r);}
+                G.cutoff = np == 0 ? 1.0 : mr * 2 * H.cutoff_ratio;
+            }
+            else if(g == G_DH)         // DebyeHuckelPotential.hpp:126-167,245-248
+            {
+                const DHParams p = dh_params(s.T, s.I, H.cutoff_ratio);
+                G.debye = p.debye; G.inv_debye = p.inv_debye; G.abs_cutoff = p.abs_cutoff;
+                G.coef_at_cutoff = p.coef_at_cutoff; G.inv4pi = p.inv4pi;
+                G.cutoff = p.debye * H.cutoff_ratio;
+            }
+            else                       // LennardJonesPotential.hpp:36-41,75-91
+            {
+                G.coef_at_cutoff = std::pow(1.0 / H.cutoff_ratio, 12) - std::pow(1.0 / H.cutoff_ratio, 6);
+                double ms = 0;
+                for(double x : H.p0) {ms = std::max(ms, x);}
+                G.cutoff = np == 0 ? 1.0 : ms * H.cutoff_ratio;
+            }
+            const double r_c = G.cutoff * (1. + G.margin);
+            G.rl2 = r_c * r_c;
+            G.current_margin = G.cutoff * G.margin;
+            G.rebuild = 1;
+            G.rebuilds = s.rebuilds[g];
+
+            // cell grid
+            if(s.boundary == B_PERIODIC)
+            {
+                // PeriodicGridCellList::set_cutoff / initialize (:67-96, :383-395)
+                const double r = 1.0 / (G.cutoff * (1.0 + G.margin) + 1e-6);
+                long long dims[3];
+                for(int x = 0; x < 3; ++x) {dims[x] = std::max<long long>(3, (long long)std::floor(d.width[x] * r));}
+                // keep the grid within a few cells per participant (wider cells stay exact)
+                const long long limit = std::max<long long>(27, 8 * np + 64);
+                while(dims[0] * dims[1] * dims[2] > limit)
+                {
+                    int big = 0;
+                    for(int x = 1; x < 3; ++x) {if(dims[x] > dims[big]) {big = x;}}
+                    if(dims[big] <= 3) {break;}
+                    dims[big] -= 1;
+                }
+                for(int x = 0; x < 3; ++x)
+                {
+                    G.dims[x] = (int)dims[x];
+                    G.inv_w[x] = 1.0 / (d.width[x] / (double)dims[x]);
+                    G.origin[x] = d.lower[x];
+                }
+                G.hashed = 0;
+            }
+            else
+            {
+                // unbounded space: cells of cutoff (1 + margin)(1 + 1e-6) hashed
+                // modulo a grid sized to the system's current extent
+                const double w = G.cutoff * (1 + G.margin) * (1 + 1e-6);
+                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                for(int64_t q = 0; q < np; ++q)
+                {
+                    const int64_t i = H.idx[q];
+                    for(int x = 0; x < 3; ++x)
+                    {
+                        lo[x] = std::min(lo[x], s.pos[3 * i + x]);
+                        hi[x] = std::max(hi[x], s.pos[3 * i + x]);
+                    }
+                }
+                long long dims[3];
+                for(int x = 0; x < 3; ++x)
+                {
+                    const double ext = np > 0 ? hi[x] - lo[x] : 0.0;
+                    dims[x] = std::max<long long>(3, (long long)std::floor(ext / w) + 3);
+                }
+                const long long limit = std::max<long long>(27, 4 * np + 64);
+                while(dims[0] * dims[1] * dims[2] > limit)
+                {
+                    int big = 0;
+                    for(int x = 1; x < 3; ++x) {if(dims[x] > dims[big]) {big = x;}}
+                    if(dims[big] <= 3) {break;}
+                    dims[big] -= 1;
+                }
+                for(int x = 0; x < 3; ++x)
+                {
+                    G.dims[x] = (int)dims[x];
+                    G.inv_w[x] = 1.0 / w;
+                    G.origin[x] = 0.0;
+                }
+                G.hashed = 1;
+            }
+            G.ncell = G.dims[0] * G.dims[1] * G.dims[2];
+            G.cell_off = ncell[g];
+            ncell[g] += G.ncell;
+            for(int q = 0; q < G.ncell; ++q) {cell_sys[g].push_back(k);}
+            G.slot_off = (int)part_particle[g].size();
+            G.nslot = (int)np;
+            for(int64_t q = 0; q < np; ++q)
+            {
+                part_particle[g].push_back((int)(s.off + H.idx[q]));
+                part_sys[g].push_back(k);
+                part_p0[g].push_back(H.p0[q]);
+                part_p1[g].push_back(H.p1.empty() ? 0.0 : H.p1[q]);
+                part_lead[g].push_back(q + 1 < np ? 1 : 0);
+            }
+        }
+
+        // local terms
+        for(int64_t t = 0; t < s.bond.m(); ++t)
+        {
+            b_idx.push_back((int)(s.off + s.bond.idx[2 * t]));
+            b_idx.push_back((int)(s.off + s.bond.idx[2 * t + 1]));
+            b_k.push_back(s.bond.k[t]); b_v0.push_back(s.bond.v0[t]); b_sys.push_back(k);
+        }
+        for(int64_t t = 0; t < s.angle.m(); ++t)
+        {
+            for(int x = 0; x < 3; ++x) {a_idx.push_back((int)(s.off + s.angle.idx[3 * t + x]));}
+            a_k.push_back(s.angle.k[t]); a_v0.push_back(s.angle.v0[t]); a_sys.push_back(k);
+        }
+        for(int64_t t = 0; t < s.dihd.m(); ++t)
+        {
+            for(int x = 0; x < 4; ++x) {d_idx.push_back((int)(s.off + s.dihd.idx[4 * t + x]));}
+            d_k.push_back(s.dihd.k[t]); d_v0.push_back(s.dihd.v0[t]); d_n.push_back(s.dihd.n[t]);
+            d_sys.push_back(k);
+        }
+    }
+
+    // ---- device upload
+    cudaStream_t st = c->stream;
+    c->n_tot = n_tot;
+    c->arena_ids = ids;
+    c->h_sys = hs;
+    c->d_sys.alloc(sizeof(SysDev) * std::max(nsys, 1));
+    upload_sys(c);
+    upload(c->d_pos, pos, st);
+    upload(c->d_vel, vel, st);
+    upload(c->d_coef, coef, st);
+    upload(c->d_psys, psys, st);
+    upload(c->d_mol, mol, st);
+    c->d_force.alloc(32 * (size_t)std::max<long long>(n_tot, 1));
+    c->d_force_scratch.alloc(32 * (size_t)std::max<long long>(n_tot, 1));
+    c->d_staging.alloc(sizeof(double) * 3 * (size_t)std::max<long long>(n_tot, 1));
+    if(c->rollback)
+    {
+        c->b_sys.alloc(c->d_sys.bytes);
+        c->b_pos.alloc(c->d_pos.bytes);
+        c->b_vel.alloc(c->d_vel.bytes);
+        c->b_force.alloc(c->d_force.bytes);
+    }
+    else
+    {
+        c->b_sys.release(); c->b_pos.release(); c->b_vel.release(); c->b_force.release();
+    }
+
+    Arena& a = c->arena;
+    a = Arena{};
+    a.precision = c->precision;
+    a.n = n_tot;
+    a.nsys = nsys;
+    a.sys = c->d_sys.as<SysDev>();
+    a.pos = c->d_pos.as<double4>();
+    a.vel = c->d_vel.as<double4>();
+    a.force = c->d_force.p;
+    a.coef = c->d_coef.as<double4>();
+    a.psys = c->d_psys.as<int>();
+    a.staging = c->d_staging.as<double>();
+    a.mol = c->d_mol.as<int>();
+
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        TermDev& T = c->term[g];
+        upload(T.ex_start, ex_start[g], st);
+        if(ex_idx[g].empty()) {ex_idx[g].push_back(0);}
+        upload(T.ex_idx, ex_idx[g], st);
+        a.ex_start[g] = T.ex_start.as<long long>();
+        a.ex_idx[g] = T.ex_idx.as<int>();
+
+        TermArrays& t = T.t;
+        t = TermArrays{};
+        const long long np = (long long)part_particle[g].size();
+        t.on = np > 0 ? 1 : 0;
+        t.np = np;
+        t.ncell = ncell[g];
+        if(!t.on)
+        {
+            DevBuf* bufs[] = {&T.part_particle, &T.part_p0, &T.part_p1, &T.part_lead, &T.part_sys,
+                              &T.part_cell, &T.cell_count, &T.cell_start, &T.cell_fill,
+                              &T.block_sums, &T.slot_part, &T.slot_particle, &T.slot_lead,
+                              &T.slot_sys, &T.slot_pd, &T.slot_p1, &T.nnb, &T.nbr,
+                              &T.max_count, &T.any_rebuild};
+            for(auto* b : bufs) {b->release();}
+            continue;
+        }
+        upload(T.part_particle, part_particle[g], st);
+        upload(T.part_p0, part_p0[g], st);
+        upload(T.part_p1, part_p1[g], st);
+        upload(T.part_lead, part_lead[g], st);
+        upload(T.part_sys, part_sys[g], st);
+        T.part_cell.alloc(sizeof(int) * np);
+        T.cell_count.alloc(sizeof(int) * t.ncell);
+        T.cell_fill.alloc(sizeof(int) * t.ncell);
+        T.cell_start.alloc(sizeof(int) * (t.ncell + 1));
+        const int nblocks = (t.ncell + 2047) / 2048;
+        // block sums, one spare word, then the cell -> system map
+        std::vector<int> bs(nblocks + 1, 0);
+        bs.insert(bs.end(), cell_sys[g].begin(), cell_sys[g].end());
+        upload(T.block_sums, bs, st);
+        CK(cudaMemsetAsync(T.cell_count.p, 0, T.cell_count.bytes, st));
+        CK(cudaMemsetAsync(T.cell_fill.p, 0, T.cell_fill.bytes, st));
+        T.slot_part.alloc(sizeof(int) * np);
+        T.slot_particle.alloc(sizeof(int) * np);
+        T.slot_lead.alloc(np);
+        T.slot_sys.alloc(sizeof(int) * np);
+        T.slot_pd.alloc(sizeof(double4) * np);
+        T.slot_p1.alloc(sizeof(double) * np);
+        T.nnb.alloc(sizeof(int) * np);
+        T.max_count.alloc(sizeof(int));
+        T.any_rebuild.alloc(sizeof(int));
+        CK(cudaMemsetAsync(T.any_rebuild.p, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(T.nnb.p, 0, T.nnb.bytes, st));
+        t.part_particle = T.part_particle.as<int>();
+        t.part_p0 = T.part_p0.as<double>();
+        t.part_p1 = g == G_LJ ? T.part_p1.as<double>() : nullptr;
+        t.part_lead = T.part_lead.as<unsigned char>();
+        t.part_sys = T.part_sys.as<int>();
+        t.part_cell = T.part_cell.as<int>();
+        t.cell_count = T.cell_count.as<int>();
+        t.cell_start = T.cell_start.as<int>();
+        t.cell_fill = T.cell_fill.as<int>();
+        t.block_sums = T.block_sums.as<int>();
+        t.slot_part = T.slot_part.as<int>();
+        t.slot_particle = T.slot_particle.as<int>();
+        t.slot_lead = T.slot_lead.as<unsigned char>();
+        t.slot_sys = T.slot_sys.as<int>();
+        t.slot_pd = T.slot_pd.as<double4>();
+        t.slot_p1 = T.slot_p1.as<double>();
+        t.nnb = T.nnb.as<int>();
+        t.max_count = T.max_count.as<int>();
+        t.any_rebuild = T.any_rebuild.as<int>();
+        t.cap = 0;
+        T.nbr.release();
+        t.nbr = nullptr;
+        alloc_lists(c, g, 0);
+    }
+
+    // local
+    upload(c->l_bond_idx, b_idx, st);  upload(c->l_bond_k, b_k, st);
+    upload(c->l_bond_v0, b_v0, st);    upload(c->l_bond_sys, b_sys, st);
+    upload(c->l_angle_idx, a_idx, st); upload(c->l_angle_k, a_k, st);
+    upload(c->l_angle_v0, a_v0, st);   upload(c->l_angle_sys, a_sys, st);
+    upload(c->l_dihd_idx, d_idx, st);  upload(c->l_dihd_k, d_k, st);
+    upload(c->l_dihd_n, d_n, st);      upload(c->l_dihd_v0, d_v0, st);
+    upload(c->l_dihd_sys, d_sys, st);
+    LocalArrays& l = c->local;
+    l = LocalArrays{};
+    l.nbond = (long long)b_k.size(); l.nangle = (long long)a_k.size(); l.ndihd = (long long)d_k.size();
+    l.bond_idx = c->l_bond_idx.as<int>();   l.bond_k = c->l_bond_k.as<double>();
+    l.bond_v0 = c->l_bond_v0.as<double>();  l.bond_sys = c->l_bond_sys.as<int>();
+    l.angle_idx = c->l_angle_idx.as<int>(); l.angle_k = c->l_angle_k.as<double>();
+    l.angle_v0 = c->l_angle_v0.as<double>(); l.angle_sys = c->l_angle_sys.as<int>();
+    l.dihd_idx = c->l_dihd_idx.as<int>();   l.dihd_k = c->l_dihd_k.as<double>();
+    l.dihd_n = c->l_dihd_n.as<int>();       l.dihd_v0 = c->l_dihd_v0.as<double>();
+    l.dihd_sys = c->l_dihd_sys.as<int>();
+
+    c->committed = true;
+    rebuild_all(c);
+    compute_initial_forces(c);
+    // systems that were resident keep their exact force array
+    for(int k = 0; k < nsys; ++k)
+    {
+        HostSystem& s = c->sys[ids[k]];
+        if(!s.force_valid || (int64_t)s.force.size() != 3 * s.n) {continue;}
+        double* stg = c->d_staging.as<double>();
+        CK(cudaMemcpyAsync(stg, s.force.data(), sizeof(double) * 3 * s.n, cudaMemcpyHostToDevice, st));
+        launch_set_force(c->arena, stg, s.off, s.n, st);
+    }
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------ step
+
+void check_status(mjg_context* c, bool& overflow)
+{
+    overflow = false;
+    for(size_t k = 0; k < c->h_sys.size(); ++k)
+    {
+        const int st = c->h_sys[k].status;
+        if(st & ST_LIST_OVERFLOW) {overflow = true;}
+        if(st & ST_FIXED_OVERFLOW)
+        {
+            throw Error(MJG_EOVERFLOW, "system " + std::to_string(c->arena_ids[k]) +
+                        ": a force left the fixed-point range (|F| >= 2^22)");
+        }
+        if(st & ST_NONFINITE)
+        {
+            throw Error(MJG_ENONFINITE, "system " + std::to_string(c->arena_ids[k]) +
+                        ": non-finite displacement (the system blew up)");
+        }
+    }
+}
+
+void run_steps(mjg_context* c, int64_t nsteps)
+{
+    if(nsteps <= 0) {return;}
+    cudaStream_t st = c->stream;
+    for(int attempt = 0; attempt < 8; ++attempt)
+    {
+        if(c->rollback)
+        {
+            CK(cudaMemcpyAsync(c->b_sys.p, c->d_sys.p, c->d_sys.bytes, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(c->b_pos.p, c->d_pos.p, c->d_pos.bytes, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(c->b_vel.p, c->d_vel.p, c->d_vel.bytes, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(c->b_force.p, c->d_force.p, c->d_force.bytes, cudaMemcpyDeviceToDevice, st));
+        }
+        if(c->graphs)
+        {
+            if(c->graph_dirty || !c->graph_exec) {capture_graph(c);}
+            for(int64_t k = 0; k < nsteps; ++k) {CK(cudaGraphLaunch(c->graph_exec, st));}
+            note_launches((int)std::min<long long>(c->graph_nodes * nsteps, (1ll << 30)));
+        }
+        else
+        {
+            for(int64_t k = 0; k < nsteps; ++k) {enqueue_step(c);}
+        }
+        CK(cudaGetLastError());
+        download_sys(c);
+        bool overflow = false;
+        check_status(c, overflow);
+        if(!overflow) {return;}
+        if(!c->rollback) {throw Error(MJG_ESTATE, "a Verlet list overflowed (enable rollback)");}
+        // roll back, grow the lists, rebuild, retry
+        CK(cudaMemcpyAsync(c->d_sys.p, c->b_sys.p, c->d_sys.bytes, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(c->d_pos.p, c->b_pos.p, c->d_pos.bytes, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(c->d_vel.p, c->b_vel.p, c->d_vel.bytes, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(c->d_force.p, c->b_force.p, c->d_force.bytes, cudaMemcpyDeviceToDevice, st));
+        for(int g = 0; g < NGLOBAL; ++g)
+        {
+            TermDev& T = c->term[g];
+            if(!T.t.on) {continue;}
+            int mx = 0;
+            CK(cudaMemcpyAsync(&mx, T.t.max_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if(mx > T.t.cap) {alloc_lists(c, g, list_capacity(mx));}
+        }
+        rebuild_all(c);
+    }
+    throw Error(MJG_ESTATE, "Verlet lists kept overflowing");
+}
+
+}  // namespace
+}  // namespace mjg
+
+// ====================================================================== ABI
+
+using namespace mjg;
+
+#define ABI_BEGIN(ctx)                      \
+    if(!(ctx)) {return MJG_EINVAL;}         \
+    try {
+#define ABI_END(ctx)                                          \
+    return MJG_OK;                                            \
+    } catch(const mjg::Error& e) {(ctx)->err = e.what(); return e.code;}   \
+    catch(const std::bad_alloc&) {(ctx)->err = "host out of memory"; return MJG_ENOMEM;} \
+    catch(const std::exception& e) {(ctx)->err = e.what(); return MJG_EINVAL;}
+
+extern "C" {
+
+int mjg_context_create(int device, int precision, mjg_context** out)
+{
+    if(!out || (precision != MJG_PRECISION_FP64 && precision != MJG_PRECISION_MIXED)) {return MJG_EINVAL;}
+    *out = nullptr;
+    auto* c = new (std::nothrow) mjg_context();
+    if(!c) {return MJG_ENOMEM;}
+    c->device = device;
+    c->precision = precision;
+    if(cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    {
+        cudaGetLastError();
+        delete c;
+        return MJG_ECUDA;
+    }
+    *out = c;
+    return MJG_OK;
+}
+
+void mjg_context_destroy(mjg_context* c)
+{
+    if(!c) {return;}
+    cudaSetDevice(c->device);
+    if(c->stream) {cudaStreamSynchronize(c->stream);}
+    release_graph(c);
+    for(auto& t : c->term)
+    {
+        DevBuf* bufs[] = {&t.part_particle, &t.part_p0, &t.part_p1, &t.part_lead, &t.part_sys,
+                          &t.part_cell, &t.cell_count, &t.cell_start, &t.cell_fill, &t.block_sums,
+                          &t.slot_part, &t.slot_particle, &t.slot_lead, &t.slot_sys, &t.slot_pd,
+                          &t.slot_p1, &t.nnb, &t.nbr, &t.max_count, &t.any_rebuild, &t.ex_start,
+                          &t.ex_idx};
+        for(auto* b : bufs) {b->release();}
+    }
+    if(c->stream) {cudaStreamDestroy(c->stream);}
+    delete c;
+}
+
+const char* mjg_last_error(const mjg_context* c) {return c ? c->err.c_str() : "null context";}
+
+int mjg_context_set_graphs(mjg_context* c, int enable)
+{
+    ABI_BEGIN(c)
+    c->graphs = enable != 0;
+    release_graph(c);
+    ABI_END(c)
+}
+
+int mjg_context_set_rollback(mjg_context* c, int enable)
+{
+    ABI_BEGIN(c)
+    if(c->committed) {throw Error(MJG_ESTATE, "set rollback before mjg_commit");}
+    c->rollback = enable != 0;
+    ABI_END(c)
+}
+
+int mjg_system_create(mjg_context* c, int64_t n, int boundary, const double* lower,
+                      const double* upper, const double* pos, const double* vel,
+                      const double* mass, int* sys_id)
+{
+    ABI_BEGIN(c)
+    if(n <= 0 || !pos || !mass || !sys_id) {throw Error(MJG_EINVAL, "system needs n > 0, pos and mass");}
+    if(n > (int64_t)1 << 30) {throw Error(MJG_EINVAL, "too many particles in one system");}
+    if(boundary != MJG_UNLIMITED && boundary != MJG_PERIODIC_CUBOID) {throw Error(MJG_EINVAL, "unknown boundary");}
+    HostSystem s;
+    s.n = n;
+    s.boundary = boundary == MJG_PERIODIC_CUBOID ? B_PERIODIC : B_UNLIMITED;
+    if(s.boundary == B_PERIODIC)
+    {
+        if(!lower || !upper) {throw Error(MJG_EINVAL, "periodic boundary needs lower and upper");}
+        for(int x = 0; x < 3; ++x)
+        {
+            s.lower[x] = lower[x]; s.upper[x] = upper[x];
+            if(!(upper[x] > lower[x])) {throw Error(MJG_EINVAL, "periodic box has no volume");}
+        }
+    }
+    s.pos.assign(pos, pos + 3 * n);
+    s.vel = vel ? std::vector<double>(vel, vel + 3 * n) : std::vector<double>(3 * n, 0.0);
+    s.mass.assign(mass, mass + n);
+    for(double m : s.mass) {if(!(m > 0)) {throw Error(MJG_EINVAL, "masses must be positive");}}
+    c->sys.push_back(std::move(s));
+    *sys_id = (int)c->sys.size() - 1;
+    ABI_END(c)
+}
+
+int mjg_system_set_attributes(mjg_context* c, int sys, double T, double I)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "attributes are fixed once committed");}
+    if(!(T > 0) || !(I > 0)) {throw Error(MJG_EINVAL, "temperature and ionic strength must be positive");}
+    s.T = T; s.I = I;
+    ABI_END(c)
+}
+
+int mjg_system_add_connections(mjg_context* c, int sys, const char* kind, int64_t m, const int64_t* pairs)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "topology is fixed once committed");}
+    if(!kind || (m > 0 && !pairs)) {throw Error(MJG_EINVAL, "bad connections");}
+    for(int64_t k = 0; k < m; ++k)
+    {
+        const int64_t i = pairs[2 * k], j = pairs[2 * k + 1];
+        if(i < 0 || j < 0 || i >= s.n || j >= s.n) {throw Error(MJG_EINVAL, "connection index out of range");}
+        s.connections.push_back({kind, {i, j}});
+    }
+    ABI_END(c)
+}
+
+int mjg_system_remove(mjg_context* c, int sys)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    s.alive = false;
+    std::vector<double>().swap(s.pos);
+    std::vector<double>().swap(s.vel);
+    std::vector<double>().swap(s.force);
+    ABI_END(c)
+}
+
+static void check_idx(const HostSystem& s, int64_t np, const int64_t* idx)
+{
+    if(np < 0 || (np > 0 && !idx)) {throw Error(MJG_EINVAL, "bad participant list");}
+    std::vector<char> seen(s.n, 0);
+    for(int64_t k = 0; k < np; ++k)
+    {
+        if(idx[k] < 0 || idx[k] >= s.n) {throw Error(MJG_EINVAL, "participant index out of range");}
+        if(seen[idx[k]]) {throw Error(MJG_EINVAL, "participant listed twice");}
+        seen[idx[k]] = 1;
+    }
+}
+
+int mjg_exv_set(mjg_context* c, int sys, double eps, double cutoff_ratio, double margin,
+                int64_t np, const int64_t* idx, const double* radius)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "interactions are fixed once committed");}
+    check_idx(s, np, idx);
+    if(!(cutoff_ratio > 0) || !(margin >= 0) || (np > 0 && !radius)) {throw Error(MJG_EINVAL, "bad ExcludedVolume parameters");}
+    HostGlobal& g = s.g[G_EXV];
+    g.on = true; g.eps = eps; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
+    g.idx.assign(idx, idx + np); g.p0.assign(radius, radius + np); g.p1.clear();
+    ABI_END(c)
+}
+
+int mjg_dh_set(mjg_context* c, int sys, double cutoff_ratio, double margin, int64_t np,
+               const int64_t* idx, const double* charge)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "interactions are fixed once committed");}
+    check_idx(s, np, idx);
+    if(!(cutoff_ratio > 0) || !(margin >= 0) || (np > 0 && !charge)) {throw Error(MJG_EINVAL, "bad DebyeHuckel parameters");}
+    HostGlobal& g = s.g[G_DH];
+    g.on = true; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
+    g.idx.assign(idx, idx + np); g.p0.assign(charge, charge + np); g.p1.clear();
+    ABI_END(c)
+}
+
+int mjg_lj_set(mjg_context* c, int sys, double cutoff_ratio, double margin, int64_t np,
+               const int64_t* idx, const double* sigma, const double* epsilon)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "interactions are fixed once committed");}
+    check_idx(s, np, idx);
+    if(!(cutoff_ratio > 0) || !(margin >= 0) || (np > 0 && (!sigma || !epsilon))) {throw Error(MJG_EINVAL, "bad LennardJones parameters");}
+    HostGlobal& g = s.g[G_LJ];
+    g.on = true; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
+    g.idx.assign(idx, idx + np); g.p0.assign(sigma, sigma + np); g.p1.assign(epsilon, epsilon + np);
+    ABI_END(c)
+}
+
+int mjg_ignore_set(mjg_context* c, int sys, int term, int ignore_molecule, int nk,
+                   const char* const* kinds, const int32_t* within)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "interactions are fixed once committed");}
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "ignore rules apply to global terms");}
+    if(ignore_molecule < 0 || ignore_molecule > 2 || nk < 0 || (nk > 0 && (!kinds || !within)))
+    {
+        throw Error(MJG_EINVAL, "bad ignore rule");
+    }
+    HostGlobal& g = s.g[term - MJG_TERM_EXV];
+    g.ignore_mol = ignore_molecule;
+    g.within.clear();
+    for(int k = 0; k < nk; ++k)
+    {
+        if(!kinds[k] || within[k] < 0) {throw Error(MJG_EINVAL, "bad ignore.particles_within");}
+        g.within.emplace_back(kinds[k], (int)within[k]);
+    }
+    ABI_END(c)
+}
+
+static void set_local(mjg_context* c, int sys, HostLocal& L, const char* topology, int64_t m,
+                      const int64_t* idx, const double* k, const double* v0, const int32_t* n, int arity,
+                      const HostSystem& s)
+{
+    (void)c; (void)sys;
+    if(s.resident) {throw Error(MJG_ESTATE, "interactions are fixed once committed");}
+    if(m < 0 || (m > 0 && (!idx || !k || !v0))) {throw Error(MJG_EINVAL, "bad local interaction");}
+    for(int64_t t = 0; t < m * arity; ++t)
+    {
+        if(idx[t] < 0 || idx[t] >= s.n) {throw Error(MJG_EINVAL, "local interaction index out of range");}
+    }
+    L.kind = topology ? topology : "none";
+    L.idx.assign(idx, idx + m * arity);
+    L.k.assign(k, k + m);
+    L.v0.assign(v0, v0 + m);
+    if(n) {L.n.assign(n, n + m);} else {L.n.clear();}
+}
+
+int mjg_bonds_set(mjg_context* c, int sys, const char* topology, int64_t m, const int64_t* idx,
+                  const double* k, const double* v0)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    set_local(c, sys, s.bond, topology, m, idx, k, v0, nullptr, 2, s);
+    ABI_END(c)
+}
+
+int mjg_angles_set(mjg_context* c, int sys, const char* topology, int64_t m, const int64_t* idx,
+                   const double* k, const double* v0)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    set_local(c, sys, s.angle, topology, m, idx, k, v0, nullptr, 3, s);
+    ABI_END(c)
+}
+
+int mjg_dihedrals_set(mjg_context* c, int sys, const char* topology, int64_t m, const int64_t* idx,
+                      const double* k, const int32_t* n, const double* v0)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(m > 0 && !n) {throw Error(MJG_EINVAL, "dihedrals need n");}
+    set_local(c, sys, s.dihd, topology, m, idx, k, v0, n, 4, s);
+    ABI_END(c)
+}
+
+int mjg_integrator_set(mjg_context* c, int sys, int kind, double dt, const double* gamma, uint64_t seed)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "the integrator is fixed once committed");}
+    if(kind != MJG_BAOAB && kind != MJG_VELOCITY_VERLET) {throw Error(MJG_EINVAL, "unknown integrator");}
+    if(!(dt > 0)) {throw Error(MJG_EINVAL, "dt must be positive");}
+    if(kind == MJG_BAOAB && !gamma) {throw Error(MJG_EINVAL, "BAOAB needs gammas");}
+    s.integrator = kind == MJG_BAOAB ? I_BAOAB : I_VV;
+    s.dt = dt;
+    s.gamma = gamma ? std::vector<double>(gamma, gamma + s.n) : std::vector<double>(s.n, 0.0);
+    s.seed = seed;
+    ABI_END(c)
+}
+
+int mjg_commit(mjg_context* c)
+{
+    ABI_BEGIN(c)
+    commit(c);
+    ABI_END(c)
+}
+
+int mjg_step(mjg_context* c, int64_t nsteps)
+{
+    ABI_BEGIN(c)
+    if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
+    if(nsteps < 0) {throw Error(MJG_EINVAL, "negative step count");}
+    run_steps(c, nsteps);
+    ABI_END(c)
+}
+
+int mjg_synchronize(mjg_context* c)
+{
+    ABI_BEGIN(c)
+    CK(cudaStreamSynchronize(c->stream));
+    ABI_END(c)
+}
+
+int mjg_rebuild(mjg_context* c)
+{
+    ABI_BEGIN(c)
+    if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
+    rebuild_all(c);
+    CK(cudaStreamSynchronize(c->stream));
+    ABI_END(c)
+}
+
+int mjg_get_state(mjg_context* c, int sys, double* pos, double* vel, double* force)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_resident(c, sys);
+    double* stg = c->d_staging.as<double>();
+    double* outs[3] = {pos, vel, force};
+    for(int w = 0; w < 3; ++w)
+    {
+        if(!outs[w]) {continue;}
+        launch_pack_state(c->arena, stg, w, s.off, s.n, c->stream);
+        CK(cudaMemcpyAsync(outs[w], stg, sizeof(double) * 3 * s.n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    ABI_END(c)
+}
+
+[[maybe_unused]] static void mark_all_rebuild(mjg_context* c)
+{
+    download_sys(c);
+    for(auto& d : c->h_sys)
+        for(auto& g : d.g) {if(g.on) {g.rebuild = 1;}}
+    upload_sys(c);
+}
+
+int mjg_set_state(mjg_context* c, int sys, const double* pos, const double* vel)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_resident(c, sys);
+    double* stg = c->d_staging.as<double>();
+    if(pos)
+    {
+        std::vector<double> p(pos, pos + 3 * s.n);
+        if(s.boundary == B_PERIODIC)
+        {
+            for(int64_t i = 0; i < s.n; ++i)
+                for(int x = 0; x < 3; ++x)
+                {
+                    const double w = s.upper[x] - s.lower[x];
+                    if(p[3 * i + x] < s.lower[x]) {p[3 * i + x] += w;}
+                    else if(p[3 * i + x] >= s.upper[x]) {p[3 * i + x] -= w;}
+                }
+        }
+        CK(cudaMemcpyAsync(stg, p.data(), sizeof(double) * 3 * s.n, cudaMemcpyHostToDevice, c->stream));
+        launch_unpack_state(c->arena, stg, nullptr, s.off, s.n, c->stream);
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if(vel)
+    {
+        CK(cudaMemcpyAsync(stg, vel, sizeof(double) * 3 * s.n, cudaMemcpyHostToDevice, c->stream));
+        launch_unpack_state(c->arena, nullptr, stg, s.off, s.n, c->stream);
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if(pos)
+    {
+        rebuild_all(c);
+        // forces at the new positions (the integrator's next B step uses them)
+        compute_initial_forces(c);
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    ABI_END(c)
+}
+
+int mjg_get_state_all(mjg_context* c, double* pos, double* vel)
+{
+    ABI_BEGIN(c)
+    if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
+    double* stg = c->d_staging.as<double>();
+    if(pos)
+    {
+        launch_pack_state(c->arena, stg, 0, 0, c->n_tot, c->stream);
+        CK(cudaMemcpyAsync(pos, stg, sizeof(double) * 3 * c->n_tot, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if(vel)
+    {
+        CK(cudaStreamSynchronize(c->stream));
+        launch_pack_state(c->arena, stg, 1, 0, c->n_tot, c->stream);
+        CK(cudaMemcpyAsync(vel, stg, sizeof(double) * 3 * c->n_tot, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    ABI_END(c)
+}
+
+int mjg_set_state_all(mjg_context* c, const double* pos, const double* vel)
+{
+    ABI_BEGIN(c)
+    if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
+    double* stg = c->d_staging.as<double>();
+    if(vel)
+    {
+        CK(cudaMemcpyAsync(stg, vel, sizeof(double) * 3 * c->n_tot, cudaMemcpyHostToDevice, c->stream));
+        launch_unpack_state(c->arena, nullptr, stg, 0, c->n_tot, c->stream);
+    }
+    if(pos)
+    {
+        // positions are taken as given (already inside their boxes)
+        CK(cudaMemcpyAsync(stg, pos, sizeof(double) * 3 * c->n_tot, cudaMemcpyHostToDevice, c->stream));
+        launch_unpack_state(c->arena, stg, nullptr, 0, c->n_tot, c->stream);
+        rebuild_all(c);
+        compute_initial_forces(c);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    ABI_END(c)
+}
+
+int mjg_energies(mjg_context* c, int sys, double* out)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_resident(c, sys);
+    if(!out) {throw Error(MJG_EINVAL, "out is NULL");}
+    launch_clear_energy(c->arena, c->stream);
+    Arena a = c->arena;
+    a.force = c->d_force_scratch.p;
+    enqueue_forces(c, a, false, true);
+    download_sys(c);
+    for(int t = 0; t < NTERMS; ++t) {out[t] = c->h_sys[s.arena_slot].energy[t];}
+    ABI_END(c)
+}
+
+int mjg_term_force(mjg_context* c, int sys, int term, double* force, double* energy)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_resident(c, sys);
+    if(term < 0 || term >= NTERMS) {throw Error(MJG_EINVAL, "unknown term");}
+    Arena a = c->arena;
+    a.force = c->d_force_scratch.p;
+    launch_clear_energy(a, c->stream);
+    launch_zero_force(a, c->stream);
+    if(term <= MJG_TERM_DIHEDRAL) {launch_local(a, c->local, 1 << term, true, true, 0, c->stream);}
+    else {launch_pair(a, term - MJG_TERM_EXV, c->term[term - MJG_TERM_EXV].t, true, true, 0, c->stream);}
+    if(force)
+    {
+        double* stg = c->d_staging.as<double>();
+        launch_pack_state(a, stg, 2, s.off, s.n, c->stream);
+        CK(cudaMemcpyAsync(force, stg, sizeof(double) * 3 * s.n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    download_sys(c);
+    if(energy) {*energy = c->h_sys[s.arena_slot].energy[term];}
+    ABI_END(c)
+}
+
+int mjg_neighbors(mjg_context* c, int sys, int term, int64_t* pairs, int64_t cap, int64_t* count)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_resident(c, sys);
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !count) {throw Error(MJG_EINVAL, "bad neighbour query");}
+    const int g = term - MJG_TERM_EXV;
+    const TermArrays& t = c->term[g].t;
+    *count = 0;
+    if(!t.on || !s.g[g].on) {throw Error(MJG_EINVAL, "term not present in this system");}
+    CK(cudaStreamSynchronize(c->stream));
+    download_sys(c);
+    const GlobalParams& G = c->h_sys[s.arena_slot].g[g];
+    const int so = G.slot_off, ns = G.nslot;
+    std::vector<int> nnb(t.np), part(t.np);
+    CK(cudaMemcpy(nnb.data(), t.nnb, sizeof(int) * t.np, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(part.data(), t.slot_particle, sizeof(int) * t.np, cudaMemcpyDeviceToHost));
+    std::vector<int> col(t.np);
+    std::vector<std::pair<int64_t, int64_t>> out;
+    for(int k = 0; k < t.cap; ++k)
+    {
+        bool any = false;
+        for(int q = so; q < so + ns; ++q) {if(nnb[q] > k) {any = true; break;}}
+        if(!any) {break;}
+        CK(cudaMemcpy(col.data(), t.nbr + (size_t)k * t.np, sizeof(int) * t.np, cudaMemcpyDeviceToHost));
+        for(int q = so; q < so + ns; ++q)
+        {
+            if(nnb[q] <= k) {continue;}
+            const int64_t i = part[q] - s.off, j = part[col[q]] - s.off;
+            if(i < j) {out.emplace_back(i, j);}
+        }
+    }
+    std::sort(out.begin(), out.end());
+    *count = (int64_t)out.size();
+    if(pairs)
+    {
+        const int64_t w = std::min<int64_t>(cap, (int64_t)out.size());
+        for(int64_t k = 0; k < w; ++k) {pairs[2 * k] = out[k].first; pairs[2 * k + 1] = out[k].second;}
+    }
+    ABI_END(c)
+}
+
+int mjg_rebuild_count(mjg_context* c, int sys, int term, int64_t* count)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_resident(c, sys);
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !count) {throw Error(MJG_EINVAL, "bad query");}
+    download_sys(c);
+    *count = c->h_sys[s.arena_slot].g[term - MJG_TERM_EXV].rebuilds;
+    ABI_END(c)
+}
+
+int mjg_step_count(mjg_context* c, int sys, int64_t* steps)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_resident(c, sys);
+    if(!steps) {throw Error(MJG_EINVAL, "steps is NULL");}
+    download_sys(c);
+    *steps = (int64_t)c->h_sys[s.arena_slot].step;
+    ABI_END(c)
+}
+
+int mjg_particle_count(mjg_context* c, int sys, int64_t* n)
+{
+    ABI_BEGIN(c)
+    if(!n) {throw Error(MJG_EINVAL, "n is NULL");}
+    if(sys < 0) {*n = c->n_tot;}
+    else {*n = get_sys(c, sys).n;}
+    ABI_END(c)
+}
+
+int mjg_device_bytes(mjg_context* c, int64_t* bytes)
+{
+    ABI_BEGIN(c)
+    if(!bytes) {throw Error(MJG_EINVAL, "bytes is NULL");}
+    *bytes = device_bytes(c);
+    ABI_END(c)
+}
+
+int mjg_context_get_stream(mjg_context* c, void** stream)
+{
+    ABI_BEGIN(c)
+    if(!stream) {throw Error(MJG_EINVAL, "stream is NULL");}
+    *stream = (void*)c->stream;
+    ABI_END(c)
+}
+
+int mjg_time_kernel(mjg_context* c, int term, int reps, double* ms)
+{
+    ABI_BEGIN(c)
+    if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
+    if(term < 0 || term >= NTERMS || reps <= 0 || !ms) {throw Error(MJG_EINVAL, "bad timing request");}
+    Arena a = c->arena;
+    a.force = c->d_force_scratch.p;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto once = [&]() {
+        if(term <= MJG_TERM_DIHEDRAL) {launch_local(a, c->local, 1 << term, true, false, 0, c->stream);}
+        else {launch_pair(a, term - MJG_TERM_EXV, c->term[term - MJG_TERM_EXV].t, true, false, 0, c->stream);}
+    };
+    once();   // warm
+    CK(cudaEventRecord(e0, c->stream));
+    for(int r = 0; r < reps; ++r) {once();}
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = (double)t / reps;
+    ABI_END(c)
+}
+
+int mjg_set_list_capacity(mjg_context* c, int term, int cap)
+{
+    ABI_BEGIN(c)
+    if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || cap < 0) {throw Error(MJG_EINVAL, "bad capacity request");}
+    TermDev& T = c->term[term - MJG_TERM_EXV];
+    if(!T.t.on) {throw Error(MJG_EINVAL, "term not present");}
+    if(cap <= T.cap_alloc)
+    {
+        // the buffer keeps its size, so the current lists stay readable; the
+        // next rebuild that needs more than cap partners reports an overflow
+        T.t.cap = cap;
+        release_graph(c);
+    }
+    else
+    {
+        alloc_lists(c, term - MJG_TERM_EXV, cap);
+        rebuild_all(c);
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    ABI_END(c)
+}
+
+int mjg_pair_count(mjg_context* c, int sys, int term, int64_t* count)
+{
+    ABI_BEGIN(c)
+    if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !count) {throw Error(MJG_EINVAL, "bad query");}
+    int slot = -1;
+    if(sys >= 0) {slot = get_resident(c, sys).arena_slot;}
+    DevBuf tmp;
+    tmp.alloc(sizeof(unsigned long long));
+    CK(cudaMemsetAsync(tmp.p, 0, tmp.bytes, c->stream));
+    launch_count_cut(c->arena, term - MJG_TERM_EXV, c->term[term - MJG_TERM_EXV].t, slot,
+                     tmp.as<unsigned long long>(), c->stream);
+    unsigned long long h = 0;
+    CK(cudaMemcpyAsync(&h, tmp.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *count = (int64_t)h;
+    ABI_END(c)
+}
+
+int mjg_launch_count(mjg_context* c, int64_t* launches)
+{
+    ABI_BEGIN(c)
+    if(!launches) {throw Error(MJG_EINVAL, "launches is NULL");}
+    *launches = g_launches.load();
+    ABI_END(c)
+}
+
+}  // extern "C"

@@ -1,0 +1,286 @@
+// BAOAB Langevin and velocity-Verlet updates (core/BAOABLangevinIntegrator.hpp
+// :170-240, core/VelocityVerletIntegrator.hpp:90-135), the Verlet-skin
+// bookkeeping of reduce_margin (core/PeriodicGridCellList.hpp:100-110), and
+// the host<->arena layout conversions.
+//
+// One thread per particle over every system of the arena; a particle finds its
+// system's box, seed and step through psys.  Arithmetic is FP64 with explicit
+// round-to-nearest products and sums, in the reference's operation order.
+#include "kernels.cuh"
+
+namespace mjg {
+
+namespace {
+
+constexpr int TPB = 256;
+
+template<int PREC>
+__device__ __forceinline__ void load_force(const void* force, long long i, double& fx, double& fy, double& fz)
+{
+    if(PREC == P_FP64)
+    {
+        const double4 f = static_cast<const double4*>(force)[i];
+        fx = f.x; fy = f.y; fz = f.z;
+    }
+    else
+    {
+        const longlong4 f = static_cast<const longlong4*>(force)[i];
+        fx = fx_to_double(f.x); fy = fx_to_double(f.y); fz = fx_to_double(f.z);
+    }
+}
+
+template<int PREC>
+__device__ __forceinline__ void zero_force(void* force, long long i)
+{
+    if(PREC == P_FP64) {static_cast<double4*>(force)[i] = make_double4(0, 0, 0, 0);}
+    else               {static_cast<longlong4*>(force)[i] = make_longlong4(0, 0, 0, 0);}
+}
+
+// B-A-O-A of BAOAB (or the first half-kick and drift of velocity Verlet),
+// force reset and the per-system largest squared displacement.
+template<int PREC>
+__global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
+{
+    const long long i = (long long)blockIdx.x * TPB + threadIdx.x;
+    const bool active = i < a.n;
+    int s = active ? a.psys[i] : 0;
+    double d2 = 0.0;
+    if(active)
+    {
+        const SysDev& S = a.sys[s];
+        double4 p = a.pos[i];
+        double4 v = a.vel[i];
+        const double4 c = a.coef[i];     // {halfdt*rmass, exp(-gamma dt), noise, halfdt | dt}
+        double fx, fy, fz;
+        load_force<PREC>(a.force, i, fx, fy, fz);
+        double dx, dy, dz;
+        if(S.integrator == I_BAOAB)
+        {
+            double r0, r1, r2;
+            gaussian3(S.seed, (unsigned long long)(i - S.off), S.step, r0, r1, r2);
+            v.x = __dadd_rn(v.x, __dmul_rn(c.x, fx));          // v += halfdt*rm*f
+            v.y = __dadd_rn(v.y, __dmul_rn(c.x, fy));
+            v.z = __dadd_rn(v.z, __dmul_rn(c.x, fz));
+            dx = __dmul_rn(c.w, v.x);                          // dp  = halfdt*v
+            dy = __dmul_rn(c.w, v.y);
+            dz = __dmul_rn(c.w, v.z);
+            v.x = __dmul_rn(v.x, c.y);                         // v  *= exp(-gamma dt)
+            v.y = __dmul_rn(v.y, c.y);
+            v.z = __dmul_rn(v.z, c.y);
+            v.x = __dadd_rn(v.x, __dmul_rn(c.z, r0));          // v  += noise*R
+            v.y = __dadd_rn(v.y, __dmul_rn(c.z, r1));
+            v.z = __dadd_rn(v.z, __dmul_rn(c.z, r2));
+            dx = __dadd_rn(dx, __dmul_rn(c.w, v.x));           // dp += halfdt*v
+            dy = __dadd_rn(dy, __dmul_rn(c.w, v.y));
+            dz = __dadd_rn(dz, __dmul_rn(c.w, v.z));
+        }
+        else
+        {
+            v.x = __dadd_rn(v.x, __dmul_rn(c.x, fx));          // v += (halfdt*rm)*f
+            v.y = __dadd_rn(v.y, __dmul_rn(c.x, fy));
+            v.z = __dadd_rn(v.z, __dmul_rn(c.x, fz));
+            dx = __dmul_rn(c.w, v.x);                          // disp = dt*v
+            dy = __dmul_rn(c.w, v.y);
+            dz = __dmul_rn(c.w, v.z);
+        }
+        p.x = __dadd_rn(p.x, dx);
+        p.y = __dadd_rn(p.y, dy);
+        p.z = __dadd_rn(p.z, dz);
+        if(S.boundary == B_PERIODIC)                           // adjust_position
+        {
+            if(p.x < S.lower[0]) {p.x = __dadd_rn(p.x, S.width[0]);} else if(p.x >= S.upper[0]) {p.x = __dsub_rn(p.x, S.width[0]);}
+            if(p.y < S.lower[1]) {p.y = __dadd_rn(p.y, S.width[1]);} else if(p.y >= S.upper[1]) {p.y = __dsub_rn(p.y, S.width[1]);}
+            if(p.z < S.lower[2]) {p.z = __dadd_rn(p.z, S.width[2]);} else if(p.z >= S.upper[2]) {p.z = __dsub_rn(p.z, S.width[2]);}
+        }
+        a.pos[i] = p;
+        a.vel[i] = v;
+        zero_force<PREC>(a.force, i);
+        d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        if(!(d2 == d2) || d2 > 1e300) {atomicOr(&a.sys[s].status, ST_NONFINITE); d2 = 0.0;}
+    }
+    // per-system maximum: warp-level when the warp sits in one system
+    const unsigned full = 0xffffffffu;
+    const int s0 = __shfl_sync(full, s, 0);
+    const bool uniform = __all_sync(full, !active || s == s0);
+    if(uniform)
+    {
+        double m = d2;
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1) {m = fmax(m, __shfl_xor_sync(full, m, o));}
+        const bool any = __any_sync(full, active);
+        if(any && (threadIdx.x & 31) == 0)
+        {
+            atomicMax(&a.sys[s0].max_disp2, (unsigned long long)__double_as_longlong(m));
+        }
+    }
+    else if(active)
+    {
+        atomicMax(&a.sys[s].max_disp2, (unsigned long long)__double_as_longlong(d2));
+    }
+}
+
+// reduce_margin(2 sqrt(max|dp|^2)) for every global term of every system;
+// a term whose skin is used up is flagged for a rebuild.  Also advances the
+// noise step counter.
+__global__ void k_margin(Arena a, int* any0, int* any1, int* any2)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if(s >= a.nsys) {return;}
+    SysDev& S = a.sys[s];
+    const double d = 2 * sqrt(__longlong_as_double((long long)S.max_disp2));
+    S.max_disp2 = 0ull;
+    S.step += 1ull;
+    int* any[3] = {any0, any1, any2};
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        GlobalParams& G = S.g[g];
+        if(!G.on) {continue;}
+        G.current_margin = __dsub_rn(G.current_margin, d);
+        if(G.current_margin < 0)
+        {
+            G.rebuild = 1;
+            if(any[g]) {atomicOr(any[g], 1);}
+        }
+    }
+}
+
+// final half-kick v += (halfdt/m) f of both integrators
+template<int PREC>
+__global__ void __launch_bounds__(TPB) k_integrate_last(Arena a)
+{
+    const long long i = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(i >= a.n) {return;}
+    const double c = a.coef[i].x;
+    double fx, fy, fz;
+    load_force<PREC>(a.force, i, fx, fy, fz);
+    double4 v = a.vel[i];
+    v.x = __dadd_rn(v.x, __dmul_rn(c, fx));
+    v.y = __dadd_rn(v.y, __dmul_rn(c, fy));
+    v.z = __dadd_rn(v.z, __dmul_rn(c, fz));
+    a.vel[i] = v;
+}
+
+template<int PREC>
+__global__ void k_zero_force(Arena a)
+{
+    const long long i = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(i < a.n) {zero_force<PREC>(a.force, i);}
+}
+
+__global__ void k_unpack(Arena a, const double* src_pos, const double* src_vel, long long first, long long count)
+{
+    const long long k = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(k >= count) {return;}
+    const long long i = first + k;
+    if(src_pos) {a.pos[i] = make_double4(src_pos[3*k], src_pos[3*k+1], src_pos[3*k+2], 0.0);}
+    if(src_vel) {a.vel[i] = make_double4(src_vel[3*k], src_vel[3*k+1], src_vel[3*k+2], 0.0);}
+}
+
+template<int PREC>
+__global__ void k_pack(Arena a, double* dst, int what, long long first, long long count)
+{
+    const long long k = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(k >= count) {return;}
+    const long long i = first + k;
+    double x, y, z;
+    if(what == 0)      {const double4 p = a.pos[i]; x = p.x; y = p.y; z = p.z;}
+    else if(what == 1) {const double4 v = a.vel[i]; x = v.x; y = v.y; z = v.z;}
+    else               {load_force<PREC>(a.force, i, x, y, z);}
+    dst[3*k] = x; dst[3*k+1] = y; dst[3*k+2] = z;
+}
+
+template<int PREC>
+__global__ void k_set_force(Arena a, const double* src, long long first, long long count)
+{
+    const long long k = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(k >= count) {return;}
+    const long long i = first + k;
+    if(PREC == P_FP64)
+    {
+        static_cast<double4*>(a.force)[i] = make_double4(src[3*k], src[3*k+1], src[3*k+2], 0.0);
+    }
+    else
+    {
+        static_cast<longlong4*>(a.force)[i] = make_longlong4(fx_from_double(src[3*k]),
+            fx_from_double(src[3*k+1]), fx_from_double(src[3*k+2]), 0);
+    }
+}
+
+__global__ void k_clear_energy(Arena a)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if(s >= a.nsys) {return;}
+    for(int t = 0; t < NTERMS; ++t) {a.sys[s].energy[t] = 0.0;}
+}
+
+inline unsigned blocks(long long n) {return (unsigned)((n + TPB - 1) / TPB);}
+
+}  // namespace
+
+void launch_integrate_first(const Arena& a, cudaStream_t s)
+{
+    if(a.n == 0) {return;}
+    if(a.precision == P_FP64) {k_integrate_first<P_FP64><<<blocks(a.n), TPB, 0, s>>>(a);}
+    else                      {k_integrate_first<P_MIXED><<<blocks(a.n), TPB, 0, s>>>(a);}
+    note_launches(1);
+}
+
+void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s)
+{
+    if(a.nsys == 0) {return;}
+    k_margin<<<(a.nsys + 127) / 128, 128, 0, s>>>(a,
+        t[0].on ? t[0].any_rebuild : nullptr, t[1].on ? t[1].any_rebuild : nullptr,
+        t[2].on ? t[2].any_rebuild : nullptr);
+    note_launches(1);
+}
+
+void launch_integrate_last(const Arena& a, cudaStream_t s)
+{
+    if(a.n == 0) {return;}
+    if(a.precision == P_FP64) {k_integrate_last<P_FP64><<<blocks(a.n), TPB, 0, s>>>(a);}
+    else                      {k_integrate_last<P_MIXED><<<blocks(a.n), TPB, 0, s>>>(a);}
+    note_launches(1);
+}
+
+void launch_zero_force(const Arena& a, cudaStream_t s)
+{
+    if(a.n == 0) {return;}
+    if(a.precision == P_FP64) {k_zero_force<P_FP64><<<blocks(a.n), TPB, 0, s>>>(a);}
+    else                      {k_zero_force<P_MIXED><<<blocks(a.n), TPB, 0, s>>>(a);}
+    note_launches(1);
+}
+
+void launch_unpack_state(const Arena& a, const double* src_pos, const double* src_vel,
+                         long long first, long long count, cudaStream_t s)
+{
+    if(count == 0) {return;}
+    k_unpack<<<blocks(count), TPB, 0, s>>>(a, src_pos, src_vel, first, count);
+    note_launches(1);
+}
+
+void launch_pack_state(const Arena& a, double* dst, int what, long long first, long long count,
+                       cudaStream_t s)
+{
+    if(count == 0) {return;}
+    if(a.precision == P_FP64) {k_pack<P_FP64><<<blocks(count), TPB, 0, s>>>(a, dst, what, first, count);}
+    else                      {k_pack<P_MIXED><<<blocks(count), TPB, 0, s>>>(a, dst, what, first, count);}
+    note_launches(1);
+}
+
+void launch_clear_energy(const Arena& a, cudaStream_t s)
+{
+    if(a.nsys == 0) {return;}
+    k_clear_energy<<<(a.nsys + 127) / 128, 128, 0, s>>>(a);
+    note_launches(1);
+}
+
+void launch_set_force(const Arena& a, const double* src, long long first, long long count,
+                      cudaStream_t s)
+{
+    if(count == 0) {return;}
+    if(a.precision == P_FP64) {k_set_force<P_FP64><<<blocks(count), TPB, 0, s>>>(a, src, first, count);}
+    else                      {k_set_force<P_MIXED><<<blocks(count), TPB, 0, s>>>(a, src, first, count);}
+    note_launches(1);
+}
+
+}  // namespace mjg

@@ -1,0 +1,90 @@
+// Host-side launch wrappers of every kernel of the hot path.  All launches go
+// to the stream given; nothing here allocates or synchronises.
+#pragma once
+#include "common.cuh"
+
+namespace mjg {
+
+// Device-resident arrays of one arena (all pointers are device pointers).
+struct Arena {
+    int       precision;        // Precision
+    long long n;                // particles
+    int       nsys;
+    SysDev*   sys;              // [nsys]
+    double4*  pos;
+    double4*  vel;
+    void*     force;            // double4 (P_FP64) or longlong4 (P_MIXED)
+    double4*  coef;
+    int*      psys;
+    double*   staging;          // [3 n] host-layout staging for copies
+    // exclusions (per global term): excluded partners of every particle,
+    // sorted, CSR over particles
+    const long long* ex_start[NGLOBAL];
+    const int*       ex_idx[NGLOBAL];
+    const int*       mol;       // molecule id per particle (global numbering)
+};
+
+// Per global term arrays (participants grouped by system, input order inside).
+struct TermArrays {
+    int        on;
+    long long  np;              // participants (= slots)
+    int        ncell;           // total cells over all systems
+    int        cap;             // neighbour capacity per slot
+    const int* part_particle;   // [np] global particle index
+    const double* part_p0;      // [np] radius / charge / sigma
+    const double* part_p1;      // [np] LJ epsilon
+    const unsigned char* part_lead; // [np] leading participant
+    const int* part_sys;        // [np]
+    int*       part_cell;       // [np]
+    int*       cell_count;      // [ncell]
+    int*       cell_start;      // [ncell + 1]
+    int*       cell_fill;       // [ncell]
+    int*       block_sums;      // scan scratch
+    int*       slot_part;       // [np] participant of slot (cell order)
+    int*       slot_particle;   // [np] global particle of slot
+    unsigned char* slot_lead;   // [np]
+    int*       slot_sys;        // [np]
+    float4*    slot_pf;         // [np] packed per-slot parameters (mixed)
+    double4*   slot_pd;         // [np] x, y, z, p0 gathered each step
+    double*    slot_p1;         // [np] LJ epsilon per slot
+    int*       nnb;             // [np] partners per slot
+    int*       nbr;             // [cap * np] column-major
+    int*       max_count;       // [1] largest list seen at the last build
+    int*       any_rebuild;     // [1]
+};
+
+void launch_unpack_state(const Arena& a, const double* src_pos, const double* src_vel,
+                         long long first, long long count, cudaStream_t s);
+void launch_pack_state(const Arena& a, double* dst, int what, long long first, long long count,
+                       cudaStream_t s);
+
+void launch_integrate_first(const Arena& a, cudaStream_t s);
+void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s);
+void launch_integrate_last(const Arena& a, cudaStream_t s);
+void launch_zero_force(const Arena& a, cudaStream_t s);
+
+void launch_rebuild(const Arena& a, int gterm, TermArrays& t, int force_all, cudaStream_t s);
+void launch_pair(const Arena& a, int gterm, TermArrays& t, bool need_force, bool need_energy,
+                 int calc_energy_form, cudaStream_t s);
+
+struct LocalArrays {
+    long long nbond, nangle, ndihd;
+    const int* bond_idx;   const double* bond_k;  const double* bond_v0;  const int* bond_sys;
+    const int* angle_idx;  const double* angle_k; const double* angle_v0; const int* angle_sys;
+    const int* dihd_idx;   const double* dihd_k;  const int* dihd_n; const double* dihd_v0;
+    const int* dihd_sys;
+};
+void launch_local(const Arena& a, const LocalArrays& l, int which_mask, bool need_force,
+                  bool need_energy, int calc_energy_form, cudaStream_t s);
+
+void launch_clear_energy(const Arena& a, cudaStream_t s);
+void launch_count_cut(const Arena& a, int g, TermArrays& t, int sys, unsigned long long* out,
+                      cudaStream_t s);
+// writes host-layout forces [3 count] (staging) into the arena's force array
+void launch_set_force(const Arena& a, const double* src, long long first, long long count,
+                      cudaStream_t s);
+
+// kernel launch accounting (every wrapper reports what it enqueued)
+void note_launches(int k);
+
+}  // namespace mjg

@@ -107,54 +107,16 @@ def lj_fluid(n: int = 4096, density: float = 0.8, jitter: float = 0.05,
                       single_molecule=True, dt=dt, gamma=np.full(n, gamma), seed=seed)
 
 
-def _random_walk_chains(rng, nchains, nbeads, bond, min_dist, radius, max_tries=200):
+def _random_walk_chains(nchains, nbeads, bond, min_dist, radius, seed):
     """Random-walk chains with `bond`-long steps from seed-drawn directions,
-    rejecting any bead closer than `min_dist` to an existing bead other than
-    the one it is bonded to, or outside the sphere of `radius` (grid hash of
-    `min_dist` cells)."""
-    cell = min_dist
-    grid = {}
+    rejecting any bead closer than `min_dist` to a bead other than the one it
+    is bonded to, or outside the sphere of `radius` (native builder)."""
+    from . import _capi as A
     out = np.empty((nchains * nbeads, 3))
-    k = 0
-
-    def ok(p, skip=-1):
-        if p @ p > radius * radius:
-            return False
-        c = np.floor(p / cell).astype(np.int64)
-        for dx in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dz in (-1, 0, 1):
-                    for q in grid.get((c[0] + dx, c[1] + dy, c[2] + dz), ()):
-                        if q == skip:
-                            continue
-                        d = p - out[q]
-                        if d @ d < min_dist * min_dist:
-                            return False
-        return True
-
-    def add(p):
-        nonlocal k
-        out[k] = p
-        c = np.floor(p / cell).astype(np.int64)
-        grid.setdefault((c[0], c[1], c[2]), []).append(k)
-        k += 1
-
-    for _c in range(nchains):
-        while True:
-            u = rng.uniform(-1, 1, 3) * radius
-            if ok(u):
-                add(u)
-                break
-        for _b in range(1, nbeads):
-            prev = out[k - 1]
-            for _t in range(max_tries):
-                d = rng.standard_normal(3)
-                p = prev + bond * d / np.linalg.norm(d)
-                if ok(p, k - 1):
-                    add(p)
-                    break
-            else:
-                raise RuntimeError("random walk got stuck; lower the density")
+    code = A.lib().mjg_synth_polymer_chains(nchains, nbeads, bond, min_dist, radius,
+                                            int(seed) & ((1 << 64) - 1), A.f64(out))
+    if code != 0:
+        raise RuntimeError(f"mjg_synth_polymer_chains failed ({code}); lower the density")
     return out
 
 
@@ -167,7 +129,7 @@ def polymer_melt(nchains: int = 50, nbeads: int = 200, radius: float = 300.0,
     v0=0), ExcludedVolume (radius 2, eps 0.2, cutoff 2), DebyeHuckel on a
     random `charged_fraction` of beads with charges +-1 and zero net charge."""
     rng = np.random.default_rng(seed)
-    pos = _random_walk_chains(rng, nchains, nbeads, 3.8, 4.0, radius)
+    pos = _random_walk_chains(nchains, nbeads, 3.8, 4.0, radius, seed)
     n = pos.shape[0]
     m = np.full(n, mass)
     vel = maxwell_boltzmann(rng, m, KB_KCAL * temperature)
@@ -205,15 +167,13 @@ def bead_fluid(n: int = 1 << 20, density: float = 0.003, charged_fraction: float
     """Periodic EXV + Debye-Hueckel bead fluid: cubic box at number density
     `density`, uniform positions with overlaps below `min_dist` redrawn, charges
     +-1 on `charged_fraction` of the beads with zero net charge."""
+    from . import _capi as A
     rng = np.random.default_rng(seed)
     L = (n / density) ** (1.0 / 3.0)
-    pos = rng.uniform(0.0, L, size=(n, 3))
-    # redraw overlapping beads until none is closer than min_dist (grid check)
-    for _ in range(64):
-        bad = _overlaps_periodic(pos, L, min_dist)
-        if bad.size == 0:
-            break
-        pos[bad] = rng.uniform(0.0, L, size=(bad.size, 3))
+    pos = np.empty((n, 3))
+    code = A.lib().mjg_synth_uniform_fluid(n, L, min_dist, int(seed) & ((1 << 64) - 1), A.f64(pos))
+    if code != 0:
+        raise RuntimeError(f"mjg_synth_uniform_fluid failed ({code})")
     m = np.full(n, mass)
     vel = maxwell_boltzmann(rng, m, KB_KCAL * temperature)
     nch = int(round(charged_fraction * n)) // 2 * 2
@@ -230,28 +190,23 @@ def bead_fluid(n: int = 1 << 20, density: float = 0.003, charged_fraction: float
         single_molecule=True, dt=dt, gamma=np.full(n, gamma), seed=seed)
 
 
-def _overlaps_periodic(pos: np.ndarray, L: float, dmin: float) -> np.ndarray:
-    """Indices of the higher-indexed bead of every pair closer than dmin."""
-    nc = max(1, int(L // dmin))
-    w = L / nc
-    c = np.floor(pos / w).astype(np.int64) % nc
-    key = (c[:, 0] * nc + c[:, 1]) * nc + c[:, 2]
-    order = np.argsort(key, kind="stable")
-    skey = key[order]
-    starts = np.searchsorted(skey, np.arange(nc ** 3))
-    ends = np.searchsorted(skey, np.arange(nc ** 3), side="right")
-    bad = set()
-    for dx in (-1, 0, 1):
-        for dy in (-1, 0, 1):
-            for dz in (-1, 0, 1):
-                nb = ((((c[:, 0] + dx) % nc) * nc + (c[:, 1] + dy) % nc) * nc + (c[:, 2] + dz) % nc)
-                cnt = ends[nb] - starts[nb]
-                mx = cnt.max() if cnt.size else 0
-                for r in range(mx):
-                    sel = np.nonzero(cnt > r)[0]
-                    j = order[starts[nb[sel]] + r]
-                    d = pos[j] - pos[sel]
-                    d -= L * np.round(d / L)
-                    close = (np.einsum("ij,ij->i", d, d) < dmin * dmin) & (j > sel)
-                    bad.update(j[close].tolist())
-    return np.array(sorted(bad), dtype=np.int64)
+def polymer_batch(nsys: int = 256, nmin: int = 500, nmax: int = 20000, seed: int = 4,
+                  beads_per_chain: int = 200, dt: float = 0.01, gamma: float = 1.0,
+                  margin: float = 0.5):
+    """Independent polymer melts built like :func:`polymer_melt`, sizes drawn
+    log-uniform in [nmin, nmax] (chains of ~200 beads; the sphere radius keeps
+    the 10,000-beads-in-300-A density), temperature U[280, 360] K and ionic
+    strength U[0.05, 0.3] M per system."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsys))
+    temps = rng.uniform(280.0, 360.0, nsys)
+    ions = rng.uniform(0.05, 0.3, nsys)
+    out = []
+    for k in range(nsys):
+        nchains = max(1, int(round(sizes[k] / beads_per_chain)))
+        nbeads = max(4, int(round(sizes[k] / nchains)))
+        radius = 300.0 * (nchains * nbeads / 10000.0) ** (1.0 / 3.0)
+        out.append(polymer_melt(nchains=nchains, nbeads=nbeads, radius=radius,
+                                temperature=float(temps[k]), ionic_strength=float(ions[k]),
+                                dt=dt, gamma=gamma, margin=margin, seed=seed * 100003 + k))
+    return out
