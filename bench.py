@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--nsys", type=int, default=NSYS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     return ap.parse_args()
 
 
@@ -242,6 +243,10 @@ def run_b200(args, ws, rank, local, pg):
         eng.add_system(d)
     eng.commit()
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
+    tuned = None
+    if not args.no_tune:
+        from mjolnir_b200 import autotune
+        tuned = autotune.tune(eng, log=lambda m: print(m, file=sys.stderr))
 
     # ---- device-resident throughput
     for _ in range(args.warmup):
@@ -353,7 +358,8 @@ def run_b200(args, ws, rank, local, pg):
             "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 pair math, f64 state, i64 fixed-point forces",
             "data": "synthetic",
-            "config": workload_config(descs, precision="mixed", chunk=CHUNK),
+            "config": {**workload_config(descs, precision="mixed", chunk=CHUNK),
+                       "autotuned": tuned},
             "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,

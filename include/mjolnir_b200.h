@@ -199,6 +199,16 @@ MJG_API int mjg_context_get_stream(mjg_context* ctx, void** stream);
  * back-to-back launches on the current lists, timed with CUDA events on the
  * context's stream; the integrator's forces are not touched. */
 MJG_API int mjg_time_kernel(mjg_context* ctx, int term, int reps, double* ms_per_launch);
+/* Performance knobs of a global term (they change no result in the mixed
+ * form, whose force sums are exact and order independent):
+ * threads cooperating on one particle's list in the pair kernel (1, 2, 4, 8
+ * or 16; re-lays out and rebuilds the lists), and the relative Verlet margin
+ * of every system that has the term (re-commits: new cell grids, new lists,
+ * state kept).  The reference fixes the margin in its input
+ * (input/read_spatial_partition.hpp:62-76). */
+MJG_API int mjg_set_threads_per_particle(mjg_context* ctx, int term, int tpp);
+MJG_API int mjg_get_threads_per_particle(mjg_context* ctx, int term, int* tpp);
+MJG_API int mjg_set_margin(mjg_context* ctx, int term, double margin);
 /* Sets the per-particle neighbour capacity of a global term's lists.  A
  * capacity below what a later rebuild needs is detected on the device, the
  * current mjg_step chunk is rolled back, the lists grow and the chunk runs

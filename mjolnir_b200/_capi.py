@@ -64,6 +64,9 @@ SIGNATURES = {
     "mjg_set_list_capacity": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "mjg_context_get_stream": (C.c_int, [_ctx, C.POINTER(C.c_void_p)]),
     "mjg_time_kernel": (C.c_int, [_ctx, C.c_int, C.c_int, _f64p]),
+    "mjg_set_threads_per_particle": (C.c_int, [_ctx, C.c_int, C.c_int]),
+    "mjg_get_threads_per_particle": (C.c_int, [_ctx, C.c_int, C.POINTER(C.c_int)]),
+    "mjg_set_margin": (C.c_int, [_ctx, C.c_int, C.c_double]),
 }
 
 # include/mjolnir_b200_synthetic.h (host-only builders)

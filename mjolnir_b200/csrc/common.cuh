@@ -138,6 +138,14 @@ __device__ __forceinline__ void gaussian3(unsigned long long seed, unsigned long
     g2 = r1 * c3;
 }
 
+// Blocked column-major list layout: partner k of slot s.  With tpp threads per
+// slot, the tpp lanes of a group read tpp consecutive words, and consecutive
+// groups read consecutive blocks; tpp = 1 is plain column-major.
+__host__ __device__ __forceinline__ long long nbr_index(long long k, long long s, long long np, int tpp)
+{
+    return ((k / tpp) * np + s) * tpp + (k % tpp);
+}
+
 // Cell coordinate of x along one axis (PeriodicGridCellList::calc_index for a
 // periodic system; a wrapped hash of the unbounded grid otherwise).
 __device__ __forceinline__ int cell_coord(double x, const GlobalParams& g, int axis)

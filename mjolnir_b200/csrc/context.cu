@@ -101,11 +101,12 @@ struct HostSystem {
 
 struct TermDev {
     DevBuf part_particle, part_p0, part_p1, part_lead, part_sys, part_cell;
-    DevBuf cell_count, cell_start, cell_fill, block_sums;
+    DevBuf cell_count, cell_start, cell_fill, work, part_chunks, cell_chunks, flagged;
     DevBuf slot_part, slot_particle, slot_lead, slot_sys, slot_pd, slot_p1;
     DevBuf nnb, nbr, max_count, any_rebuild;
     DevBuf ex_start, ex_idx;
     int cap_alloc = 0;           // capacity the nbr buffer was sized for
+    bool tpp_fixed = false;      // threads per slot chosen by the caller
     TermArrays t{};
 };
 
@@ -136,9 +137,11 @@ struct mjg_context {
     mjg::LocalArrays local{};
     std::vector<mjg::SysDev> h_sys;
 
-    cudaGraph_t graph = nullptr;
+    cudaGraph_t graph = nullptr;            // first step of a chunk
     cudaGraphExec_t graph_exec = nullptr;
-    long long graph_nodes = 0;
+    cudaGraph_t graph2 = nullptr;           // later steps: closing kick fused in
+    cudaGraphExec_t graph2_exec = nullptr;
+    long long graph_nodes = 0, graph2_nodes = 0;
     bool graph_dirty = true;
 };
 
@@ -159,7 +162,7 @@ int64_t device_bytes(const mjg_context* c)
     {
         const DevBuf* tb[] = {&t.part_particle, &t.part_p0, &t.part_p1, &t.part_lead, &t.part_sys,
                               &t.part_cell, &t.cell_count, &t.cell_start, &t.cell_fill,
-                              &t.block_sums, &t.slot_part, &t.slot_particle, &t.slot_lead,
+                              &t.work, &t.part_chunks, &t.cell_chunks, &t.flagged, &t.slot_part, &t.slot_particle, &t.slot_lead,
                               &t.slot_sys, &t.slot_pd, &t.slot_p1, &t.nnb, &t.nbr, &t.max_count,
                               &t.any_rebuild, &t.ex_start, &t.ex_idx};
         for(auto* x : tb) {b += (int64_t)x->bytes;}
@@ -194,6 +197,8 @@ void release_graph(mjg_context* c)
 {
     if(c->graph_exec) {cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr;}
     if(c->graph) {cudaGraphDestroy(c->graph); c->graph = nullptr;}
+    if(c->graph2_exec) {cudaGraphExecDestroy(c->graph2_exec); c->graph2_exec = nullptr;}
+    if(c->graph2) {cudaGraphDestroy(c->graph2); c->graph2 = nullptr;}
     c->graph_dirty = true;
 }
 
@@ -205,30 +210,37 @@ void enqueue_forces(mjg_context* c, const Arena& a, bool nf, bool ne)
     for(int g = 0; g < NGLOBAL; ++g) {launch_pair(a, g, c->term[g].t, nf, ne, 0, c->stream);}
 }
 
-void enqueue_step(mjg_context* c)
+// One integrator step without its closing half-kick.  kick: open with the
+// previous step's closing half-kick (fused into the same pass).
+void enqueue_step_body(mjg_context* c, bool kick)
 {
     const Arena& a = c->arena;
     TermArrays ts[NGLOBAL] = {c->term[0].t, c->term[1].t, c->term[2].t};
-    launch_integrate_first(a, c->stream);
+    launch_integrate_first(a, c->stream, kick);
     launch_margin(a, ts, c->stream);
     for(int g = 0; g < NGLOBAL; ++g) {launch_rebuild(a, g, c->term[g].t, 0, c->stream);}
     enqueue_forces(c, a, true, false);
-    launch_integrate_last(a, c->stream);
+}
+
+
+void capture_one(mjg_context* c, bool kick, cudaGraph_t& g, cudaGraphExec_t& ge, long long& nodes)
+{
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step_body(c, kick);
+    g = nullptr;
+    CK(cudaStreamEndCapture(c->stream, &g));
+    CK(cudaGraphInstantiate(&ge, g, 0));
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    nodes = (long long)nn;
 }
 
 void capture_graph(mjg_context* c)
 {
     release_graph(c);
     const long long before = g_launches.load();
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(c);
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamEndCapture(c->stream, &g));
-    c->graph = g;
-    CK(cudaGraphInstantiate(&c->graph_exec, g, 0));
-    size_t nn = 0;
-    CK(cudaGraphGetNodes(g, nullptr, &nn));
-    c->graph_nodes = (long long)nn;
+    capture_one(c, false, c->graph, c->graph_exec, c->graph_nodes);
+    capture_one(c, true, c->graph2, c->graph2_exec, c->graph2_nodes);
     // capture counted the launches once; graph replays add them per replay
     g_launches.fetch_sub(g_launches.load() - before);
     c->graph_dirty = false;
@@ -254,7 +266,19 @@ void upload_sys(mjg_context* c)
     }
 }
 
-int list_capacity(int max_count) {return max_count + max_count / 4 + 16;}
+// room for growth; a multiple of 16 so that every threads-per-slot choice
+// tiles the blocked layout
+int list_capacity(int max_count) {return ((max_count + max_count / 4 + 16) + 15) / 16 * 16;}
+
+// threads per slot of the pair kernel from the longest list (refined by the
+// autotuner through mjg_set_threads_per_particle)
+int default_tpp(int max_count)
+{
+    if(max_count >= 192) {return 8;}
+    if(max_count >= 48)  {return 4;}
+    if(max_count >= 12)  {return 2;}
+    return 1;
+}
 
 // (re)allocates the neighbour arrays of term g for capacity cap
 void alloc_lists(mjg_context* c, int g, int cap)
@@ -282,6 +306,7 @@ void rebuild_all(mjg_context* c)
             CK(cudaMemcpyAsync(&mx, T.t.max_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
             if(mx <= T.t.cap) {break;}
+            if(!T.tpp_fixed) {T.t.tpp = default_tpp(mx);}
             alloc_lists(c, g, list_capacity(mx));
         }
     }
@@ -365,7 +390,8 @@ void commit(mjg_context* c)
     for(int g = 0; g < NGLOBAL; ++g) {ex_start[g].push_back(0);}
 
     // per term participant data
-    std::vector<int> part_particle[NGLOBAL], part_sys[NGLOBAL], cell_sys[NGLOBAL];
+    std::vector<int> part_particle[NGLOBAL], part_sys[NGLOBAL];
+    long long part_chunk_cap[NGLOBAL] = {0, 0, 0}, cell_chunk_cap[NGLOBAL] = {0, 0, 0};
     std::vector<double> part_p0[NGLOBAL], part_p1[NGLOBAL];
     std::vector<unsigned char> part_lead[NGLOBAL];
     int ncell[NGLOBAL] = {0, 0, 0};
@@ -560,7 +586,8 @@ void commit(mjg_context* c)
             G.ncell = G.dims[0] * G.dims[1] * G.dims[2];
             G.cell_off = ncell[g];
             ncell[g] += G.ncell;
-            for(int q = 0; q < G.ncell; ++q) {cell_sys[g].push_back(k);}
+            cell_chunk_cap[g] += (G.ncell + 255) / 256;
+            part_chunk_cap[g] += (np + 255) / 256;
             G.slot_off = (int)part_particle[g].size();
             G.nslot = (int)np;
             for(int64_t q = 0; q < np; ++q)
@@ -653,7 +680,7 @@ void commit(mjg_context* c)
         {
             DevBuf* bufs[] = {&T.part_particle, &T.part_p0, &T.part_p1, &T.part_lead, &T.part_sys,
                               &T.part_cell, &T.cell_count, &T.cell_start, &T.cell_fill,
-                              &T.block_sums, &T.slot_part, &T.slot_particle, &T.slot_lead,
+                              &T.work, &T.part_chunks, &T.cell_chunks, &T.flagged, &T.slot_part, &T.slot_particle, &T.slot_lead,
                               &T.slot_sys, &T.slot_pd, &T.slot_p1, &T.nnb, &T.nbr,
                               &T.max_count, &T.any_rebuild};
             for(auto* b : bufs) {b->release();}
@@ -668,11 +695,18 @@ void commit(mjg_context* c)
         T.cell_count.alloc(sizeof(int) * t.ncell);
         T.cell_fill.alloc(sizeof(int) * t.ncell);
         T.cell_start.alloc(sizeof(int) * (t.ncell + 1));
-        const int nblocks = (t.ncell + 2047) / 2048;
-        // block sums, one spare word, then the cell -> system map
-        std::vector<int> bs(nblocks + 1, 0);
-        bs.insert(bs.end(), cell_sys[g].begin(), cell_sys[g].end());
-        upload(T.block_sums, bs, st);
+        // rebuild work lists (sized for every system flagged at once)
+        T.work.alloc(sizeof(int) * 4);
+        CK(cudaMemsetAsync(T.work.p, 0, T.work.bytes, st));
+        T.part_chunks.alloc(sizeof(int4) * std::max<long long>(1, part_chunk_cap[g]));
+        T.cell_chunks.alloc(sizeof(int4) * std::max<long long>(1, cell_chunk_cap[g]));
+        T.flagged.alloc(sizeof(int) * std::max(1, nsys));
+        {
+            std::vector<int> last(1, (int)np);   // cell_start[ncell] = total slots
+            CK(cudaMemcpyAsync(T.cell_start.as<int>() + t.ncell, last.data(), sizeof(int),
+                               cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
         CK(cudaMemsetAsync(T.cell_count.p, 0, T.cell_count.bytes, st));
         CK(cudaMemsetAsync(T.cell_fill.p, 0, T.cell_fill.bytes, st));
         T.slot_part.alloc(sizeof(int) * np);
@@ -695,7 +729,10 @@ void commit(mjg_context* c)
         t.cell_count = T.cell_count.as<int>();
         t.cell_start = T.cell_start.as<int>();
         t.cell_fill = T.cell_fill.as<int>();
-        t.block_sums = T.block_sums.as<int>();
+        t.work = T.work.as<int>();
+        t.part_chunks = T.part_chunks.as<int4>();
+        t.cell_chunks = T.cell_chunks.as<int4>();
+        t.flagged = T.flagged.as<int>();
         t.slot_part = T.slot_part.as<int>();
         t.slot_particle = T.slot_particle.as<int>();
         t.slot_lead = T.slot_lead.as<unsigned char>();
@@ -706,6 +743,7 @@ void commit(mjg_context* c)
         t.max_count = T.max_count.as<int>();
         t.any_rebuild = T.any_rebuild.as<int>();
         t.cap = 0;
+        t.tpp = 1;
         T.nbr.release();
         t.nbr = nullptr;
         alloc_lists(c, g, 0);
@@ -751,10 +789,13 @@ void commit(mjg_context* c)
 void check_status(mjg_context* c, bool& overflow)
 {
     overflow = false;
+    // a truncated list makes every later force of the chunk meaningless, so
+    // a list overflow is handled (rolled back) before anything else is judged
+    for(const auto& d : c->h_sys) {if(d.status & ST_LIST_OVERFLOW) {overflow = true;}}
+    if(overflow) {return;}
     for(size_t k = 0; k < c->h_sys.size(); ++k)
     {
         const int st = c->h_sys[k].status;
-        if(st & ST_LIST_OVERFLOW) {overflow = true;}
         if(st & ST_FIXED_OVERFLOW)
         {
             throw Error(MJG_EOVERFLOW, "system " + std::to_string(c->arena_ids[k]) +
@@ -781,16 +822,21 @@ void run_steps(mjg_context* c, int64_t nsteps)
             CK(cudaMemcpyAsync(c->b_vel.p, c->d_vel.p, c->d_vel.bytes, cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(c->b_force.p, c->d_force.p, c->d_force.bytes, cudaMemcpyDeviceToDevice, st));
         }
+        // step 1 of the chunk, then steps 2..n with the previous closing
+        // half-kick fused into their first pass, then the last closing kick
         if(c->graphs)
         {
             if(c->graph_dirty || !c->graph_exec) {capture_graph(c);}
-            for(int64_t k = 0; k < nsteps; ++k) {CK(cudaGraphLaunch(c->graph_exec, st));}
-            note_launches((int)std::min<long long>(c->graph_nodes * nsteps, (1ll << 30)));
+            CK(cudaGraphLaunch(c->graph_exec, st));
+            for(int64_t k = 1; k < nsteps; ++k) {CK(cudaGraphLaunch(c->graph2_exec, st));}
+            note_launches((int)std::min<long long>(c->graph_nodes + c->graph2_nodes * (nsteps - 1),
+                                                   (1ll << 30)));
         }
         else
         {
-            for(int64_t k = 0; k < nsteps; ++k) {enqueue_step(c);}
+            for(int64_t k = 0; k < nsteps; ++k) {enqueue_step_body(c, k > 0);}
         }
+        launch_integrate_last(c->arena, st);
         CK(cudaGetLastError());
         download_sys(c);
         bool overflow = false;
@@ -861,7 +907,7 @@ void mjg_context_destroy(mjg_context* c)
     for(auto& t : c->term)
     {
         DevBuf* bufs[] = {&t.part_particle, &t.part_p0, &t.part_p1, &t.part_lead, &t.part_sys,
-                          &t.part_cell, &t.cell_count, &t.cell_start, &t.cell_fill, &t.block_sums,
+                          &t.part_cell, &t.cell_count, &t.cell_start, &t.cell_fill, &t.work, &t.part_chunks, &t.cell_chunks, &t.flagged,
                           &t.slot_part, &t.slot_particle, &t.slot_lead, &t.slot_sys, &t.slot_pd,
                           &t.slot_p1, &t.nnb, &t.nbr, &t.max_count, &t.any_rebuild, &t.ex_start,
                           &t.ex_idx};
@@ -1279,18 +1325,18 @@ int mjg_neighbors(mjg_context* c, int sys, int term, int64_t* pairs, int64_t cap
     std::vector<int> nnb(t.np), part(t.np);
     CK(cudaMemcpy(nnb.data(), t.nnb, sizeof(int) * t.np, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(part.data(), t.slot_particle, sizeof(int) * t.np, cudaMemcpyDeviceToHost));
-    std::vector<int> col(t.np);
-    std::vector<std::pair<int64_t, int64_t>> out;
-    for(int k = 0; k < t.cap; ++k)
+    std::vector<int> all((size_t)t.cap * (size_t)t.np);
+    if(!all.empty())
     {
-        bool any = false;
-        for(int q = so; q < so + ns; ++q) {if(nnb[q] > k) {any = true; break;}}
-        if(!any) {break;}
-        CK(cudaMemcpy(col.data(), t.nbr + (size_t)k * t.np, sizeof(int) * t.np, cudaMemcpyDeviceToHost));
-        for(int q = so; q < so + ns; ++q)
+        CK(cudaMemcpy(all.data(), t.nbr, sizeof(int) * all.size(), cudaMemcpyDeviceToHost));
+    }
+    std::vector<std::pair<int64_t, int64_t>> out;
+    for(int q = so; q < so + ns; ++q)
+    {
+        for(int k = 0; k < nnb[q]; ++k)
         {
-            if(nnb[q] <= k) {continue;}
-            const int64_t i = part[q] - s.off, j = part[col[q]] - s.off;
+            const int r = all[(size_t)nbr_index(k, q, t.np, t.tpp)];
+            const int64_t i = part[q] - s.off, j = part[r] - s.off;
             if(i < j) {out.emplace_back(i, j);}
         }
     }
@@ -1373,6 +1419,45 @@ int mjg_time_kernel(mjg_context* c, int term, int reps, double* ms)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *ms = (double)t / reps;
+    ABI_END(c)
+}
+
+int mjg_set_threads_per_particle(mjg_context* c, int term, int tpp)
+{
+    ABI_BEGIN(c)
+    if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "threads per slot apply to global terms");}
+    if(tpp != 1 && tpp != 2 && tpp != 4 && tpp != 8 && tpp != 16) {throw Error(MJG_EINVAL, "tpp must be 1, 2, 4, 8 or 16");}
+    TermDev& T = c->term[term - MJG_TERM_EXV];
+    if(!T.t.on) {throw Error(MJG_EINVAL, "term not present");}
+    T.tpp_fixed = true;
+    if(T.t.tpp != tpp)
+    {
+        T.t.tpp = tpp;          // the layout changes: rebuild every list
+        release_graph(c);
+        rebuild_all(c);
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    ABI_END(c)
+}
+
+int mjg_get_threads_per_particle(mjg_context* c, int term, int* tpp)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !tpp) {throw Error(MJG_EINVAL, "bad query");}
+    *tpp = c->term[term - MJG_TERM_EXV].t.tpp;
+    ABI_END(c)
+}
+
+int mjg_set_margin(mjg_context* c, int term, double margin)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !(margin >= 0)) {throw Error(MJG_EINVAL, "bad margin");}
+    for(auto& s : c->sys)
+    {
+        if(s.alive && s.g[term - MJG_TERM_EXV].on) {s.g[term - MJG_TERM_EXV].margin = margin;}
+    }
+    if(c->committed) {commit(c);}   // new cell grids and lists; the state is kept
     ABI_END(c)
 }
 

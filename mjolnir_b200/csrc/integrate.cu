@@ -37,8 +37,10 @@ __device__ __forceinline__ void zero_force(void* force, long long i)
 }
 
 // B-A-O-A of BAOAB (or the first half-kick and drift of velocity Verlet),
-// force reset and the per-system largest squared displacement.
-template<int PREC>
+// force reset and the per-system largest squared displacement.  With KICK the
+// previous step's closing half-kick v += (halfdt/m) f is applied first, as a
+// separate rounding step, so that consecutive steps of a chunk share one pass.
+template<int PREC, bool KICK>
 __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
 {
     const long long i = (long long)blockIdx.x * TPB + threadIdx.x;
@@ -53,6 +55,12 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
         const double4 c = a.coef[i];     // {halfdt*rmass, exp(-gamma dt), noise, halfdt | dt}
         double fx, fy, fz;
         load_force<PREC>(a.force, i, fx, fy, fz);
+        if(KICK)
+        {
+            v.x = __dadd_rn(v.x, __dmul_rn(c.x, fx));
+            v.y = __dadd_rn(v.y, __dmul_rn(c.x, fy));
+            v.z = __dadd_rn(v.z, __dmul_rn(c.x, fz));
+        }
         double dx, dy, dz;
         if(S.integrator == I_BAOAB)
         {
@@ -217,11 +225,19 @@ inline unsigned blocks(long long n) {return (unsigned)((n + TPB - 1) / TPB);}
 
 }  // namespace
 
-void launch_integrate_first(const Arena& a, cudaStream_t s)
+void launch_integrate_first(const Arena& a, cudaStream_t s, bool kick)
 {
     if(a.n == 0) {return;}
-    if(a.precision == P_FP64) {k_integrate_first<P_FP64><<<blocks(a.n), TPB, 0, s>>>(a);}
-    else                      {k_integrate_first<P_MIXED><<<blocks(a.n), TPB, 0, s>>>(a);}
+    if(a.precision == P_FP64)
+    {
+        if(kick) {k_integrate_first<P_FP64, true ><<<blocks(a.n), TPB, 0, s>>>(a);}
+        else     {k_integrate_first<P_FP64, false><<<blocks(a.n), TPB, 0, s>>>(a);}
+    }
+    else
+    {
+        if(kick) {k_integrate_first<P_MIXED, true ><<<blocks(a.n), TPB, 0, s>>>(a);}
+        else     {k_integrate_first<P_MIXED, false><<<blocks(a.n), TPB, 0, s>>>(a);}
+    }
     note_launches(1);
 }
 

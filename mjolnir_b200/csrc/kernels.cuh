@@ -29,7 +29,8 @@ struct TermArrays {
     int        on;
     long long  np;              // participants (= slots)
     int        ncell;           // total cells over all systems
-    int        cap;             // neighbour capacity per slot
+    int        cap;             // neighbour capacity per slot (a multiple of tpp)
+    int        tpp;             // threads per slot of the pair kernel (1, 2, 4, 8, 16)
     const int* part_particle;   // [np] global particle index
     const double* part_p0;      // [np] radius / charge / sigma
     const double* part_p1;      // [np] LJ epsilon
@@ -39,7 +40,10 @@ struct TermArrays {
     int*       cell_count;      // [ncell]
     int*       cell_start;      // [ncell + 1]
     int*       cell_fill;       // [ncell]
-    int*       block_sums;      // scan scratch
+    int*       work;            // [3] rebuild work counters
+    int4*      part_chunks;     // rebuild work: participant chunks {sys, begin, end}
+    int4*      cell_chunks;     // rebuild work: cell chunks
+    int*       flagged;         // [nsys] systems rebuilding this step
     int*       slot_part;       // [np] participant of slot (cell order)
     int*       slot_particle;   // [np] global particle of slot
     unsigned char* slot_lead;   // [np]
@@ -58,7 +62,8 @@ void launch_unpack_state(const Arena& a, const double* src_pos, const double* sr
 void launch_pack_state(const Arena& a, double* dst, int what, long long first, long long count,
                        cudaStream_t s);
 
-void launch_integrate_first(const Arena& a, cudaStream_t s);
+// kick: apply the previous step's closing half-kick in the same pass
+void launch_integrate_first(const Arena& a, cudaStream_t s, bool kick = false);
 void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s);
 void launch_integrate_last(const Arena& a, cudaStream_t s);
 void launch_zero_force(const Arena& a, cudaStream_t s);

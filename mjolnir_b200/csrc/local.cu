@@ -4,9 +4,10 @@
 //   BondAngle  + Harmonic   forcefield/local/BondAngleInteraction.hpp:129-188
 //   Dihedral   + Cosine     forcefield/local/DihedralAngleInteraction.hpp:157-227,
 //                           forcefield/local/CosinePotential.hpp:29-39
-// One thread per bond / angle / dihedral of every system; the forces land in
-// the particles by atomics (FP64 atomics in the plain form, int64 fixed point
-// in the mixed form, where the sum is exact and order independent).
+// One fused launch: one thread per bond / angle / dihedral of every system;
+// the forces are summed per block in shared memory and land in the particles
+// by atomics (FP64 atomics in the plain form, int64 fixed point in the mixed
+// form, where the sum is exact and order independent).
 #include "kernels.cuh"
 
 namespace mjg {
@@ -15,22 +16,80 @@ namespace {
 
 constexpr int TPB = 256;
 
+// Forces of one block of consecutive terms are summed in shared memory over a
+// window of WINDOW particles starting at the block's smallest particle index
+// (consecutive bonds, angles and dihedrals of a chain touch a narrow index
+// range), then added to global memory once per particle; a particle outside
+// the window goes to global memory directly.
+constexpr int WINDOW = 1024;
+
+template<int PREC> struct WinT;
+template<> struct WinT<P_FP64>  {using type = double;};
+template<> struct WinT<P_MIXED> {using type = unsigned long long;};
+
 template<int PREC>
-__device__ __forceinline__ void add_force(void* force, int i, double fx, double fy, double fz)
-{
-    if(PREC == P_FP64)
+struct Window {
+    using T = typename WinT<PREC>::type;
+    T* w;         // [3 * WINDOW] in shared memory
+    int base;
+    __device__ __forceinline__ void add(void* force, int i, double fx, double fy, double fz)
     {
-        double* f = reinterpret_cast<double*>(static_cast<double4*>(force) + i);
-        atomicAdd(f + 0, fx); atomicAdd(f + 1, fy); atomicAdd(f + 2, fz);
+        const int k = i - base;
+        if(k >= 0 && k < WINDOW)
+        {
+            if(PREC == P_FP64)
+            {
+                atomicAdd(reinterpret_cast<double*>(w) + 3 * k + 0, fx);
+                atomicAdd(reinterpret_cast<double*>(w) + 3 * k + 1, fy);
+                atomicAdd(reinterpret_cast<double*>(w) + 3 * k + 2, fz);
+            }
+            else
+            {
+                atomicAdd(reinterpret_cast<unsigned long long*>(w) + 3 * k + 0, (unsigned long long)fx_from_double(fx));
+                atomicAdd(reinterpret_cast<unsigned long long*>(w) + 3 * k + 1, (unsigned long long)fx_from_double(fy));
+                atomicAdd(reinterpret_cast<unsigned long long*>(w) + 3 * k + 2, (unsigned long long)fx_from_double(fz));
+            }
+            return;
+        }
+        global_add(force, i, fx, fy, fz);
     }
-    else
+    __device__ __forceinline__ static void global_add(void* force, int i, double fx, double fy, double fz)
     {
-        unsigned long long* f = reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(force) + i);
-        atomicAdd(f + 0, (unsigned long long)fx_from_double(fx));
-        atomicAdd(f + 1, (unsigned long long)fx_from_double(fy));
-        atomicAdd(f + 2, (unsigned long long)fx_from_double(fz));
+        if(PREC == P_FP64)
+        {
+            double* f = reinterpret_cast<double*>(static_cast<double4*>(force) + i);
+            atomicAdd(f + 0, fx); atomicAdd(f + 1, fy); atomicAdd(f + 2, fz);
+        }
+        else
+        {
+            unsigned long long* f = reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(force) + i);
+            atomicAdd(f + 0, (unsigned long long)fx_from_double(fx));
+            atomicAdd(f + 1, (unsigned long long)fx_from_double(fy));
+            atomicAdd(f + 2, (unsigned long long)fx_from_double(fz));
+        }
     }
-}
+    __device__ __forceinline__ void flush(void* force, long long n) const
+    {
+        for(int k = threadIdx.x; k < WINDOW; k += blockDim.x)
+        {
+            const long long i = (long long)base + k;
+            if(i >= n) {break;}
+            const T x = w[3 * k], y = w[3 * k + 1], z = w[3 * k + 2];
+            if(x == T(0) && y == T(0) && z == T(0)) {continue;}
+            if(PREC == P_FP64)
+            {
+                double* f = reinterpret_cast<double*>(static_cast<double4*>(force) + i);
+                atomicAdd(f + 0, (double)x); atomicAdd(f + 1, (double)y); atomicAdd(f + 2, (double)z);
+            }
+            else
+            {
+                unsigned long long* f = reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(force) + i);
+                atomicAdd(f + 0, (unsigned long long)x); atomicAdd(f + 1, (unsigned long long)y);
+                atomicAdd(f + 2, (unsigned long long)z);
+            }
+        }
+    }
+};
 
 __device__ __forceinline__ double3 direction(const SysDev& S, const double4& from, const double4& to)
 {
@@ -68,9 +127,8 @@ __device__ __forceinline__ void reduce_energy(Arena& a, int sys, bool active, do
 }
 
 template<int PREC, bool NF, bool NE>
-__global__ void __launch_bounds__(TPB) k_bonds(Arena a, LocalArrays l)
+__device__ __forceinline__ void do_bond(Arena& a, const LocalArrays& l, long long b, Window<PREC>& W)
 {
-    const long long b = (long long)blockIdx.x * TPB + threadIdx.x;
     const bool active = b < l.nbond;
     const int sys = active ? l.bond_sys[b] : 0;
     double e = 0.0;
@@ -88,17 +146,16 @@ __global__ void __launch_bounds__(TPB) k_bonds(Arena a, LocalArrays l)
         if(NF)
         {
             const double c = -(2 * k * dv) * rlen;
-            add_force<PREC>(a.force, i0, -d.x * c, -d.y * c, -d.z * c);
-            add_force<PREC>(a.force, i1,  d.x * c,  d.y * c,  d.z * c);
+            W.add(a.force, i0, -d.x * c, -d.y * c, -d.z * c);
+            W.add(a.force, i1,  d.x * c,  d.y * c,  d.z * c);
         }
     }
     if(NE) {reduce_energy(a, sys, active, e, T_BOND);}
 }
 
 template<int PREC, bool NF, bool NE>
-__global__ void __launch_bounds__(TPB) k_angles(Arena a, LocalArrays l)
+__device__ __forceinline__ void do_angle(Arena& a, const LocalArrays& l, long long b, Window<PREC>& W)
 {
-    const long long b = (long long)blockIdx.x * TPB + threadIdx.x;
     const bool active = b < l.nangle;
     const int sys = active ? l.angle_sys[b] : 0;
     double e = 0.0;
@@ -126,18 +183,17 @@ __global__ void __launch_bounds__(TPB) k_angles(Arena a, LocalArrays l)
             const double ci = cis * inv_ij, ck = cis * inv_kj;
             const double3 Fi = make_double3(ci * (cos_t * eij.x - ekj.x), ci * (cos_t * eij.y - ekj.y), ci * (cos_t * eij.z - ekj.z));
             const double3 Fk = make_double3(ck * (cos_t * ekj.x - eij.x), ck * (cos_t * ekj.y - eij.y), ck * (cos_t * ekj.z - eij.z));
-            add_force<PREC>(a.force, i0, Fi.x, Fi.y, Fi.z);
-            add_force<PREC>(a.force, i1, -Fi.x - Fk.x, -Fi.y - Fk.y, -Fi.z - Fk.z);
-            add_force<PREC>(a.force, i2, Fk.x, Fk.y, Fk.z);
+            W.add(a.force, i0, Fi.x, Fi.y, Fi.z);
+            W.add(a.force, i1, -Fi.x - Fk.x, -Fi.y - Fk.y, -Fi.z - Fk.z);
+            W.add(a.force, i2, Fk.x, Fk.y, Fk.z);
         }
     }
     if(NE) {reduce_energy(a, sys, active, e, T_ANGLE);}
 }
 
 template<int PREC, bool NF, bool NE>
-__global__ void __launch_bounds__(TPB) k_dihedrals(Arena a, LocalArrays l)
+__device__ __forceinline__ void do_dihedral(Arena& a, const LocalArrays& l, long long b, Window<PREC>& W)
 {
-    const long long b = (long long)blockIdx.x * TPB + threadIdx.x;
     const bool active = b < l.ndihd;
     const int sys = active ? l.dihd_sys[b] : 0;
     double e = 0.0;
@@ -174,23 +230,77 @@ __global__ void __launch_bounds__(TPB) k_dihedrals(Arena a, LocalArrays l)
             const double3 Fl = make_double3(cfl * n.x, cfl * n.y, cfl * n.z);
             const double cijk = dot(r_ij, r_kj) * r_kj_rlensq;
             const double cjkl = dot(r_kl, r_kj) * r_kj_rlensq;
-            add_force<PREC>(a.force, i0, Fi.x, Fi.y, Fi.z);
-            add_force<PREC>(a.force, i1, (cijk - 1.0) * Fi.x - cjkl * Fl.x, (cijk - 1.0) * Fi.y - cjkl * Fl.y,
+            W.add(a.force, i0, Fi.x, Fi.y, Fi.z);
+            W.add(a.force, i1, (cijk - 1.0) * Fi.x - cjkl * Fl.x, (cijk - 1.0) * Fi.y - cjkl * Fl.y,
                             (cijk - 1.0) * Fi.z - cjkl * Fl.z);
-            add_force<PREC>(a.force, i2, (cjkl - 1.0) * Fl.x - cijk * Fi.x, (cjkl - 1.0) * Fl.y - cijk * Fi.y,
+            W.add(a.force, i2, (cjkl - 1.0) * Fl.x - cijk * Fi.x, (cjkl - 1.0) * Fl.y - cijk * Fi.y,
                             (cjkl - 1.0) * Fl.z - cijk * Fi.z);
-            add_force<PREC>(a.force, i3, Fl.x, Fl.y, Fl.z);
+            W.add(a.force, i3, Fl.x, Fl.y, Fl.z);
         }
     }
     if(NE) {reduce_energy(a, sys, active, e, T_DIHEDRAL);}
 }
 
+// smallest particle index touched by the block's terms
+template<int ARITY>
+__device__ __forceinline__ int block_base(const int* idx, long long first, long long count, int* sh)
+{
+    if(threadIdx.x == 0) {*sh = 0x7fffffff;}
+    __syncthreads();
+    const long long b = first + threadIdx.x;
+    if(b < count)
+    {
+        int m = idx[ARITY * b];
+#pragma unroll
+        for(int x = 1; x < ARITY; ++x) {m = min(m, idx[ARITY * b + x]);}
+        atomicMin(sh, m);
+    }
+    __syncthreads();
+    return *sh;
+}
+
+// blocks [0, nbb) bonds, [nbb, nbb + nba) angles, then dihedrals
+template<int PREC, bool NF, bool NE>
+__global__ void __launch_bounds__(TPB) k_local(Arena a, LocalArrays l, int nbb, int nba)
+{
+    __shared__ typename WinT<PREC>::type win[3 * WINDOW];
+    __shared__ int sh_base;
+    Window<PREC> W{win, 0};
+    int blk = blockIdx.x, kind = 0;
+    if(blk >= nbb) {blk -= nbb; kind = 1; if(blk >= nba) {blk -= nba; kind = 2;}}
+    const long long first = (long long)blk * TPB;
+    if(NF)
+    {
+        W.base = kind == 0 ? block_base<2>(l.bond_idx, first, l.nbond, &sh_base)
+               : kind == 1 ? block_base<3>(l.angle_idx, first, l.nangle, &sh_base)
+                           : block_base<4>(l.dihd_idx, first, l.ndihd, &sh_base);
+        for(int k = threadIdx.x; k < 3 * WINDOW; k += TPB) {win[k] = 0;}
+        __syncthreads();
+    }
+    const long long b = first + threadIdx.x;
+    if(kind == 0)      {do_bond    <PREC, NF, NE>(a, l, b, W);}
+    else if(kind == 1) {do_angle   <PREC, NF, NE>(a, l, b, W);}
+    else               {do_dihedral<PREC, NF, NE>(a, l, b, W);}
+    if(NF)
+    {
+        __syncthreads();
+        W.flush(a.force, a.n);
+    }
+}
+
 template<int PREC, bool NF, bool NE>
 void run_all(const Arena& a, const LocalArrays& l, int mask, cudaStream_t s)
 {
-    if((mask & 1) && l.nbond  > 0) {k_bonds    <PREC, NF, NE><<<(unsigned)((l.nbond  + TPB - 1) / TPB), TPB, 0, s>>>(a, l); note_launches(1);}
-    if((mask & 2) && l.nangle > 0) {k_angles   <PREC, NF, NE><<<(unsigned)((l.nangle + TPB - 1) / TPB), TPB, 0, s>>>(a, l); note_launches(1);}
-    if((mask & 4) && l.ndihd  > 0) {k_dihedrals<PREC, NF, NE><<<(unsigned)((l.ndihd  + TPB - 1) / TPB), TPB, 0, s>>>(a, l); note_launches(1);}
+    LocalArrays m = l;
+    if(!(mask & 1)) {m.nbond = 0;}
+    if(!(mask & 2)) {m.nangle = 0;}
+    if(!(mask & 4)) {m.ndihd = 0;}
+    const int nbb = (int)((m.nbond + TPB - 1) / TPB);
+    const int nba = (int)((m.nangle + TPB - 1) / TPB);
+    const int nbd = (int)((m.ndihd + TPB - 1) / TPB);
+    if(nbb + nba + nbd == 0) {return;}
+    k_local<PREC, NF, NE><<<nbb + nba + nbd, TPB, 0, s>>>(a, m, nbb, nba);
+    note_launches(1);
 }
 
 }  // namespace

@@ -23,7 +23,7 @@ namespace mjg {
 
 namespace {
 
-constexpr int TPB = 128;
+constexpr int TPB = 256;
 
 __global__ void k_gather(Arena a, TermArrays t)
 {
@@ -44,6 +44,12 @@ template<> struct Acc<P_FP64>
     {
         x = fma(dx, c, x); y = fma(dy, c, y); z = fma(dz, c, z);
     }
+    __device__ __forceinline__ void shfl_add(int o)
+    {
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+        y += __shfl_xor_sync(0xffffffffu, y, o);
+        z += __shfl_xor_sync(0xffffffffu, z, o);
+    }
     __device__ __forceinline__ void store(void* force, long long i) const
     {
         double4* f = static_cast<double4*>(force) + i;
@@ -63,6 +69,12 @@ template<> struct Acc<P_MIXED>
         ovf |= !(m < FX_LIMIT * FX_INV_SCALE);
         x += fx_from_double(fx); y += fx_from_double(fy); z += fx_from_double(fz);
     }
+    __device__ __forceinline__ void shfl_add(int o)
+    {
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+        y += __shfl_xor_sync(0xffffffffu, y, o);
+        z += __shfl_xor_sync(0xffffffffu, z, o);
+    }
     __device__ __forceinline__ void store(void* force, long long i) const
     {
         longlong4* f = static_cast<longlong4*>(force) + i;
@@ -72,14 +84,19 @@ template<> struct Acc<P_MIXED>
     }
 };
 
-template<int PREC, int G, bool NF, bool NE>
+template<int PREC, int G, bool NF, bool NE, int TPP>
 __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
 {
-    const long long s = (long long)blockIdx.x * TPB + threadIdx.x;
+    // TPP consecutive threads share one slot; lane lg walks partners lg,
+    // lg + TPP, ... which the blocked list layout stores next to each other
+    const long long gt = (long long)blockIdx.x * TPB + threadIdx.x;
+    const long long s = gt / TPP;
+    const int lg = (int)(threadIdx.x % TPP);
     const bool active = s < t.np;
     const int sys = active ? t.slot_sys[s] : 0;
     double energy = 0.0;
     bool ovf = false;
+    Acc<PREC> acc;
     if(active)
     {
         const SysDev& S = a.sys[sys];
@@ -90,7 +107,6 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
         const double4 pi = t.slot_pd[s];
         const long long np = t.np;
         const int n = t.nnb[s];
-        Acc<PREC> acc;
 
         // potential constants
         const double crsq  = P.cutoff_ratio_sq;
@@ -103,11 +119,13 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
         const double epsi  = (G == G_LJ) ? t.slot_p1[s] : 0.0;
         const float  eps12f = (float)eps12, epsf = (float)eps, coefcf = (float)coefc;
         const float  debf = (float)debye, invdf = (float)inv_debye;
+        const int* __restrict__ nbr = t.nbr + s * TPP + lg;
+        const double4* __restrict__ pd = t.slot_pd;
 
-        for(int k = 0; k < n; ++k)
+        for(int k = lg; k < n; k += TPP)
         {
-            const int q = t.nbr[(long long)k * np + s];
-            const double4 pj = t.slot_pd[q];
+            const int q = __ldg(nbr + (long long)(k / TPP) * np * TPP);
+            const double4 pj = pd[q];
             double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
             if(periodic)
             {
@@ -188,9 +206,12 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
                 }
             }
         }
-        if(NF) {acc.store(a.force, t.slot_particle[s]);}
-        if(ovf) {atomicOr(&a.sys[sys].status, ST_FIXED_OVERFLOW);}
     }
+    // group reduction: exact in fixed point, fixed order in FP64
+#pragma unroll
+    for(int o = TPP / 2; o > 0; o >>= 1) {acc.shfl_add(o);}
+    if(active && NF && lg == 0) {acc.store(a.force, t.slot_particle[s]);}
+    if(ovf) {atomicOr(&a.sys[sys].status, ST_FIXED_OVERFLOW);}
     if(NE)
     {
         const unsigned full = 0xffffffffu;
@@ -224,7 +245,7 @@ __global__ void k_count_cut(Arena a, TermArrays t, int sys_filter, unsigned long
         const int n = t.nnb[s];
         for(int k = 0; k < n; ++k)
         {
-            const int q = t.nbr[(long long)k * t.np + s];
+            const int q = t.nbr[nbr_index(k, s, t.np, t.tpp)];
             if(q <= s) {continue;}
             const double4 pj = t.slot_pd[q];
             double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
@@ -247,13 +268,26 @@ __global__ void k_count_cut(Arena a, TermArrays t, int sys_filter, unsigned long
     if((threadIdx.x & 31) == 0 && cnt) {atomicAdd(out, cnt);}
 }
 
+template<int PREC, int G, int TPP>
+void dispatch_tpp(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
+{
+    const unsigned nb = (unsigned)((t.np * TPP + TPB - 1) / TPB);
+    if(nf && ne)  {k_pair<PREC, G, true,  true,  TPP><<<nb, TPB, 0, s>>>(a, t);}
+    else if(nf)   {k_pair<PREC, G, true,  false, TPP><<<nb, TPB, 0, s>>>(a, t);}
+    else if(ne)   {k_pair<PREC, G, false, true,  TPP><<<nb, TPB, 0, s>>>(a, t);}
+}
+
 template<int PREC, int G>
 void dispatch(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
 {
-    const unsigned nb = (unsigned)((t.np + TPB - 1) / TPB);
-    if(nf && ne)  {k_pair<PREC, G, true,  true ><<<nb, TPB, 0, s>>>(a, t);}
-    else if(nf)   {k_pair<PREC, G, true,  false><<<nb, TPB, 0, s>>>(a, t);}
-    else if(ne)   {k_pair<PREC, G, false, true ><<<nb, TPB, 0, s>>>(a, t);}
+    switch(t.tpp)
+    {
+        case 1:  dispatch_tpp<PREC, G, 1 >(a, t, nf, ne, s); break;
+        case 2:  dispatch_tpp<PREC, G, 2 >(a, t, nf, ne, s); break;
+        case 4:  dispatch_tpp<PREC, G, 4 >(a, t, nf, ne, s); break;
+        case 8:  dispatch_tpp<PREC, G, 8 >(a, t, nf, ne, s); break;
+        default: dispatch_tpp<PREC, G, 16>(a, t, nf, ne, s); break;
+    }
 }
 
 }  // namespace

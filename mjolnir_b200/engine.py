@@ -219,6 +219,22 @@ class Engine:
         self._c(self.lib.mjg_time_kernel(self.ctx, t, int(reps), C.byref(ms)))
         return ms.value
 
+    def set_threads_per_particle(self, term, tpp: int):
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        self._c(self.lib.mjg_set_threads_per_particle(self.ctx, t, int(tpp)))
+
+    def get_threads_per_particle(self, term) -> int:
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        v = C.c_int()
+        self._c(self.lib.mjg_get_threads_per_particle(self.ctx, t, C.byref(v)))
+        if v.value == 0:
+            raise A.MjgError(A.EINVAL, f"term {term} not present")
+        return v.value
+
+    def set_margin(self, term, margin: float):
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        self._c(self.lib.mjg_set_margin(self.ctx, t, float(margin)))
+
     def launch_count(self) -> int:
         c = C.c_int64()
         self._c(self.lib.mjg_launch_count(self.ctx, C.byref(c)))
