@@ -309,10 +309,12 @@ def run_b200(args, ws, rank, local, pg):
                       "gbs": bytes_alg / (ms * 1e-3) / 1e9}
     dom = max(kern, key=lambda k: kern[k]["ms"])
     k = kern[dom]
+    local_ms = {t: eng.time_kernel(t, reps=20) for t in ("bond", "angle", "dihedral")}
     roofline = {"bound": "hbm", "kernel": f"k_pair<{dom}> (+ its slot gather)", "achieved": k["gbs"],
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": k["gbs"] / peak,
                 "traffic": None, "ms_per_launch": k["ms"], "pairs_in_cutoff": k["pcut"],
-                "algorithmic_bytes": k["bytes"], "other": {t: kern[t] for t in kern if t != dom}}
+                "algorithmic_bytes": k["bytes"], "other": {t: kern[t] for t in kern if t != dom},
+                "local_ms_per_launch": local_ms}
 
     # ---- plain single-system FP64 path on a sample of the same systems
     plain = None

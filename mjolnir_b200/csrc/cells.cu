@@ -2,14 +2,19 @@
 //
 // Replaces PeriodicGridCellList::make / UnlimitedGridCellList::make
 // (core/PeriodicGridCellList.hpp:198-351, core/UnlimitedGridCellList.hpp
-// :152-255) for every system of the arena that reduce_margin flagged:
+// :152-255) for every system of the arena that reduce_margin flagged.  A
+// planning kernel turns the flagged systems into a work list of 256-item
+// chunks (participants and cells); every later kernel is a persistent grid
+// that walks only those chunks, so a step in which 5 of 256 systems rebuild
+// costs 5 systems' worth of work:
 //   1. zero the flagged systems' cell counters,
 //   2. bin their participants (one atomic increment per participant),
-//   3. exclusive scan over all cells of the term (3-phase, 2048 cells/block),
+//   3. exclusive scan of each flagged system's cells (one block per system),
 //   4. scatter participants into cell order, sort each cell by participant,
 //   5. renumber: slot = position in cell order (spatially coherent slots),
-//   6. build each slot's partner list from the 27 neighbouring cells with the
-//      reference's membership test, evaluated in FP64 without contraction:
+//   6. build each slot's partner list from the 27 neighbouring cells (one
+//      warp per slot) with the reference's membership test, evaluated in FP64
+//      without contraction:
 //      has_interaction (i < j of a leading participant, not excluded) and
 //      |adjust_direction(r_i, r_j)|^2 < (cutoff (1 + margin))^2.
 // The lists hold both directions of every pair (full lists); a pair (a, b) is
@@ -167,7 +172,7 @@ __global__ void __launch_bounds__(TPB) k_cells_sort(TermArrays t, const int* slo
     }
 }
 
-__global__ void __launch_bounds__(TPB) k_slots_setup(TermArrays t)
+__global__ void __launch_bounds__(TPB) k_slots_setup(Arena a, TermArrays t)
 {
     const int n = t.work[0];
     for(int c = blockIdx.x; c < n; c += gridDim.x)
@@ -176,10 +181,12 @@ __global__ void __launch_bounds__(TPB) k_slots_setup(TermArrays t)
         const int s = w.y + threadIdx.x;
         if(s >= w.z) {continue;}
         const int p = t.slot_part[s];
-        t.slot_particle[s] = t.part_particle[p];
+        const int i = t.part_particle[p];
+        const double4 r = a.pos[i];
+        t.slot_particle[s] = i;
         t.slot_lead[s]     = t.part_lead[p];
         t.slot_sys[s]      = w.x;
-        t.slot_pd[s].w     = t.part_p0[p];
+        t.slot_pd[s]       = make_double4(r.x, r.y, r.z, t.part_p0[p]);
         if(t.part_p1) {t.slot_p1[s] = t.part_p1[p];}
     }
 }
@@ -198,72 +205,121 @@ __device__ __forceinline__ bool is_excluded(const Arena& a, int g, int ignore_mo
     return false;
 }
 
+// One warp per slot.  The 27 stencil cells (in the reference's order: z, y, x
+// from -1 to +1) are flattened into one candidate sequence that the 32 lanes
+// walk together; the distance test reads the cell-ordered slot coordinates
+// (consecutive candidates are consecutive in memory), the topology checks run
+// only for candidates inside the list radius, and an ordered ballot
+// compaction keeps the output order identical to a serial walk.
 __global__ void __launch_bounds__(TPB) k_build_list(Arena a, int g, TermArrays t)
 {
     const int n = t.work[0];
     const int cap = t.cap;
     const long long np = t.np;
-    for(int c = blockIdx.x; c < n; c += gridDim.x)
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    // every warp of the grid takes the next (chunk, slot) pair, so that all
+    // warps have work even when only a few systems rebuild
+    const long long nwork = (long long)n * CHUNK;
+    const long long wstride = (long long)gridDim.x * (TPB / 32);
+    for(long long gw = (long long)blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); gw < nwork; gw += wstride)
     {
-        const int4 w = t.part_chunks[c];
-        const int s = w.y + threadIdx.x;
+        const int4 w = t.part_chunks[gw / CHUNK];
+        const int s = w.y + (int)(gw % CHUNK);
         if(s >= w.z) {continue;}
         const int sys = w.x;
         const SysDev& S = a.sys[sys];
         const GlobalParams& G = S.g[g];
-        const int i = t.slot_particle[s];
-        const bool lead_i = t.slot_lead[s] != 0;
-        const double4 ri = a.pos[i];
-        const int cx = cell_coord(ri.x, G, 0);
-        const int cy = cell_coord(ri.y, G, 1);
-        const int cz = cell_coord(ri.z, G, 2);
         const bool periodic = S.boundary == B_PERIODIC;
         const int dx_ = G.dims[0], dy_ = G.dims[1], dz_ = G.dims[2];
         const bool wrap = periodic || G.hashed;
-        int count = 0;
-
-        for(int oz = -1; oz <= 1; ++oz)
-        for(int oy = -1; oy <= 1; ++oy)
-        for(int ox = -1; ox <= 1; ++ox)
+        const double rl2 = G.rl2;
         {
-            int x = cx + ox, y = cy + oy, z = cz + oz;
-            if(wrap)
+            const int i = t.slot_particle[s];
+            const bool lead_i = t.slot_lead[s] != 0;
+            const double4 ri = t.slot_pd[s];
+            const int cx = cell_coord(ri.x, G, 0);
+            const int cy = cell_coord(ri.y, G, 1);
+            const int cz = cell_coord(ri.z, G, 2);
+            // this lane's stencil cell
+            int cstart = 0, ccount = 0;
+            if(lane < 27)
             {
-                x = x < 0 ? x + dx_ : (x >= dx_ ? x - dx_ : x);
-                y = y < 0 ? y + dy_ : (y >= dy_ ? y - dy_ : y);
-                z = z < 0 ? z + dz_ : (z >= dz_ ? z - dz_ : z);
+                int x = cx + lane % 3 - 1, y = cy + (lane / 3) % 3 - 1, z = cz + lane / 9 - 1;
+                bool inside = true;
+                if(wrap)
+                {
+                    x = x < 0 ? x + dx_ : (x >= dx_ ? x - dx_ : x);
+                    y = y < 0 ? y + dy_ : (y >= dy_ ? y - dy_ : y);
+                    z = z < 0 ? z + dz_ : (z >= dz_ ? z - dz_ : z);
+                }
+                else if(x < 0 || y < 0 || z < 0 || x >= dx_ || y >= dy_ || z >= dz_) {inside = false;}
+                if(inside)
+                {
+                    const int cell = G.cell_off + x + dx_ * (y + dy_ * z);
+                    cstart = t.cell_start[cell];
+                    ccount = t.cell_count[cell];
+                }
             }
-            else if(x < 0 || y < 0 || z < 0 || x >= dx_ || y >= dy_ || z >= dz_) {continue;}
-            const int cell = G.cell_off + x + dx_ * (y + dy_ * z);
-            const int b = t.cell_start[cell], e = b + t.cell_count[cell];
-            for(int q = b; q < e; ++q)
+            int incl = ccount;
+#pragma unroll
+            for(int o = 1; o < 32; o <<= 1)
             {
-                const int j = t.slot_particle[q];
-                if(j == i) {continue;}
-                const bool lead_lo = (i < j) ? lead_i : (t.slot_lead[q] != 0);
-                if(!lead_lo) {continue;}
-                if(is_excluded(a, g, G.ignore_mol, i < j ? i : j, i < j ? j : i)) {continue;}
-                const double4 rj = a.pos[j];
-                double ddx = __dsub_rn(rj.x, ri.x);
-                double ddy = __dsub_rn(rj.y, ri.y);
-                double ddz = __dsub_rn(rj.z, ri.z);
-                if(periodic)
+                const int y = __shfl_up_sync(full, incl, o);
+                if(lane >= o) {incl += y;}
+            }
+            const int excl = incl - ccount;
+            const int total = __shfl_sync(full, incl, 31);
+            int count = 0;
+            for(int base = 0; base < total; base += 32)
+            {
+                const int k = base + lane;
+                // cell of candidate k: the last stencil lane whose range starts at or before k
+                int L = 0;
+#pragma unroll
+                for(int b = 16; b > 0; b >>= 1)
                 {
-                    ddx = min_image(ddx, S.halfw[0], S.width[0]);
-                    ddy = min_image(ddy, S.halfw[1], S.width[1]);
-                    ddz = min_image(ddz, S.halfw[2], S.width[2]);
+                    const int cand = L + b;
+                    const int e = __shfl_sync(full, excl, cand < 32 ? cand : 31);
+                    if(cand < 27 && e <= k) {L = cand;}
                 }
-                const double l2 = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
-                if(l2 < G.rl2)
+                const int q = __shfl_sync(full, cstart, L) + (k - __shfl_sync(full, excl, L));
+                bool keep = false;
+                if(k < total && q != s)
                 {
-                    if(count < cap) {t.nbr[nbr_index(count, s, np, t.tpp)] = q;}
-                    ++count;
+                    const double4 rj = t.slot_pd[q];
+                    double ddx = __dsub_rn(rj.x, ri.x);
+                    double ddy = __dsub_rn(rj.y, ri.y);
+                    double ddz = __dsub_rn(rj.z, ri.z);
+                    if(periodic)
+                    {
+                        ddx = min_image(ddx, S.halfw[0], S.width[0]);
+                        ddy = min_image(ddy, S.halfw[1], S.width[1]);
+                        ddz = min_image(ddz, S.halfw[2], S.width[2]);
+                    }
+                    const double l2 = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
+                    if(l2 < rl2)
+                    {
+                        const int j = t.slot_particle[q];
+                        const bool lead_lo = (i < j) ? lead_i : (t.slot_lead[q] != 0);
+                        keep = lead_lo && !is_excluded(a, g, G.ignore_mol, i < j ? i : j, i < j ? j : i);
+                    }
                 }
+                const unsigned m = __ballot_sync(full, keep);
+                if(keep)
+                {
+                    const int pos = count + __popc(m & ((1u << lane) - 1u));
+                    if(pos < cap) {t.nbr[nbr_index(pos, s, np, t.tpp)] = q;}
+                }
+                count += __popc(m);
+            }
+            if(lane == 0)
+            {
+                t.nnb[s] = count < cap ? count : cap;
+                atomicMax(t.max_count, count);
+                if(count > cap) {atomicOr(&a.sys[sys].status, ST_LIST_OVERFLOW);}
             }
         }
-        t.nnb[s] = count < cap ? count : cap;
-        atomicMax(t.max_count, count);
-        if(count > cap) {atomicOr(&a.sys[sys].status, ST_LIST_OVERFLOW);}
     }
 }
 
@@ -296,7 +352,7 @@ void launch_rebuild(const Arena& a, int g, TermArrays& t, int force_all, cudaStr
     k_scan_sys    <<<min(a.nsys, 1024), SCAN_TPB, 0, s>>>(a, g, t);
     k_cells_scatter<<<GRID, TPB, 0, s>>>(t, t.slot_particle);
     k_cells_sort  <<<GRID, TPB, 0, s>>>(t, t.slot_particle);
-    k_slots_setup <<<GRID, TPB, 0, s>>>(t);
+    k_slots_setup <<<GRID, TPB, 0, s>>>(a, t);
     k_build_list  <<<GRID, TPB, 0, s>>>(a, g, t);
     k_rebuild_done<<<blocks(a.nsys, 128), 128, 0, s>>>(a, g, t, force_all);
     note_launches(9);

@@ -107,6 +107,7 @@ struct TermDev {
     DevBuf ex_start, ex_idx;
     int cap_alloc = 0;           // capacity the nbr buffer was sized for
     bool tpp_fixed = false;      // threads per slot chosen by the caller
+    int tpp_choice = 1;          // ... and its value (kept across commits)
     TermArrays t{};
 };
 
@@ -133,6 +134,7 @@ struct mjg_context {
     mjg::DevBuf l_bond_idx, l_bond_k, l_bond_v0, l_bond_sys;
     mjg::DevBuf l_angle_idx, l_angle_k, l_angle_v0, l_angle_sys;
     mjg::DevBuf l_dihd_idx, l_dihd_k, l_dihd_n, l_dihd_v0, l_dihd_sys;
+    mjg::DevBuf l_win_bond, l_win_angle, l_win_dihd, l_bond_kv, l_angle_kv, l_dihd_p;
     mjg::Arena arena{};
     mjg::LocalArrays local{};
     std::vector<mjg::SysDev> h_sys;
@@ -156,7 +158,8 @@ int64_t device_bytes(const mjg_context* c)
                             &c->d_force_scratch, &c->l_bond_idx, &c->l_bond_k, &c->l_bond_v0,
                             &c->l_bond_sys, &c->l_angle_idx, &c->l_angle_k, &c->l_angle_v0,
                             &c->l_angle_sys, &c->l_dihd_idx, &c->l_dihd_k, &c->l_dihd_n,
-                            &c->l_dihd_v0, &c->l_dihd_sys};
+                            &c->l_dihd_v0, &c->l_dihd_sys, &c->l_win_bond, &c->l_win_angle,
+                            &c->l_win_dihd, &c->l_bond_kv, &c->l_angle_kv, &c->l_dihd_p};
     for(auto* x : bufs) {b += (int64_t)x->bytes;}
     for(const auto& t : c->term)
     {
@@ -567,7 +570,7 @@ void commit(mjg_context* c)
                     const double ext = np > 0 ? hi[x] - lo[x] : 0.0;
                     dims[x] = std::max<long long>(3, (long long)std::floor(ext / w) + 3);
                 }
-                const long long limit = std::max<long long>(27, 4 * np + 64);
+                const long long limit = std::max<long long>(27, 2 * np + 64);
                 while(dims[0] * dims[1] * dims[2] > limit)
                 {
                     int big = 0;
@@ -743,13 +746,69 @@ void commit(mjg_context* c)
         t.max_count = T.max_count.as<int>();
         t.any_rebuild = T.any_rebuild.as<int>();
         t.cap = 0;
-        t.tpp = 1;
+        t.tpp = T.tpp_fixed ? T.tpp_choice : 1;
+        t.any_periodic = 0;
+        for(int id : ids)
+        {
+            if(c->sys[id].g[g].on && c->sys[id].boundary == B_PERIODIC) {t.any_periodic = 1;}
+        }
         T.nbr.release();
         t.nbr = nullptr;
         alloc_lists(c, g, 0);
     }
 
-    // local
+    // local: terms sorted by their smallest particle, CSR over 256-particle windows
+    const int nwin = (int)((n_tot + 255) / 256);
+    auto sort_terms = [&](std::vector<int>& idx, int arity, std::vector<double>& kk,
+                          std::vector<double>& v0, std::vector<int>& sysv, std::vector<int>* nn,
+                          std::vector<long long>& win) {
+        const size_t m = kk.size();
+        std::vector<int> key(m);
+        for(size_t t = 0; t < m; ++t)
+        {
+            int mn = idx[arity * t];
+            for(int x = 1; x < arity; ++x) {mn = std::min(mn, idx[arity * t + x]);}
+            key[t] = mn;
+        }
+        std::vector<size_t> perm(m);
+        for(size_t t = 0; t < m; ++t) {perm[t] = t;}
+        std::stable_sort(perm.begin(), perm.end(), [&](size_t x, size_t y) {return key[x] < key[y];});
+        std::vector<int> idx2(idx.size()), sys2(m), n2(nn ? m : 0);
+        std::vector<double> k2(m), v2(m);
+        for(size_t t = 0; t < m; ++t)
+        {
+            const size_t p = perm[t];
+            for(int x = 0; x < arity; ++x) {idx2[arity * t + x] = idx[arity * p + x];}
+            k2[t] = kk[p]; v2[t] = v0[p]; sys2[t] = sysv[p];
+            if(nn) {n2[t] = (*nn)[p];}
+        }
+        idx.swap(idx2); kk.swap(k2); v0.swap(v2); sysv.swap(sys2);
+        if(nn) {nn->swap(n2);}
+        win.assign((size_t)nwin + 1, 0);
+        for(size_t t = 0; t < m; ++t) {win[(size_t)key[perm[t]] / 256 + 1] += 1;}
+        for(int w = 0; w < nwin; ++w) {win[w + 1] += win[w];}
+    };
+    std::vector<long long> w_bond, w_angle, w_dihd;
+    sort_terms(b_idx, 2, b_k, b_v0, b_sys, nullptr, w_bond);
+    sort_terms(a_idx, 3, a_k, a_v0, a_sys, nullptr, w_angle);
+    sort_terms(d_idx, 4, d_k, d_v0, d_sys, &d_n, w_dihd);
+    {
+        std::vector<float2> bkv(b_k.size()), akv(a_k.size());
+        std::vector<float4> dp(d_k.size());
+        for(size_t t = 0; t < b_k.size(); ++t) {bkv[t] = make_float2((float)b_k[t], (float)b_v0[t]);}
+        for(size_t t = 0; t < a_k.size(); ++t) {akv[t] = make_float2((float)a_k[t], (float)a_v0[t]);}
+        for(size_t t = 0; t < d_k.size(); ++t)
+        {
+            const double nv = (double)d_n[t] * d_v0[t];
+            dp[t] = make_float4((float)d_k[t], (float)std::cos(nv), (float)std::sin(nv), (float)d_n[t]);
+        }
+        upload(c->l_bond_kv, bkv, st);
+        upload(c->l_angle_kv, akv, st);
+        upload(c->l_dihd_p, dp, st);
+    }
+    upload(c->l_win_bond, w_bond, st);
+    upload(c->l_win_angle, w_angle, st);
+    upload(c->l_win_dihd, w_dihd, st);
     upload(c->l_bond_idx, b_idx, st);  upload(c->l_bond_k, b_k, st);
     upload(c->l_bond_v0, b_v0, st);    upload(c->l_bond_sys, b_sys, st);
     upload(c->l_angle_idx, a_idx, st); upload(c->l_angle_k, a_k, st);
@@ -767,6 +826,13 @@ void commit(mjg_context* c)
     l.dihd_idx = c->l_dihd_idx.as<int>();   l.dihd_k = c->l_dihd_k.as<double>();
     l.dihd_n = c->l_dihd_n.as<int>();       l.dihd_v0 = c->l_dihd_v0.as<double>();
     l.dihd_sys = c->l_dihd_sys.as<int>();
+    l.nwin = nwin;
+    l.bond_kv = c->l_bond_kv.as<float2>();
+    l.angle_kv = c->l_angle_kv.as<float2>();
+    l.dihd_p = c->l_dihd_p.as<float4>();
+    l.win_bond = c->l_win_bond.as<long long>();
+    l.win_angle = c->l_win_angle.as<long long>();
+    l.win_dihd = c->l_win_dihd.as<long long>();
 
     c->committed = true;
     rebuild_all(c);
@@ -1431,6 +1497,7 @@ int mjg_set_threads_per_particle(mjg_context* c, int term, int tpp)
     TermDev& T = c->term[term - MJG_TERM_EXV];
     if(!T.t.on) {throw Error(MJG_EINVAL, "term not present");}
     T.tpp_fixed = true;
+    T.tpp_choice = tpp;
     if(T.t.tpp != tpp)
     {
         T.t.tpp = tpp;          // the layout changes: rebuild every list

@@ -31,6 +31,7 @@ struct TermArrays {
     int        ncell;           // total cells over all systems
     int        cap;             // neighbour capacity per slot (a multiple of tpp)
     int        tpp;             // threads per slot of the pair kernel (1, 2, 4, 8, 16)
+    int        any_periodic;    // some system with this term has a periodic box
     const int* part_particle;   // [np] global particle index
     const double* part_p0;      // [np] radius / charge / sigma
     const double* part_p1;      // [np] LJ epsilon
@@ -78,6 +79,16 @@ struct LocalArrays {
     const int* angle_idx;  const double* angle_k; const double* angle_v0; const int* angle_sys;
     const int* dihd_idx;   const double* dihd_k;  const int* dihd_n; const double* dihd_v0;
     const int* dihd_sys;
+    // float parameters of the mixed form: {k, v0}, {k, v0}, {k, cos(n v0), sin(n v0), n}
+    const float2* bond_kv;
+    const float2* angle_kv;
+    const float4* dihd_p;
+    // terms sorted by their smallest particle index; window w of 256 particles
+    // owns terms win_x[w] .. win_x[w + 1]
+    int nwin;
+    const long long* win_bond;
+    const long long* win_angle;
+    const long long* win_dihd;
 };
 void launch_local(const Arena& a, const LocalArrays& l, int which_mask, bool need_force,
                   bool need_energy, int calc_energy_form, cudaStream_t s);

@@ -1,4 +1,5 @@
-// Local (bonded) terms, FP64 in both precision modes:
+// Local (bonded) terms; the FP64 form keeps the reference's formulas, the
+// mixed form evaluates them in FP32 from FP64 displacements (see below):
 //   BondLength + Harmonic   forcefield/local/BondLengthInteraction.hpp:126-199,
 //                           forcefield/local/HarmonicPotential.hpp:25-35 (V = k (v - v0)^2)
 //   BondAngle  + Harmonic   forcefield/local/BondAngleInteraction.hpp:129-188
@@ -16,12 +17,14 @@ namespace {
 
 constexpr int TPB = 256;
 
-// Forces of one block of consecutive terms are summed in shared memory over a
-// window of WINDOW particles starting at the block's smallest particle index
-// (consecutive bonds, angles and dihedrals of a chain touch a narrow index
-// range), then added to global memory once per particle; a particle outside
-// the window goes to global memory directly.
-constexpr int WINDOW = 1024;
+// Forces of one block's terms are summed in shared memory over a window of
+// WINDOW particles starting at the block's first particle (bonds, angles and
+// dihedrals of a chain touch a narrow index range), then added to global
+// memory once per particle; a particle outside the window goes to global
+// memory directly.
+constexpr int SEG = 256;              // particles owned by one block (window start)
+constexpr int HALO = 64;              // terms may reach this far past the window
+constexpr int WINDOW = SEG + HALO;
 
 template<int PREC> struct WinT;
 template<> struct WinT<P_FP64>  {using type = double;};
@@ -127,9 +130,9 @@ __device__ __forceinline__ void reduce_energy(Arena& a, int sys, bool active, do
 }
 
 template<int PREC, bool NF, bool NE>
-__device__ __forceinline__ void do_bond(Arena& a, const LocalArrays& l, long long b, Window<PREC>& W)
+__device__ __forceinline__ void do_bond(Arena& a, const LocalArrays& l, long long b, bool active,
+                                         Window<PREC>& W)
 {
-    const bool active = b < l.nbond;
     const int sys = active ? l.bond_sys[b] : 0;
     double e = 0.0;
     if(active)
@@ -154,9 +157,9 @@ __device__ __forceinline__ void do_bond(Arena& a, const LocalArrays& l, long lon
 }
 
 template<int PREC, bool NF, bool NE>
-__device__ __forceinline__ void do_angle(Arena& a, const LocalArrays& l, long long b, Window<PREC>& W)
+__device__ __forceinline__ void do_angle(Arena& a, const LocalArrays& l, long long b, bool active,
+                                         Window<PREC>& W)
 {
-    const bool active = b < l.nangle;
     const int sys = active ? l.angle_sys[b] : 0;
     double e = 0.0;
     if(active)
@@ -192,9 +195,9 @@ __device__ __forceinline__ void do_angle(Arena& a, const LocalArrays& l, long lo
 }
 
 template<int PREC, bool NF, bool NE>
-__device__ __forceinline__ void do_dihedral(Arena& a, const LocalArrays& l, long long b, Window<PREC>& W)
+__device__ __forceinline__ void do_dihedral(Arena& a, const LocalArrays& l, long long b, bool active,
+                                         Window<PREC>& W)
 {
-    const bool active = b < l.ndihd;
     const int sys = active ? l.dihd_sys[b] : 0;
     double e = 0.0;
     if(active)
@@ -241,46 +244,201 @@ __device__ __forceinline__ void do_dihedral(Arena& a, const LocalArrays& l, long
     if(NE) {reduce_energy(a, sys, active, e, T_DIHEDRAL);}
 }
 
-// smallest particle index touched by the block's terms
-template<int ARITY>
-__device__ __forceinline__ int block_base(const int* idx, long long first, long long count, int* sh)
+// ----------------------------------------------------------- mixed form
+// The same terms in FP32 from FP64 displacements: bond stretch via
+// (r^2 - v0^2) / (r + v0) with r^2 - v0^2 in FP64, the angle from atan2 of the
+// cross and dot products, the dihedral from (cos phi, sin phi) of the normals
+// (phi = atan2(|r_kj| r_ij.n, m.n) has the reference's sign convention) and
+// cos / sin of n (phi - v0) by the multiple-angle recurrence, so no FP64
+// transcendental is evaluated.  Parameters come pre-packed as floats.
+
+__device__ __forceinline__ float3 fdir(const SysDev& S, const double4& from, const double4& to)
 {
-    if(threadIdx.x == 0) {*sh = 0x7fffffff;}
-    __syncthreads();
-    const long long b = first + threadIdx.x;
-    if(b < count)
-    {
-        int m = idx[ARITY * b];
-#pragma unroll
-        for(int x = 1; x < ARITY; ++x) {m = min(m, idx[ARITY * b + x]);}
-        atomicMin(sh, m);
-    }
-    __syncthreads();
-    return *sh;
+    const double3 d = direction(S, from, to);
+    return make_float3((float)d.x, (float)d.y, (float)d.z);
+}
+__device__ __forceinline__ float fdot(float3 a, float3 b) {return a.x * b.x + a.y * b.y + a.z * b.z;}
+__device__ __forceinline__ float3 fcross(float3 a, float3 b)
+{
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 
-// blocks [0, nbb) bonds, [nbb, nbb + nba) angles, then dihedrals
 template<int PREC, bool NF, bool NE>
-__global__ void __launch_bounds__(TPB) k_local(Arena a, LocalArrays l, int nbb, int nba)
+__device__ __forceinline__ void do_bond_f32(Arena& a, const LocalArrays& l, long long b, bool active,
+                                            Window<PREC>& W)
+{
+    const int sys = active ? l.bond_sys[b] : 0;
+    double e = 0.0;
+    if(active)
+    {
+        const SysDev& S = a.sys[sys];
+        const int i0 = l.bond_idx[2 * b], i1 = l.bond_idx[2 * b + 1];
+        const float2 kv = l.bond_kv[b];
+        const double3 d = direction(S, a.pos[i0], a.pos[i1]);
+        const double len2 = dot(d, d);
+        const float lenf = sqrtf((float)len2);
+        const float dv = (float)(len2 - (double)kv.y * (double)kv.y) / (lenf + kv.y);
+        if(NE) {e = (double)(kv.x * dv * dv);}
+        if(NF)
+        {
+            const double c = (double)(-(2.0f * kv.x * dv) / lenf);
+            W.add(a.force, i0, -d.x * c, -d.y * c, -d.z * c);
+            W.add(a.force, i1,  d.x * c,  d.y * c,  d.z * c);
+        }
+    }
+    if(NE) {reduce_energy(a, sys, active, e, T_BOND);}
+}
+
+template<int PREC, bool NF, bool NE>
+__device__ __forceinline__ void do_angle_f32(Arena& a, const LocalArrays& l, long long b, bool active,
+                                             Window<PREC>& W)
+{
+    const int sys = active ? l.angle_sys[b] : 0;
+    double e = 0.0;
+    if(active)
+    {
+        const SysDev& S = a.sys[sys];
+        const int i0 = l.angle_idx[3 * b], i1 = l.angle_idx[3 * b + 1], i2 = l.angle_idx[3 * b + 2];
+        const float2 kv = l.angle_kv[b];
+        const double4 p1 = a.pos[i1];
+        const float3 rij = fdir(S, p1, a.pos[i0]);
+        const float3 rkj = fdir(S, p1, a.pos[i2]);
+        const float inv_ij = rsqrtf(fdot(rij, rij));
+        const float inv_kj = rsqrtf(fdot(rkj, rkj));
+        const float3 eij = make_float3(rij.x * inv_ij, rij.y * inv_ij, rij.z * inv_ij);
+        const float3 ekj = make_float3(rkj.x * inv_kj, rkj.y * inv_kj, rkj.z * inv_kj);
+        const float3 cr = fcross(eij, ekj);
+        const float sin_t = sqrtf(fdot(cr, cr));
+        const float cos_t = fdot(eij, ekj);
+        const float theta = atan2f(sin_t, cos_t);
+        const float dv = theta - kv.y;
+        if(NE) {e = (double)(kv.x * dv * dv);}
+        if(NF)
+        {
+            const float cis = -(2.0f * kv.x * dv) / fmaxf(sin_t, 1e-8f);
+            const float ci = cis * inv_ij, ck = cis * inv_kj;
+            const float cc = fminf(fmaxf(cos_t, -1.0f), 1.0f);
+            const double3 Fi = make_double3(ci * (cc * eij.x - ekj.x), ci * (cc * eij.y - ekj.y), ci * (cc * eij.z - ekj.z));
+            const double3 Fk = make_double3(ck * (cc * ekj.x - eij.x), ck * (cc * ekj.y - eij.y), ck * (cc * ekj.z - eij.z));
+            W.add(a.force, i0, Fi.x, Fi.y, Fi.z);
+            W.add(a.force, i1, -Fi.x - Fk.x, -Fi.y - Fk.y, -Fi.z - Fk.z);
+            W.add(a.force, i2, Fk.x, Fk.y, Fk.z);
+        }
+    }
+    if(NE) {reduce_energy(a, sys, active, e, T_ANGLE);}
+}
+
+template<int PREC, bool NF, bool NE>
+__device__ __forceinline__ void do_dihedral_f32(Arena& a, const LocalArrays& l, long long b, bool active,
+                                                Window<PREC>& W)
+{
+    const int sys = active ? l.dihd_sys[b] : 0;
+    double e = 0.0;
+    if(active)
+    {
+        const SysDev& S = a.sys[sys];
+        const int i0 = l.dihd_idx[4 * b], i1 = l.dihd_idx[4 * b + 1];
+        const int i2 = l.dihd_idx[4 * b + 2], i3 = l.dihd_idx[4 * b + 3];
+        const float4 p = l.dihd_p[b];                 // {k, cos(n v0), sin(n v0), n}
+        const int nn = (int)p.w;
+        const double4 rj = a.pos[i1], rk = a.pos[i2];
+        const float3 r_ij = fdir(S, rj, a.pos[i0]);
+        const float3 r_kj = fdir(S, rj, rk);
+        const float3 r_lk = fdir(S, rk, a.pos[i3]);
+        const float3 r_kl = make_float3(-r_lk.x, -r_lk.y, -r_lk.z);
+        const float r_kj_lensq  = fdot(r_kj, r_kj);
+        const float r_kj_rlen   = rsqrtf(r_kj_lensq);
+        const float r_kj_len    = r_kj_rlen * r_kj_lensq;
+        const float3 m = fcross(r_ij, r_kj);
+        const float3 n = fcross(r_kj, r_kl);
+        const float m_lensq = fdot(m, m);
+        const float n_lensq = fdot(n, n);
+        // (cos phi, sin phi) of the reference's phi = copysign(acos(m.n), r_ij.n)
+        const float x = fdot(m, n);
+        const float y = r_kj_len * fdot(r_ij, n);
+        const float h = rsqrtf(x * x + y * y);
+        const float c1 = x * h, s1 = y * h;
+        float cn = 1.0f, sn = 0.0f;
+        const int na = nn < 0 ? -nn : nn;
+        for(int q = 0; q < na; ++q)
+        {
+            const float c2 = cn * c1 - sn * s1;
+            sn = sn * c1 + cn * s1;
+            cn = c2;
+        }
+        if(nn < 0) {sn = -sn;}
+        // cos, sin of n (phi - v0)
+        const float cd = cn * p.y + sn * p.z;
+        const float sd = sn * p.y - cn * p.z;
+        if(NE) {e = (double)(p.x * (1.0f + cd));}
+        if(NF)
+        {
+            const float coef = p.x * (float)nn * sd;     // -dV/dphi
+            const float cfi =  coef * r_kj_len / m_lensq;
+            const float cfl = -coef * r_kj_len / n_lensq;
+            const float3 Fi = make_float3(cfi * m.x, cfi * m.y, cfi * m.z);
+            const float3 Fl = make_float3(cfl * n.x, cfl * n.y, cfl * n.z);
+            const float rl2 = r_kj_rlen * r_kj_rlen;
+            const float cijk = fdot(r_ij, r_kj) * rl2;
+            const float cjkl = fdot(r_kl, r_kj) * rl2;
+            W.add(a.force, i0, Fi.x, Fi.y, Fi.z);
+            W.add(a.force, i1, (cijk - 1.0f) * Fi.x - cjkl * Fl.x, (cijk - 1.0f) * Fi.y - cjkl * Fl.y,
+                  (cijk - 1.0f) * Fi.z - cjkl * Fl.z);
+            W.add(a.force, i2, (cjkl - 1.0f) * Fl.x - cijk * Fi.x, (cjkl - 1.0f) * Fl.y - cijk * Fi.y,
+                  (cjkl - 1.0f) * Fl.z - cijk * Fi.z);
+            W.add(a.force, i3, Fl.x, Fl.y, Fl.z);
+        }
+    }
+    if(NE) {reduce_energy(a, sys, active, e, T_DIHEDRAL);}
+}
+
+// One block per window of SEG particles: every bond, angle and dihedral whose
+// smallest particle index falls in the window (terms are sorted by it at
+// commit; win_* hold the per-window term ranges) adds its forces to the
+// block's shared accumulator of SEG + HALO particles, which is flushed once
+// per particle.  The trip counts are uniform over the block, so the warp
+// energy reductions see whole warps.
+template<int PREC, bool NF, bool NE>
+__global__ void __launch_bounds__(TPB) k_local(Arena a, LocalArrays l, int mask)
 {
     __shared__ typename WinT<PREC>::type win[3 * WINDOW];
-    __shared__ int sh_base;
-    Window<PREC> W{win, 0};
-    int blk = blockIdx.x, kind = 0;
-    if(blk >= nbb) {blk -= nbb; kind = 1; if(blk >= nba) {blk -= nba; kind = 2;}}
-    const long long first = (long long)blk * TPB;
+    const int w = blockIdx.x;
+    Window<PREC> W{win, w * SEG};
     if(NF)
     {
-        W.base = kind == 0 ? block_base<2>(l.bond_idx, first, l.nbond, &sh_base)
-               : kind == 1 ? block_base<3>(l.angle_idx, first, l.nangle, &sh_base)
-                           : block_base<4>(l.dihd_idx, first, l.ndihd, &sh_base);
         for(int k = threadIdx.x; k < 3 * WINDOW; k += TPB) {win[k] = 0;}
         __syncthreads();
     }
-    const long long b = first + threadIdx.x;
-    if(kind == 0)      {do_bond    <PREC, NF, NE>(a, l, b, W);}
-    else if(kind == 1) {do_angle   <PREC, NF, NE>(a, l, b, W);}
-    else               {do_dihedral<PREC, NF, NE>(a, l, b, W);}
+    if(mask & 1)
+    {
+        const long long b0 = l.win_bond[w], b1 = l.win_bond[w + 1];
+        for(long long base = b0; base < b1; base += TPB)
+        {
+            const long long b = base + threadIdx.x;
+            if(PREC == P_FP64) {do_bond<PREC, NF, NE>(a, l, b, b < b1, W);}
+            else               {do_bond_f32<PREC, NF, NE>(a, l, b, b < b1, W);}
+        }
+    }
+    if(mask & 2)
+    {
+        const long long b0 = l.win_angle[w], b1 = l.win_angle[w + 1];
+        for(long long base = b0; base < b1; base += TPB)
+        {
+            const long long b = base + threadIdx.x;
+            if(PREC == P_FP64) {do_angle<PREC, NF, NE>(a, l, b, b < b1, W);}
+            else               {do_angle_f32<PREC, NF, NE>(a, l, b, b < b1, W);}
+        }
+    }
+    if(mask & 4)
+    {
+        const long long b0 = l.win_dihd[w], b1 = l.win_dihd[w + 1];
+        for(long long base = b0; base < b1; base += TPB)
+        {
+            const long long b = base + threadIdx.x;
+            if(PREC == P_FP64) {do_dihedral<PREC, NF, NE>(a, l, b, b < b1, W);}
+            else               {do_dihedral_f32<PREC, NF, NE>(a, l, b, b < b1, W);}
+        }
+    }
     if(NF)
     {
         __syncthreads();
@@ -291,15 +449,8 @@ __global__ void __launch_bounds__(TPB) k_local(Arena a, LocalArrays l, int nbb, 
 template<int PREC, bool NF, bool NE>
 void run_all(const Arena& a, const LocalArrays& l, int mask, cudaStream_t s)
 {
-    LocalArrays m = l;
-    if(!(mask & 1)) {m.nbond = 0;}
-    if(!(mask & 2)) {m.nangle = 0;}
-    if(!(mask & 4)) {m.ndihd = 0;}
-    const int nbb = (int)((m.nbond + TPB - 1) / TPB);
-    const int nba = (int)((m.nangle + TPB - 1) / TPB);
-    const int nbd = (int)((m.ndihd + TPB - 1) / TPB);
-    if(nbb + nba + nbd == 0) {return;}
-    k_local<PREC, NF, NE><<<nbb + nba + nbd, TPB, 0, s>>>(a, m, nbb, nba);
+    if(l.nwin == 0 || (l.nbond + l.nangle + l.ndihd) == 0) {return;}
+    k_local<PREC, NF, NE><<<l.nwin, TPB, 0, s>>>(a, l, mask);
     note_launches(1);
 }
 

@@ -84,7 +84,9 @@ template<> struct Acc<P_MIXED>
     }
 };
 
-template<int PREC, int G, bool NF, bool NE, int TPP>
+// PER: some system of the arena is periodic (the minimum image is applied
+// where the system asks for it); without it the image code is compiled out.
+template<int PREC, int G, bool NF, bool NE, int TPP, bool PER>
 __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
 {
     // TPP consecutive threads share one slot; lane lg walks partners lg,
@@ -101,9 +103,7 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
     {
         const SysDev& S = a.sys[sys];
         const GlobalParams& P = S.g[G];
-        const bool periodic = S.boundary == B_PERIODIC;
-        const double hw0 = S.halfw[0], hw1 = S.halfw[1], hw2 = S.halfw[2];
-        const double w0 = S.width[0], w1 = S.width[1], w2 = S.width[2];
+        const bool periodic = PER && S.boundary == B_PERIODIC;
         const double4 pi = t.slot_pd[s];
         const long long np = t.np;
         const int n = t.nnb[s];
@@ -122,16 +122,25 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
         const int* __restrict__ nbr = t.nbr + s * TPP + lg;
         const double4* __restrict__ pd = t.slot_pd;
 
-        for(int k = lg; k < n; k += TPP)
+        // software pipeline: the next partner's index and coordinates are
+        // requested before the current pair is evaluated
+        int k = lg;
+        int q = 0;
+        double4 pj = make_double4(0.0, 0.0, 0.0, 0.0);
+        if(k < n) {q = __ldg(nbr + (long long)(k / TPP) * np * TPP); pj = pd[q];}
+        for(; k < n; k += TPP)
         {
-            const int q = __ldg(nbr + (long long)(k / TPP) * np * TPP);
-            const double4 pj = pd[q];
+            const int kn = k + TPP;
+            int qn = q;
+            double4 pn = pj;
+            if(kn < n) {qn = __ldg(nbr + (long long)(kn / TPP) * np * TPP); pn = pd[qn];}
+            do {
             double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-            if(periodic)
+            if(PER && periodic)
             {
-                dx = min_image(dx, hw0, w0);
-                dy = min_image(dy, hw1, w1);
-                dz = min_image(dz, hw2, w2);
+                dx = min_image(dx, S.halfw[0], S.width[0]);
+                dy = min_image(dy, S.halfw[1], S.width[1]);
+                dz = min_image(dz, S.halfw[2], S.width[2]);
             }
             const double l2 = fma(dz, dz, fma(dy, dy, dx * dx));
             const bool count_e = NE && (s < q);
@@ -139,9 +148,10 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
             {
                 const double sigma = pi.w + pj.w;
                 const double sigma_sq = sigma * sigma;
-                if(sigma_sq * crsq < l2) {continue;}
+                const bool in = !(sigma_sq * crsq < l2);
                 if(PREC == P_FP64)
                 {
+                    if(!in) {break;}
                     const double rcp = 1.0 / l2;
                     const double s2 = sigma_sq * rcp;
                     const double s6 = s2 * s2 * s2;
@@ -150,16 +160,19 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
                 }
                 else
                 {
+                    // branch-free: every lane evaluates, pairs outside the
+                    // cutoff add an exact zero
                     const float rcp = __frcp_rn((float)l2);
                     const float s2 = (float)sigma_sq * rcp;
                     const float s6 = s2 * s2 * s2;
-                    if(NF) {acc.add((double)(-eps12f * s6 * s6 * rcp), dx, dy, dz, ovf);}
-                    if(count_e) {energy += (double)(epsf * (s6 * s6 - coefcf));}
+                    const float cf = in ? -eps12f * s6 * s6 * rcp : 0.0f;
+                    if(NF) {acc.add((double)cf, dx, dy, dz, ovf);}
+                    if(count_e && in) {energy += (double)(epsf * (s6 * s6 - coefcf));}
                 }
             }
             else if(G == G_DH)
             {
-                if(!(l2 < abs_cut_sq)) {continue;}
+                if(!(l2 < abs_cut_sq)) {break;}
                 if(PREC == P_FP64)
                 {
                     const double qq = (qi * pj.w) * inv4pi;     // symmetric in i, j
@@ -186,7 +199,7 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
                 const double epsj = t.slot_p1[q];
                 const double epsilon = (epsi == epsj) ? epsi : sqrt(epsi * epsj);
                 const double sigma_sq = sigma * sigma;
-                if(sigma_sq * crsq < l2) {continue;}
+                if(sigma_sq * crsq < l2) {break;}
                 if(PREC == P_FP64)
                 {
                     const double rcp = 1.0 / l2;
@@ -205,6 +218,10 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
                     if(count_e) {energy += (double)(4.0f * ef * (s6 * s6 - s6 - coefcf));}
                 }
             }
+            } while(0);
+            q = qn;
+            pj = pn;
+
         }
     }
     // group reduction: exact in fixed point, fixed order in FP64
@@ -268,13 +285,20 @@ __global__ void k_count_cut(Arena a, TermArrays t, int sys_filter, unsigned long
     if((threadIdx.x & 31) == 0 && cnt) {atomicAdd(out, cnt);}
 }
 
+template<int PREC, int G, int TPP, bool PER>
+void dispatch_per(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
+{
+    const unsigned nb = (unsigned)((t.np * TPP + TPB - 1) / TPB);
+    if(nf && ne)  {k_pair<PREC, G, true,  true,  TPP, PER><<<nb, TPB, 0, s>>>(a, t);}
+    else if(nf)   {k_pair<PREC, G, true,  false, TPP, PER><<<nb, TPB, 0, s>>>(a, t);}
+    else if(ne)   {k_pair<PREC, G, false, true,  TPP, PER><<<nb, TPB, 0, s>>>(a, t);}
+}
+
 template<int PREC, int G, int TPP>
 void dispatch_tpp(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
 {
-    const unsigned nb = (unsigned)((t.np * TPP + TPB - 1) / TPB);
-    if(nf && ne)  {k_pair<PREC, G, true,  true,  TPP><<<nb, TPB, 0, s>>>(a, t);}
-    else if(nf)   {k_pair<PREC, G, true,  false, TPP><<<nb, TPB, 0, s>>>(a, t);}
-    else if(ne)   {k_pair<PREC, G, false, true,  TPP><<<nb, TPB, 0, s>>>(a, t);}
+    if(t.any_periodic) {dispatch_per<PREC, G, TPP, true >(a, t, nf, ne, s);}
+    else               {dispatch_per<PREC, G, TPP, false>(a, t, nf, ne, s);}
 }
 
 template<int PREC, int G>
