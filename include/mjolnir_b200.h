@@ -228,6 +228,33 @@ MJG_API int mjg_device_bytes(mjg_context* ctx, int64_t* bytes);
  * each kernel node). */
 MJG_API int mjg_launch_count(mjg_context* ctx, int64_t* launches);
 
+/* ------------------------------------------------- allocation-free variant
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory themselves -- a host framework that owns every device allocation
+ * through its own pool, or an embedding that forbids cudaMalloc once it has
+ * started -- and so cannot create a context (mjg_commit allocates its arena).
+ *
+ * ExcludedVolume forces and energy of one system whose arrays the caller
+ * already holds in device memory: pos [3n] and radius [n] in, force [3n] and
+ * energy [1] out (both overwritten), enqueued on `stream` (a cudaStream_t;
+ * NULL for the default stream).  Every particle takes part, no pair is
+ * excluded, FP64 arithmetic -- the quantity mjg_term_force gives for
+ * MJG_TERM_EXV of a system without ignore rules.  lower/upper (host, 3 each)
+ * give the periodic box for MJG_PERIODIC_CUBOID, whose positions must lie
+ * inside it; they are ignored for MJG_UNLIMITED.
+ *
+ * The call allocates nothing: its cell list lives in one fixed device array of
+ * about 1 MiB that every GPU loading the library keeps until the process
+ * exits, which limits n to 65536 (larger n returns MJG_EINVAL and prints the
+ * limit).  The first call on a device looks up that array's device address;
+ * make this first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other threads) race and give
+ * wrong results, so serialise them. */
+MJG_API int mjg_exv_force_noalloc(int64_t n, int boundary, const double* lower,
+                                  const double* upper, const double* pos, const double* radius,
+                                  double epsilon, double cutoff_ratio, double* force,
+                                  double* energy, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
