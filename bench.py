@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--serve", type=float, default=20.0,
+                    help="seconds of the Poisson serving run (configs[4]); 0 skips it")
     return ap.parse_args()
 
 
@@ -341,6 +343,14 @@ def run_b200(args, ws, rank, local, pg):
                  "sample": f"{len(sample)} systems run one at a time, FP64, {CHUNK} steps each",
                  "batched_over_plain": value / ws / (tot_ps / tot_t)}
 
+    # ---- serving: Poisson arrivals at 200 jobs/s, continuous batching
+    serving = None
+    if args.serve > 0 and rank == 0 and ws == 1:
+        from mjolnir_b200.serve import serve_poisson
+        serving = serve_poisson(duration=args.serve, rate=200.0, chunk=500)
+        serving["note"] = ("offered load far above one GPU: most arrivals stay queued; "
+                           "latency is over completed jobs")
+
     # ---- CPU baseline: the reference's OpenMP path on a bounded sample
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
@@ -369,6 +379,7 @@ def run_b200(args, ws, rank, local, pg):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_fp64_single_system": plain,
+            "serving": serving,
         }
         print(json.dumps(line))
     eng.close()

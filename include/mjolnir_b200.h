@@ -87,6 +87,12 @@ MJG_API int mjg_system_set_attributes(mjg_context* ctx, int sys, double temperat
  * (forcefield/local/DummyInteraction.hpp). */
 MJG_API int mjg_system_add_connections(mjg_context* ctx, int sys, const char* kind,
                                int64_t m, const int64_t* pairs);
+/* Freezes (1) or releases (0) a system: while frozen it does not advance in
+ * mjg_step and its forces, energies and state stay as they are (its terms are
+ * not evaluated), so a finished job can wait in the arena until the next
+ * mjg_commit removes it.  Takes effect between mjg_step calls.  No
+ * counterpart in the reference (one simulation per process). */
+MJG_API int mjg_system_freeze(mjg_context* ctx, int sys, int frozen);
 /* Removes a system; its device state is freed at the next mjg_commit. */
 MJG_API int mjg_system_remove(mjg_context* ctx, int sys);
 

@@ -73,7 +73,7 @@ struct SysDev {
     unsigned long long step;
     unsigned long long max_disp2;   // bits of a non-negative double (atomicMax)
     int    status;
-    int    pad;
+    int    frozen;          // 1: the system does not advance (set by the host between chunks)
     double energy[NTERMS];
     GlobalParams g[NGLOBAL];
 };

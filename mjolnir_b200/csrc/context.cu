@@ -80,6 +80,7 @@ struct HostLocal {
 struct HostSystem {
     bool alive = true;
     bool resident = false;       // part of the current arena
+    bool frozen = false;         // does not advance (serving: a finished job)
     int arena_slot = -1;
     int64_t n = 0;
     int boundary = B_UNLIMITED;
@@ -422,6 +423,7 @@ void commit(mjg_context* c)
         }
         d.seed = s.seed;
         d.step = s.step;
+        d.frozen = s.frozen ? 1 : 0;
 
         // particles
         const double halfdt = s.dt / 2;
@@ -1051,6 +1053,22 @@ int mjg_system_add_connections(mjg_context* c, int sys, const char* kind, int64_
         const int64_t i = pairs[2 * k], j = pairs[2 * k + 1];
         if(i < 0 || j < 0 || i >= s.n || j >= s.n) {throw Error(MJG_EINVAL, "connection index out of range");}
         s.connections.push_back({kind, {i, j}});
+    }
+    ABI_END(c)
+}
+
+int mjg_system_freeze(mjg_context* c, int sys, int frozen)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    s.frozen = frozen != 0;
+    if(c->committed && s.resident)
+    {
+        CK(cudaStreamSynchronize(c->stream));
+        download_sys(c);
+        c->h_sys[s.arena_slot].frozen = s.frozen ? 1 : 0;
+        upload_sys(c);
+        CK(cudaStreamSynchronize(c->stream));
     }
     ABI_END(c)
 }

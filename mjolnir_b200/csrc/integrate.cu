@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
     const bool active = i < a.n;
     int s = active ? a.psys[i] : 0;
     double d2 = 0.0;
-    if(active)
+    if(active && !a.sys[s].frozen)
     {
         const SysDev& S = a.sys[s];
         double4 p = a.pos[i];
@@ -135,6 +135,7 @@ __global__ void k_margin(Arena a, int* any0, int* any1, int* any2)
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if(s >= a.nsys) {return;}
     SysDev& S = a.sys[s];
+    if(S.frozen) {return;}
     const double d = 2 * sqrt(__longlong_as_double((long long)S.max_disp2));
     S.max_disp2 = 0ull;
     S.step += 1ull;
@@ -157,7 +158,7 @@ template<int PREC>
 __global__ void __launch_bounds__(TPB) k_integrate_last(Arena a)
 {
     const long long i = (long long)blockIdx.x * TPB + threadIdx.x;
-    if(i >= a.n) {return;}
+    if(i >= a.n || a.sys[a.psys[i]].frozen) {return;}
     const double c = a.coef[i].x;
     double fx, fy, fz;
     load_force<PREC>(a.force, i, fx, fy, fz);
@@ -172,7 +173,7 @@ template<int PREC>
 __global__ void k_zero_force(Arena a)
 {
     const long long i = (long long)blockIdx.x * TPB + threadIdx.x;
-    if(i < a.n) {zero_force<PREC>(a.force, i);}
+    if(i < a.n && !a.sys[a.psys[i]].frozen) {zero_force<PREC>(a.force, i);}
 }
 
 __global__ void k_unpack(Arena a, const double* src_pos, const double* src_vel, long long first, long long count)

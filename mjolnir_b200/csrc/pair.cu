@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
         const bool periodic = PER && S.boundary == B_PERIODIC;
         const double4 pi = t.slot_pd[s];
         const long long np = t.np;
-        const int n = t.nnb[s];
+        const int n = S.frozen ? 0 : t.nnb[s];       // a frozen system keeps its forces
 
         // potential constants
         const double crsq  = P.cutoff_ratio_sq;

@@ -118,6 +118,9 @@ class Engine:
         self._c(self.lib.mjg_system_remove(self.ctx, sid))
         self.n_of.pop(sid, None)
 
+    def freeze(self, sid: int, frozen: bool = True):
+        self._c(self.lib.mjg_system_freeze(self.ctx, sid, 1 if frozen else 0))
+
     def commit(self):
         self._c(self.lib.mjg_commit(self.ctx))
 
