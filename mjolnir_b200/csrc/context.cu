@@ -98,6 +98,13 @@ struct HostSystem {
     uint64_t step = 0;
     int rebuilds[NGLOBAL] = {0, 0, 0};
     int64_t off = 0;             // particle offset in the arena
+    // derived once, by the first commit that packs the system (topology and
+    // interactions are fixed from then on): molecule ids, exclusion lists in
+    // local indices, local terms ordered by their smallest particle
+    bool derived = false;
+    std::vector<int32_t> mol_local;
+    std::vector<long long> ex_start_local[NGLOBAL];   // n + 1 entries
+    std::vector<int> ex_idx_local[NGLOBAL];
 };
 
 struct TermDev {
@@ -131,6 +138,8 @@ struct mjg_context {
     mjg::DevBuf d_sys, d_pos, d_vel, d_force, d_coef, d_psys, d_staging, d_mol;
     mjg::DevBuf b_sys, b_pos, b_vel, b_force;   // rollback copies
     mjg::DevBuf d_force_scratch;
+    double* h_pinned = nullptr;             // page-locked host staging (commit)
+    size_t h_pinned_bytes = 0;
     mjg::TermDev term[mjg::NGLOBAL];
     mjg::DevBuf l_bond_idx, l_bond_k, l_bond_v0, l_bond_sys;
     mjg::DevBuf l_angle_idx, l_angle_k, l_angle_v0, l_angle_sys;
@@ -328,31 +337,6 @@ void compute_initial_forces(mjg_context* c)
 
 // ------------------------------------------------------------- commit
 
-void save_resident_state(mjg_context* c)
-{
-    if(!c->committed) {return;}
-    CK(cudaStreamSynchronize(c->stream));
-    download_sys(c);
-    for(size_t k = 0; k < c->arena_ids.size(); ++k)
-    {
-        HostSystem& s = c->sys[c->arena_ids[k]];
-        const SysDev& d = c->h_sys[k];
-        s.step = d.step;
-        for(int g = 0; g < NGLOBAL; ++g) {s.rebuilds[g] = d.g[g].rebuilds;}
-        if(!s.alive) {continue;}
-        s.pos.resize(3 * s.n); s.vel.resize(3 * s.n); s.force.resize(3 * s.n);
-        double* st = c->d_staging.as<double>();
-        launch_pack_state(c->arena, st, 0, s.off, s.n, c->stream);
-        CK(cudaMemcpyAsync(s.pos.data(), st, sizeof(double) * 3 * s.n, cudaMemcpyDeviceToHost, c->stream));
-        launch_pack_state(c->arena, st, 1, s.off, s.n, c->stream);
-        CK(cudaMemcpyAsync(s.vel.data(), st, sizeof(double) * 3 * s.n, cudaMemcpyDeviceToHost, c->stream));
-        launch_pack_state(c->arena, st, 2, s.off, s.n, c->stream);
-        CK(cudaMemcpyAsync(s.force.data(), st, sizeof(double) * 3 * s.n, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        s.force_valid = true;
-    }
-}
-
 int kind_id(std::map<std::string, int>& kinds, const std::string& k)
 {
     auto it = kinds.find(k);
@@ -360,6 +344,119 @@ int kind_id(std::map<std::string, int>& kinds, const std::string& k)
     const int id = (int)kinds.size();
     kinds[k] = id;
     return id;
+}
+
+double* pinned(mjg_context* c, size_t bytes)
+{
+    if(bytes > c->h_pinned_bytes)
+    {
+        if(c->h_pinned) {cudaFreeHost(c->h_pinned); c->h_pinned = nullptr; c->h_pinned_bytes = 0;}
+        CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_pinned), bytes));
+        c->h_pinned_bytes = bytes;
+    }
+    return c->h_pinned;
+}
+
+// copies position, velocity and force of every live resident system back to
+// its host description: one packed pass over the whole arena per field
+void save_resident_state(mjg_context* c)
+{
+    if(!c->committed) {return;}
+    CK(cudaStreamSynchronize(c->stream));
+    download_sys(c);
+    bool any = false;
+    for(size_t k = 0; k < c->arena_ids.size(); ++k)
+    {
+        HostSystem& s = c->sys[c->arena_ids[k]];
+        const SysDev& d = c->h_sys[k];
+        s.step = d.step;
+        for(int g = 0; g < NGLOBAL; ++g) {s.rebuilds[g] = d.g[g].rebuilds;}
+        any = any || s.alive;
+    }
+    if(!any || c->n_tot == 0) {return;}
+    const size_t per = 3 * (size_t)c->n_tot;
+    double* h = pinned(c, sizeof(double) * per);
+    double* st = c->d_staging.as<double>();
+    for(int field = 0; field < 3; ++field)
+    {
+        launch_pack_state(c->arena, st, field, 0, c->n_tot, c->stream);
+        CK(cudaMemcpyAsync(h, st, sizeof(double) * per, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for(size_t k = 0; k < c->arena_ids.size(); ++k)
+        {
+            HostSystem& s = c->sys[c->arena_ids[k]];
+            if(!s.alive) {continue;}
+            std::vector<double>& dst = field == 0 ? s.pos : field == 1 ? s.vel : s.force;
+            dst.assign(h + 3 * s.off, h + 3 * (s.off + s.n));
+            if(field == 2) {s.force_valid = true;}
+        }
+    }
+}
+
+// the per-system data that depends on topology only (molecules, exclusion
+// lists), computed once in the edge order the reference's local force field
+// writes the topology, after which the local terms are put in order of their
+// smallest particle (the order the bonded kernel walks them in)
+void derive(HostSystem& s)
+{
+    if(s.derived) {return;}
+    std::map<std::string, int> kinds;
+    const int bond_kind = kind_id(kinds, "bond");
+    TopologyGraph topo(s.n);
+    auto add_edges = [&](const HostLocal& L, int arity) {
+        if(L.kind.empty() || L.kind == "none") {return;}
+        const int kd = kind_id(kinds, L.kind);
+        for(int64_t t = 0; t < L.m(); ++t)
+        {
+            const int64_t* q = &L.idx[arity * t];
+            for(int x = 0; x < arity; ++x)
+                for(int y = x + 1; y < arity; ++y) {topo.add(q[x], q[y], kd);}
+        }
+    };
+    add_edges(s.bond, 2);
+    add_edges(s.angle, 3);
+    add_edges(s.dihd, 4);
+    for(const auto& e : s.connections) {topo.add(e.second.first, e.second.second, kind_id(kinds, e.first));}
+    const std::vector<int64_t> m = topo.molecules(bond_kind);
+    s.mol_local.assign(m.begin(), m.end());
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        std::vector<std::pair<int, int>> kw;
+        for(const auto& w : s.g[g].within) {kw.emplace_back(kind_id(kinds, w.first), w.second);}
+        s.ex_start_local[g].assign(1, 0);
+        s.ex_idx_local[g].clear();
+        exclusion_csr(topo, s.n, kw, 0, s.ex_start_local[g], s.ex_idx_local[g]);
+    }
+    auto order = [](HostLocal& L, int arity) {
+        const int64_t mm = L.m();
+        std::vector<int64_t> key(mm);
+        for(int64_t t = 0; t < mm; ++t)
+        {
+            int64_t mn = L.idx[arity * t];
+            for(int x = 1; x < arity; ++x) {mn = std::min(mn, L.idx[arity * t + x]);}
+            key[t] = mn;
+        }
+        if(std::is_sorted(key.begin(), key.end())) {return;}
+        std::vector<int64_t> perm(mm);
+        for(int64_t t = 0; t < mm; ++t) {perm[t] = t;}
+        std::stable_sort(perm.begin(), perm.end(), [&](int64_t x, int64_t y) {return key[x] < key[y];});
+        HostLocal o;
+        o.kind = L.kind;
+        o.idx.resize(L.idx.size()); o.k.resize(mm); o.v0.resize(mm);
+        if(!L.n.empty()) {o.n.resize(mm);}
+        for(int64_t t = 0; t < mm; ++t)
+        {
+            const int64_t p = perm[t];
+            for(int x = 0; x < arity; ++x) {o.idx[arity * t + x] = L.idx[arity * p + x];}
+            o.k[t] = L.k[p]; o.v0[t] = L.v0[p];
+            if(!L.n.empty()) {o.n[t] = L.n[p];}
+        }
+        L = std::move(o);
+    };
+    order(s.bond, 2);
+    order(s.angle, 3);
+    order(s.dihd, 4);
+    s.derived = true;
 }
 
 void commit(mjg_context* c)
@@ -456,31 +553,13 @@ void commit(mjg_context* c)
             psys[gi] = k;
         }
 
-        // topology: edges in the order the reference's local force field
-        // writes them (bond, angle, dihedral), then explicit connections
-        std::map<std::string, int> kinds;
-        const int bond_kind = kind_id(kinds, "bond");
-        TopologyGraph topo(s.n);
-        auto add_edges = [&](const HostLocal& L, int arity) {
-            if(L.kind.empty() || L.kind == "none") {return;}
-            const int kd = kind_id(kinds, L.kind);
-            for(int64_t t = 0; t < L.m(); ++t)
-            {
-                const int64_t* q = &L.idx[arity * t];
-                for(int x = 0; x < arity; ++x)
-                    for(int y = x + 1; y < arity; ++y) {topo.add(q[x], q[y], kd);}
-            }
-        };
-        add_edges(s.bond, 2);
-        add_edges(s.angle, 3);
-        add_edges(s.dihd, 4);
-        for(const auto& e : s.connections) {topo.add(e.second.first, e.second.second, kind_id(kinds, e.first));}
-        const std::vector<int64_t> m = topo.molecules(bond_kind);
+        // topology-derived data, computed at the system's first commit
+        derive(s);
         int64_t nmol = 0;
         for(int64_t i = 0; i < s.n; ++i)
         {
-            mol[s.off + i] = (int)(mol_base + m[i]);
-            nmol = std::max(nmol, m[i] + 1);
+            mol[s.off + i] = (int)(mol_base + s.mol_local[i]);
+            nmol = std::max<int64_t>(nmol, s.mol_local[i] + 1);
         }
         mol_base += nmol;
 
@@ -489,9 +568,12 @@ void commit(mjg_context* c)
         {
             const HostGlobal& H = s.g[g];
             GlobalParams& G = d.g[g];
-            std::vector<std::pair<int, int>> kw;
-            for(const auto& w : H.within) {kw.emplace_back(kind_id(kinds, w.first), w.second);}
-            exclusion_csr(topo, s.n, kw, s.off, ex_start[g], ex_idx[g]);
+            {
+                const long long base = (long long)ex_idx[g].size();
+                const std::vector<long long>& ls = s.ex_start_local[g];
+                for(int64_t i = 1; i <= s.n; ++i) {ex_start[g].push_back(base + ls[i]);}
+                for(const int j : s.ex_idx_local[g]) {ex_idx[g].push_back((int)(j + s.off));}
+            }
             if(!H.on) {continue;}
             G.on = 1;
             G.margin = H.margin;
@@ -772,6 +854,13 @@ void commit(mjg_context* c)
             for(int x = 1; x < arity; ++x) {mn = std::min(mn, idx[arity * t + x]);}
             key[t] = mn;
         }
+        win.assign((size_t)nwin + 1, 0);
+        if(std::is_sorted(key.begin(), key.end()))      // every system's terms are kept in order
+        {
+            for(size_t t = 0; t < m; ++t) {win[(size_t)key[t] / 256 + 1] += 1;}
+            for(int w = 0; w < nwin; ++w) {win[w + 1] += win[w];}
+            return;
+        }
         std::vector<size_t> perm(m);
         for(size_t t = 0; t < m; ++t) {perm[t] = t;}
         std::stable_sort(perm.begin(), perm.end(), [&](size_t x, size_t y) {return key[x] < key[y];});
@@ -786,7 +875,6 @@ void commit(mjg_context* c)
         }
         idx.swap(idx2); kk.swap(k2); v0.swap(v2); sysv.swap(sys2);
         if(nn) {nn->swap(n2);}
-        win.assign((size_t)nwin + 1, 0);
         for(size_t t = 0; t < m; ++t) {win[(size_t)key[perm[t]] / 256 + 1] += 1;}
         for(int w = 0; w < nwin; ++w) {win[w + 1] += win[w];}
     };
@@ -839,14 +927,35 @@ void commit(mjg_context* c)
     c->committed = true;
     rebuild_all(c);
     compute_initial_forces(c);
-    // systems that were resident keep their exact force array
-    for(int k = 0; k < nsys; ++k)
+    // systems that were resident keep their exact force array: one upload,
+    // then one conversion per run of consecutive such systems
     {
-        HostSystem& s = c->sys[ids[k]];
-        if(!s.force_valid || (int64_t)s.force.size() != 3 * s.n) {continue;}
-        double* stg = c->d_staging.as<double>();
-        CK(cudaMemcpyAsync(stg, s.force.data(), sizeof(double) * 3 * s.n, cudaMemcpyHostToDevice, st));
-        launch_set_force(c->arena, stg, s.off, s.n, st);
+        auto keeps = [&](int k) {
+            const HostSystem& s = c->sys[ids[k]];
+            return s.force_valid && (int64_t)s.force.size() == 3 * s.n;
+        };
+        bool any = false;
+        for(int k = 0; k < nsys && !any; ++k) {any = keeps(k);}
+        if(any)
+        {
+            double* h = pinned(c, sizeof(double) * 3 * (size_t)n_tot);
+            for(int k = 0; k < nsys; ++k)
+            {
+                if(keeps(k)) {const HostSystem& s = c->sys[ids[k]]; std::copy(s.force.begin(), s.force.end(), h + 3 * s.off);}
+            }
+            double* stg = c->d_staging.as<double>();
+            CK(cudaMemcpyAsync(stg, h, sizeof(double) * 3 * (size_t)n_tot, cudaMemcpyHostToDevice, st));
+            for(int k = 0; k < nsys;)
+            {
+                if(!keeps(k)) {++k; continue;}
+                int e = k;
+                while(e + 1 < nsys && keeps(e + 1)) {++e;}
+                const int64_t off = c->sys[ids[k]].off;
+                const int64_t cnt = c->sys[ids[e]].off + c->sys[ids[e]].n - off;
+                launch_set_force(c->arena, stg + 3 * off, off, cnt, st);
+                k = e + 1;
+            }
+        }
     }
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
@@ -981,6 +1090,7 @@ void mjg_context_destroy(mjg_context* c)
                           &t.ex_idx};
         for(auto* b : bufs) {b->release();}
     }
+    if(c->h_pinned) {cudaFreeHost(c->h_pinned);}
     if(c->stream) {cudaStreamDestroy(c->stream);}
     delete c;
 }
@@ -1077,10 +1187,14 @@ int mjg_system_remove(mjg_context* c, int sys)
 {
     ABI_BEGIN(c)
     HostSystem& s = get_sys(c, sys);
-    s.alive = false;
-    std::vector<double>().swap(s.pos);
-    std::vector<double>().swap(s.vel);
-    std::vector<double>().swap(s.force);
+    // keep only what the arena bookkeeping reads until the next commit
+    HostSystem dead;
+    dead.alive = false;
+    dead.resident = s.resident;
+    dead.arena_slot = s.arena_slot;
+    dead.n = s.n;
+    dead.off = s.off;
+    s = std::move(dead);
     ABI_END(c)
 }
 

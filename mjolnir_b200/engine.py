@@ -77,11 +77,14 @@ class Engine:
             chain = np.stack([np.arange(d.n - 1), np.arange(1, d.n)], axis=1).astype(np.int64)
             chain = np.ascontiguousarray(chain)
             self._c(L.mjg_system_add_connections(self.ctx, s, b"bond", d.n - 1, A.i64(chain)))
-        ign = A.IGNORE[d.ignore_molecule]
-        within = [("bond", d.ignore_bond_within)] if d.ignore_bond_within > 0 else []
         for term, t in ((A.TERM_EXV, d.exv), (A.TERM_DH, d.dh), (A.TERM_LJ, d.lj)):
             if t is None:
                 continue
+            ign = A.IGNORE[t.ignore_molecule if t.ignore_molecule is not None else d.ignore_molecule]
+            if t.ignore_within is not None:
+                within = [(k, int(v)) for k, v in t.ignore_within.items() if int(v) > 0]
+            else:
+                within = [("bond", d.ignore_bond_within)] if d.ignore_bond_within > 0 else []
             idx = _arr(t.idx, np.int64)
             p0 = _arr(t.param0, np.float64)
             if term == A.TERM_EXV:
@@ -99,16 +102,16 @@ class Engine:
             self._c(L.mjg_ignore_set(self.ctx, s, term, ign, len(within), kinds, A.i32(vals)))
         if d.bonds is not None:
             idx, k, v0 = (_arr(d.bonds[0], np.int64), _arr(d.bonds[1], np.float64), _arr(d.bonds[2], np.float64))
-            self._c(L.mjg_bonds_set(self.ctx, s, b"bond", len(k), A.i64(idx), A.f64(k), A.f64(v0)))
+            self._c(L.mjg_bonds_set(self.ctx, s, d.bond_topology.encode(), len(k), A.i64(idx), A.f64(k), A.f64(v0)))
         if d.angles is not None:
             idx, k, v0 = (_arr(d.angles[0], np.int64), _arr(d.angles[1], np.float64), _arr(d.angles[2], np.float64))
-            self._c(L.mjg_angles_set(self.ctx, s, b"none", len(k), A.i64(idx), A.f64(k), A.f64(v0)))
+            self._c(L.mjg_angles_set(self.ctx, s, d.angle_topology.encode(), len(k), A.i64(idx), A.f64(k), A.f64(v0)))
         if d.dihedrals is not None:
             idx = _arr(d.dihedrals[0], np.int64)
             k = _arr(d.dihedrals[1], np.float64)
             nn = _arr(d.dihedrals[2], np.int32)
             v0 = _arr(d.dihedrals[3], np.float64)
-            self._c(L.mjg_dihedrals_set(self.ctx, s, b"none", len(k), A.i64(idx), A.f64(k), A.i32(nn), A.f64(v0)))
+            self._c(L.mjg_dihedrals_set(self.ctx, s, d.dihedral_topology.encode(), len(k), A.i64(idx), A.f64(k), A.i32(nn), A.f64(v0)))
         kind = A.VELOCITY_VERLET if d.integrator == "VelocityVerlet" else A.BAOAB
         gam = _arr(d.gamma if d.gamma is not None else np.zeros(d.n), np.float64)
         self._c(L.mjg_integrator_set(self.ctx, s, kind, float(d.dt), A.f64(gam), int(d.seed) & ((1 << 64) - 1)))

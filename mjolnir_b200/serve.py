@@ -3,12 +3,13 @@
 Every admitted job is one system in the engine's arena, and all admitted
 systems advance together in the same kernels.  The loop:
 
-  1. admit queued jobs (in arrival order) while their estimated device
-     footprint fits the HBM budget; newly admitted systems and the removal of
-     finished ones take effect at one ``commit`` (which keeps the state of the
-     systems that stay);
+  1. admit queued jobs (in arrival order) while the resident particles stay
+     under a cap and their estimated device footprint fits the HBM budget;
+     newly admitted systems and the removal of finished ones take effect at
+     one ``commit`` (which keeps the state of the systems that stay);
   2. advance every running job by ``min(chunk, fewest steps any running job
-     still needs)`` steps, so each job ends exactly on its step count;
+     still needs)`` steps (fewer if that would take longer than
+     ``chunk_seconds``), so each job ends exactly on its step count;
   3. read back the jobs that finished, freeze them (they stop advancing and
      cost no force evaluation) and retire them at the next commit.
 
@@ -54,13 +55,25 @@ class Job:
 
 
 class Server:
+    """Admission control: a queued job is admitted (in arrival order) when the
+    resident particles stay within ``max_particles`` and the estimated device
+    footprint within ``hbm_fraction`` of device memory.  ``max_particles`` is
+    the concurrency at which the arena's throughput has saturated: admitting
+    more raises no throughput, only every running job's latency.  Chunks are
+    sized so one lasts about ``chunk_seconds`` (at most ``chunk`` steps), which
+    bounds how long an arrival waits for the next admission."""
+
     def __init__(self, precision: str = "mixed", chunk: int = 500, hbm_fraction: float = 0.8,
                  device: int = 0, bytes_per_particle: float = 2048.0, min_commit_interval: float = 0.0,
-                 keep_results: bool = True, builders: int = 4):
+                 keep_results: bool = True, builders: int = 4, max_particles: int = 2_000_000,
+                 chunk_seconds: Optional[float] = None, lookahead: int = 64):
         self.eng = Engine(precision, device=device)
         self.chunk = int(chunk)
+        self.chunk_seconds = chunk_seconds
         self.keep_results = keep_results
         self.min_commit_interval = min_commit_interval
+        self.max_particles = int(max_particles)
+        self.lookahead = int(lookahead)
         total = self._device_total(device)
         self.budget = hbm_fraction * total
         self.bpp = bytes_per_particle           # refined after every commit
@@ -75,6 +88,11 @@ class Server:
         self.last_commit = -1e9
         self.particle_steps = 0
         self.commits = 0
+        self.commit_s = 0.0
+        self.step_s = 0.0
+        self.steps_run = 0
+        self.sec_per_step = None                # of the current arena, measured
+        self.max_queue = 0
 
     @staticmethod
     def _device_total(device: int) -> float:
@@ -89,10 +107,18 @@ class Server:
 
     # ---------------------------------------------------------------- input
     def submit(self, job: Job):
-        """Queues a job (thread safe); its system is built in the background."""
+        """Queues a job (thread safe); its system is built in the background
+        once it is near the head of the queue."""
         with self.lock:
             self.queue.append(job)
-            if job.desc is None and job.build is not None:
+            self.max_queue = max(self.max_queue, len(self.queue))
+            self._prefetch()
+
+    def _prefetch(self):
+        for k, job in enumerate(self.queue):
+            if k >= self.lookahead:
+                break
+            if job.desc is None and job.build is not None and job.job_id not in self.futures:
                 self.futures[job.job_id] = self.pool.submit(job.build)
 
     # ---------------------------------------------------------------- loop
@@ -102,7 +128,7 @@ class Server:
     def _admit(self) -> bool:
         """Adds every queued job that fits; returns True if the arena changed."""
         changed = False
-        used = self._resident_particles() * self.bpp
+        resident = self._resident_particles()
         with self.lock:
             while self.queue:
                 job = self.queue[0]
@@ -112,30 +138,41 @@ class Server:
                         break                   # keep arrival order
                     job.desc = fut.result()
                     del self.futures[job.job_id]
-                need = job.desc.n * self.bpp
-                if self.running and used + need > self.budget:
+                n = job.desc.n
+                if self.running and ((resident + n) * self.bpp > self.budget
+                                     or resident + n > self.max_particles):
                     break
                 self.queue.popleft()
-                job.n = job.desc.n
+                job.n = n
                 job.sid = self.eng.add_system(job.desc)
                 job.admitted = self.now()
                 if not self.keep_results:
                     job.desc = None
                 self.running[job.sid] = job
-                used += need
+                resident += n
                 changed = True
+            self._prefetch()
         return changed
 
     def _commit(self):
+        t = time.perf_counter()
         for sid in self.retiring:
             self.eng.remove_system(sid)
         self.retiring = []
         self.eng.commit()
         self.commits += 1
+        self.commit_s += time.perf_counter() - t
         self.last_commit = self.now()
+        self.sec_per_step = None
         n = self._resident_particles()
         if n > 0:
             self.bpp = max(self.bpp * 0.5, self.eng.device_bytes() / n)
+
+    def _chunk_steps(self, live) -> int:
+        k = min(self.chunk, min(j.nsteps - j.done for j in live))
+        if self.chunk_seconds is not None and self.sec_per_step:
+            k = min(k, max(10, int(self.chunk_seconds / self.sec_per_step)))
+        return max(1, k)
 
     def step_once(self) -> bool:
         """One admission/advance/retire round; False when nothing is running."""
@@ -148,8 +185,14 @@ class Server:
             if self.retiring:
                 self._commit()
             return False
-        k = min(self.chunk, min(j.nsteps - j.done for j in live))
+        k = self._chunk_steps(live)
+        t = time.perf_counter()
         self.eng.step(k)
+        dt = time.perf_counter() - t
+        self.step_s += dt
+        self.steps_run += k
+        if k >= 10:
+            self.sec_per_step = dt / k
         t = self.now()
         for j in live:
             j.done += k
@@ -179,10 +222,12 @@ class Server:
         lat = sorted(j.latency for j in self.finished)
         q = lambda p: lat[min(len(lat) - 1, int(p * len(lat)))] if lat else None  # noqa: E731
         return {"completed": len(lat), "queued": len(self.queue), "running": len(self.running),
+                "resident_particles": self._resident_particles(), "max_queue": self.max_queue,
                 "latency_p50_s": q(0.50), "latency_p90_s": q(0.90), "latency_p99_s": q(0.99),
                 "latency_mean_s": statistics.mean(lat) if lat else None,
                 "particle_steps_per_s": self.particle_steps / wall if wall > 0 else None,
-                "commits": self.commits}
+                "commits": self.commits, "commit_s": self.commit_s, "step_s": self.step_s,
+                "md_steps": self.steps_run}
 
     def close(self):
         self.pool.shutdown(wait=False, cancel_futures=True)
@@ -227,12 +272,15 @@ def poisson_workload(rate: float, duration: float, seed: int = 7, nmin: int = 20
     return jobs
 
 
-def serve_poisson(duration: float = 60.0, rate: float = 200.0, chunk: int = 500, seed: int = 7,
-                  precision: str = "mixed", tune: bool = False) -> dict:
+def serve_poisson(duration: float = 60.0, rate: float = 200.0, chunk: int = 2000, seed: int = 7,
+                  precision: str = "mixed", max_particles: int = 2_000_000,
+                  chunk_seconds: float = 0.5, min_commit_interval: float = 0.5) -> dict:
     """Replays a Poisson stream in real time for `duration` seconds and
     reports completion latency, queue depth and aggregate throughput."""
     jobs = poisson_workload(rate, duration, seed=seed)
-    srv = Server(precision=precision, chunk=chunk, keep_results=False, min_commit_interval=0.25)
+    srv = Server(precision=precision, chunk=chunk, keep_results=False,
+                 min_commit_interval=min_commit_interval, max_particles=max_particles,
+                 chunk_seconds=chunk_seconds)
     srv.t0 = time.perf_counter()
     i = 0
     while srv.now() < duration:
@@ -243,6 +291,7 @@ def serve_poisson(duration: float = 60.0, rate: float = 200.0, chunk: int = 500,
             time.sleep(0.002)
     wall = srv.now()
     out = srv.stats(wall)
-    out.update({"arrived": i, "duration_s": wall, "rate_jobs_per_s": rate, "chunk_steps": chunk})
+    out.update({"arrived": i, "duration_s": wall, "rate_jobs_per_s": rate, "max_chunk_steps": chunk,
+                "chunk_seconds": chunk_seconds, "max_particles": max_particles})
     srv.close()
     return out

@@ -31,6 +31,9 @@ class PairTerm:
     cutoff: float = 2.0                # relative cutoff (potential default)
     margin: float = 0.5                # relative Verlet skin of the cell list
     epsilon: float = 0.2               # ExcludedVolume epsilon
+    # this term's own ``ignore`` table; None falls back to the system-wide rule
+    ignore_molecule: Optional[str] = None       # "Nothing" | "Self" | "Others"
+    ignore_within: Optional[dict] = None        # {connection kind: topological distance}
 
 
 @dataclasses.dataclass
@@ -52,6 +55,9 @@ class SystemDesc:
     bonds: Optional[tuple] = None      # (idx (m,2) int64, k (m,), v0 (m,))
     angles: Optional[tuple] = None     # (idx (m,3), k, v0)
     dihedrals: Optional[tuple] = None  # (idx (m,4), k, n int32, v0)
+    bond_topology: str = "bond"        # connection kind each local term writes
+    angle_topology: str = "none"
+    dihedral_topology: str = "none"
     integrator: str = "BAOAB"          # "BAOAB" | "VelocityVerlet"
     dt: float = 0.01
     gamma: Optional[np.ndarray] = None

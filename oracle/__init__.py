@@ -61,6 +61,29 @@ def _ptr(a, ct):
     return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
 
 
+def _uniform_ignore(desc):
+    """The oracle takes one ignore rule for all pair terms, with exclusions
+    along "bond" connections only, and the default topology kinds of the
+    local terms; anything else is outside what it restates."""
+    rules = set()
+    for t in desc.pair_terms():
+        mol = t.ignore_molecule if getattr(t, "ignore_molecule", None) is not None else desc.ignore_molecule
+        w = getattr(t, "ignore_within", None)
+        if w is None:
+            w = {"bond": desc.ignore_bond_within} if desc.ignore_bond_within > 0 else {}
+        w = {k: int(v) for k, v in w.items() if int(v) > 0}
+        if set(w) - {"bond"}:
+            raise NotImplementedError("the oracle excludes along \"bond\" connections only")
+        rules.add((mol, w.get("bond", 0)))
+    if len(rules) > 1:
+        raise NotImplementedError("the oracle takes one ignore rule for every pair term")
+    kinds = (getattr(desc, "bond_topology", "bond"), getattr(desc, "angle_topology", "none"),
+             getattr(desc, "dihedral_topology", "none"))
+    if kinds != ("bond", "none", "none"):
+        raise NotImplementedError("the oracle writes bonds as \"bond\" and angles, dihedrals as \"none\"")
+    return rules.pop() if rules else (desc.ignore_molecule, int(desc.ignore_bond_within))
+
+
 def make_spec(desc):
     """Returns (OrcSpec, keepalive) for a SystemDesc-like object."""
     keep = []
@@ -83,8 +106,9 @@ def make_spec(desc):
     s.mass = _ptr(arr(desc.mass, np.float64), C.c_double)
     s.temperature = desc.temperature
     s.ionic_strength = desc.ionic_strength
-    s.ignore_molecule = {"Nothing": 0, "Self": 1, "Intra": 1, "Others": 2, "Inter": 2}[desc.ignore_molecule]
-    s.ignore_bond_within = int(desc.ignore_bond_within)
+    mol, within = _uniform_ignore(desc)
+    s.ignore_molecule = {"Nothing": 0, "Self": 1, "Intra": 1, "Others": 2, "Inter": 2}[mol]
+    s.ignore_bond_within = within
     if desc.exv is not None:
         t = desc.exv
         s.exv_on, s.exv_eps, s.exv_cutoff, s.exv_margin = 1, t.epsilon, t.cutoff, t.margin

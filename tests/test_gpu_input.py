@@ -1,0 +1,35 @@
+"""A system read from a Mjolnir input file runs exactly like the same system
+handed to the engine directly, and the runner writes the energy file."""
+import numpy as np
+import pytest
+
+from mjolnir_b200 import input as I
+from mjolnir_b200 import systems as S
+from mjolnir_b200.__main__ import run
+from mjolnir_b200.engine import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+def test_toml_run_matches_direct(tmp_path):
+    d = S.polymer_melt(nchains=4, nbeads=50, radius=45.0, seed=21)
+    path = str(tmp_path / "melt.toml")
+    I.dump(d, path, total_step=40, save_step=20, prefix="melt")
+    text = open(path).read().replace('output.path = "./"', f'output.path = "{tmp_path}/"')
+    open(path, "w").write(text)
+    res = run(path, precision="mixed")
+    ene = np.loadtxt(res["energy_file"])
+    assert ene.shape == (3, 7)                       # steps 0, 20, 40; 5 terms + kinetic
+    assert list(ene[:, 0]) == [0, 20, 40]
+    e = Engine("mixed")
+    sid = e.add_system(d)
+    e.commit()
+    e.step(40)
+    en = e.energies(sid)
+    row = ene[-1]
+    for k, t in enumerate(("bond", "angle", "dihedral", "exv", "dh")):
+        assert row[1 + k] == pytest.approx(en[t], rel=1e-9, abs=1e-9)
+    p, v, _ = e.state(sid)
+    kin = 0.5 * float(np.sum(d.mass[:, None] * v * v))
+    assert row[6] == pytest.approx(kin, rel=1e-9)
+    e.close()

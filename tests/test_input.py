@@ -1,0 +1,214 @@
+"""The TOML reader follows the reference's input schema: includes, file_name
+tables, env variables, offsets, defaults and its error cases; a system written
+out and read back gives the oracle the same forces, energies and lists as the
+golden fixtures made by the reference."""
+import os
+import textwrap
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden_cases
+from mjolnir_b200 import input as I
+from mjolnir_b200 import systems as S
+
+CASES = golden_cases()
+
+
+def _write(tmp_path, name, text):
+    p = tmp_path / name
+    p.write_text(textwrap.dedent(text))
+    return str(p)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_written_input_reproduces_golden(name, tmp_path):
+    d, fx = CASES[name]
+    path = str(tmp_path / "in.toml")
+    I.dump(d, path)
+    got = I.load(path).desc
+    assert np.array_equal(got.pos, d.pos) and np.array_equal(got.vel, d.vel)
+    o = oracle.Oracle(got)
+    for t in ("bond", "angle", "dihedral", "exv", "dh", "lj"):
+        if f"force_{t}" in fx:
+            f, e = o.term_force(t, got.pos)
+            ref = fx[f"force_{t}"]
+            assert np.abs(f - ref).max() <= 1e-14 * max(np.abs(ref).max(), 1e-300), (name, t)
+            assert e == pytest.approx(float(fx[f"energy_{t}"]), rel=1e-14, abs=1e-300)
+        if f"pairs_{t}" in fx:
+            assert np.array_equal(o.neighbors(t, got.pos), fx[f"pairs_{t}"].astype(np.int64)), (name, t)
+
+
+def test_round_trip_keeps_every_field(tmp_path):
+    d = S.polymer_melt(nchains=3, nbeads=12, radius=40.0, seed=5)
+    path = str(tmp_path / "melt.toml")
+    I.dump(d, path, total_step=500, save_step=50)
+    inp = I.load(path)
+    g = inp.desc
+    assert (inp.total_step, inp.save_step, inp.precision) == (500, 50, "double")
+    assert g.boundary == "Unlimited" and g.integrator == "BAOAB" and g.seed == d.seed
+    assert g.dt == d.dt and g.temperature == d.temperature and g.ionic_strength == d.ionic_strength
+    np.testing.assert_array_equal(g.mass, d.mass)
+    np.testing.assert_array_equal(g.gamma, d.gamma)
+    for a, b in ((g.bonds, d.bonds), (g.angles, d.angles), (g.dihedrals, d.dihedrals)):
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+    for key in ("exv", "dh"):
+        ta, tb = getattr(g, key), getattr(d, key)
+        np.testing.assert_array_equal(ta.idx, tb.idx)
+        np.testing.assert_array_equal(ta.param0, tb.param0)
+        assert (ta.cutoff, ta.margin, ta.epsilon) == (tb.cutoff, tb.margin, tb.epsilon)
+    assert g.ignore_molecule == "Nothing" and g.ignore_bond_within == 3
+
+
+SIM = """
+[simulator]
+type          = "MolecularDynamics"
+boundary_type = "PeriodicCuboid"
+precision     = "double"
+parallelism   = "OpenMP"
+seed          = 2374
+delta_t       = 0.005
+total_step    = 100
+save_step     = 10
+integrator.type = "BAOABLangevin"
+integrator.env.g = 1.0
+integrator.gammas = [
+{index = 0, gamma = "g"},
+{index = 0, offset = 1, gamma = 0.5},
+{index = 2, "γ" = 2.0},
+{index = 3, gamma = 1.0},
+]
+"""
+
+SYSTEM = """
+[[systems]]
+attributes.temperature = 300.0
+boundary_shape.lower = [0.0, 0.0, 0.0]
+boundary_shape.upper = [10.0, 10.0, 10.0]
+particles = [
+{mass = 1.0, position = [1.0, 1.0, 1.0]},
+{m    = 2.0, pos      = [2.5, 1.0, 1.0]},
+{mass = 1.0, position = [11.0, 1.0, -1.0]},
+{mass = 1.0, position = [5.0, 5.0, 5.0], name = "C", group = "NONE"},
+]
+"""
+
+FF = """
+[[forcefields]]
+[[forcefields.local]]
+interaction = "BondLength"
+potential   = "Harmonic"
+topology    = "bond"
+env.k = 10.0
+parameters  = [
+{indices = [0, 1], k = "k", v0 = 1.5},
+{indices = [0, 1], offset = 1, k = 10.0, v0 = 1.5},
+]
+[[forcefields.global]]
+interaction = "Pair"
+potential   = "LennardJones"
+ignore.molecule = "Nothing"
+ignore.particles_within.bond = 1
+spatial_partition = {type = "CellList", margin = 0.25}
+env.s = 1.0
+parameters = [
+{index = 0, sigma = "s", epsilon = 1.0},
+{index = 1, "σ" = 1.0, "ε" = 0.5},
+{index = 1, offset = 1, sigma = 1.0, epsilon = 1.0},
+{index = 3, sigma = 1.0, epsilon = 1.0},
+]
+"""
+
+HEAD = """
+[files]
+output.prefix = "t"
+output.path   = "./"
+output.format = "xyz"
+input.path    = "{path}"
+
+[units]
+length = "angstrom"
+energy = "kcal/mol"
+"""
+
+
+def test_env_offsets_defaults_and_wrapping(tmp_path):
+    path = _write(tmp_path, "in.toml", HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF)
+    inp = I.load(path)
+    d = inp.desc
+    assert inp.parallelism == "OpenMP" and inp.seed == 2374 and d.seed == 2374
+    np.testing.assert_array_equal(d.gamma, [1.0, 0.5, 2.0, 1.0])
+    np.testing.assert_array_equal(d.mass, [1.0, 2.0, 1.0, 1.0])
+    np.testing.assert_array_equal(d.pos[2], [1.0, 1.0, 9.0])       # wrapped into the box
+    np.testing.assert_array_equal(d.bonds[0], [[0, 1], [1, 2]])
+    np.testing.assert_array_equal(d.bonds[1], [10.0, 10.0])
+    assert d.lj.cutoff == 2.5 and d.lj.margin == 0.25                # default LJ cutoff
+    np.testing.assert_array_equal(d.lj.idx, [0, 1, 2, 3])
+    np.testing.assert_array_equal(d.lj.param1, [1.0, 0.5, 1.0, 1.0])
+    assert d.ignore_bond_within == 1
+    # no velocities given: Maxwell-Boltzmann draws from the seed, reproducibly
+    assert np.all(np.isfinite(d.vel)) and np.any(d.vel != 0)
+    np.testing.assert_array_equal(I.load(path).desc.vel, d.vel)
+
+
+def test_include_and_file_name(tmp_path):
+    _write(tmp_path, "sim.toml", SIM.replace("[simulator]", ""))
+    _write(tmp_path, "sys.toml", SYSTEM)
+    _write(tmp_path, "ff.toml", FF.replace("[[forcefields]]", "").replace("[[forcefields.local]]", "[[local]]")
+           .replace("[[forcefields.global]]", "[[global]]"))
+    main = HEAD.format(path=str(tmp_path) + "/") + """
+[simulator]
+include = "sim.toml"
+[[systems]]
+file_name = "sys.toml"
+[[forcefields]]
+include = "ff.toml"
+"""
+    path = _write(tmp_path, "main.toml", main)
+    d = I.load(path).desc
+    flat = I.load(_write(tmp_path, "flat.toml", HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF)).desc
+    np.testing.assert_array_equal(d.pos, flat.pos)
+    np.testing.assert_array_equal(d.bonds[0], flat.bonds[0])
+    np.testing.assert_array_equal(d.lj.param0, flat.lj.param0)
+
+
+@pytest.mark.parametrize("edit, msg", [
+    (lambda t: t.replace('potential   = "LennardJones"', 'potential   = "WCA"'), "WCA"),
+    (lambda t: t.replace('ignore.molecule = "Nothing"', 'ignore.molecule = "Nothing"\nignore.group.intra = ["A"]'),
+     "ignore.group"),
+    (lambda t: t.replace('length = "angstrom"', 'length = "nm"'), "angstrom"),
+    (lambda t: t.replace('{index = 3, sigma', '{index = 2, sigma'), "twice"),
+    (lambda t: t.replace('{mass = 1.0, position = [1.0, 1.0, 1.0]}',
+                         '{mass = 1.0, position = [1.0, 1.0, 1.0], velocity = [0.0, 0.0, 0.0]}'), "velocity"),
+    (lambda t: t.replace('integrator.type = "BAOABLangevin"', 'integrator.type = "UnderdampedLangevin"'),
+     "BAOABLangevin"),
+    (lambda t: t.replace('k = "k"', 'k = "kk"'), "kk"),
+    (lambda t: t.replace('type = "CellList"', 'type = "Naive"'), "CellList"),
+    (lambda t: t.replace('[0, 1], offset = 1', '[0, 7], offset = 1'), "out of range"),
+])
+def test_errors_name_the_problem(tmp_path, edit, msg):
+    text = edit(HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF)
+    path = _write(tmp_path, "bad.toml", text)
+    with pytest.raises(I.InputError, match=msg):
+        I.load(path)
+
+
+def test_per_term_ignore_rules(tmp_path):
+    text = HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF + """
+[[forcefields.global]]
+interaction = "Pair"
+potential   = "DebyeHuckel"
+ignore.molecule = "Self"
+spatial_partition = {type = "VerletList", margin = 0.5}
+parameters = [{index = 0, charge = 1.0}, {index = 3, charge = -1.0}]
+"""
+    text = text.replace("attributes.temperature = 300.0",
+                        "attributes.temperature = 300.0\nattributes.ionic_strength = 0.1")
+    d = I.load(_write(tmp_path, "in.toml", text)).desc
+    assert d.dh.ignore_molecule == "Self" and d.dh.ignore_within == {}
+    assert d.lj.ignore_molecule == "Nothing" and d.lj.ignore_within == {"bond": 1}
+    assert d.dh.cutoff == 5.5
+    with pytest.raises(NotImplementedError):
+        oracle.make_spec(d)
