@@ -15,8 +15,8 @@
  * path:line inside the Mjolnir source tree (v1.31.0).
  *
  * Indices are 0-based particle indices local to their system.  Units are
- * those of the caller's input (the reference's kcal/mol + angstrom by
- * default: input/read_units.hpp:32-91).
+ * kcal/mol and angstrom: kB, the vacuum permittivity and the volume factor
+ * are those input/read_units.hpp:32-91 derives for these units.
  */
 #ifndef MJOLNIR_B200_H
 #define MJOLNIR_B200_H
