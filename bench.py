@@ -223,7 +223,7 @@ def run_reference_arm(args, ws, rank, pg):
     print(json.dumps(line))
 
 
-def pair_kernels(eng, descs, sys_id, precision):
+def pair_kernels(eng, descs, sys_id, precision, label="batch"):
     """Time and algorithmic bytes of each pair kernel launch (slot gather +
     pair kernel).  Algorithmic bytes per launch: per participant its position
     and parameter (16 B as float4 in the mixed form, 32 B as double4 in FP64)
@@ -231,8 +231,11 @@ def pair_kernels(eng, descs, sys_id, precision):
     pair inside the cutoff (P_cut, margin-free)."""
     out = {}
     per_slot = (16 if precision == "mixed" else 32) + 24
+    import torch
     for term in ("exv", "dh"):
+        torch.cuda.nvtx.range_push(f"{label}_{precision}_{term}")   # profiler selection
         ms = eng.time_kernel(term, reps=20)
+        torch.cuda.nvtx.range_pop()
         pcut = eng.pair_count(sys_id, term)
         nslots = sum(len(getattr(d, term).idx) for d in descs)
         bytes_alg = nslots * per_slot + 4 * pcut
@@ -245,6 +248,7 @@ def fluid_pair_roofline(local, peak):
     """Pair kernels on the precision-at-scale fluid: 1,048,576 beads at
     0.003 per cubic A in a periodic cube, ExcludedVolume on all beads and
     DebyeHuckel on 30 % (I = 0.15 M, T = 300 K), single system."""
+    from mjolnir_b200 import autotune
     from mjolnir_b200 import systems as S
     from mjolnir_b200.engine import Engine
     d = S.bead_fluid(n=1 << 20, density=0.003, seed=3, margin=0.2)
@@ -254,10 +258,11 @@ def fluid_pair_roofline(local, peak):
         e.add_system(d)
         e.commit()
         e.step(2)
-        k = pair_kernels(e, [d], 0, prec)
+        shape = autotune.tune_shapes(e, terms=("exv", "dh"))
+        k = pair_kernels(e, [d], 0, prec, label="fluid")
         tot_b = sum(v["bytes"] for v in k.values())
         tot_ms = sum(v["ms"] for v in k.values())
-        out[prec] = {"terms": k, "gbs": tot_b / (tot_ms * 1e-3) / 1e9,
+        out[prec] = {"terms": k, "shape": shape, "gbs": tot_b / (tot_ms * 1e-3) / 1e9,
                      "frac": tot_b / (tot_ms * 1e-3) / 1e9 / peak, "ms": tot_ms}
         e.close()
     return out

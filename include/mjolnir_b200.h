@@ -215,6 +215,19 @@ MJG_API int mjg_time_kernel(mjg_context* ctx, int term, int reps, double* ms_per
 MJG_API int mjg_set_threads_per_particle(mjg_context* ctx, int term, int tpp);
 MJG_API int mjg_get_threads_per_particle(mjg_context* ctx, int term, int* tpp);
 MJG_API int mjg_set_margin(mjg_context* ctx, int term, double margin);
+/* Partners a thread requests per batch in a global term's force launch (1, 2
+ * or 4): deeper batches keep more loads in flight per thread at the cost of
+ * registers.  A launch-shape knob like the threads per particle; it changes
+ * no result.  No counterpart in the reference. */
+MJG_API int mjg_set_pair_unroll(mjg_context* ctx, int term, int unroll);
+MJG_API int mjg_get_pair_unroll(mjg_context* ctx, int term, int* unroll);
+/* Schedule of a global term's force launch in the mixed form: 0 = one
+ * particle per group of threads-per-particle threads; 1 = warp-balanced, a
+ * warp splits the combined lists of its 32 particles evenly over its lanes
+ * and adds each partial sum with integer atomics (exact, so the forces are
+ * identical).  The FP64 form always uses 0.  No counterpart in the reference. */
+MJG_API int mjg_set_pair_schedule(mjg_context* ctx, int term, int schedule);
+MJG_API int mjg_get_pair_schedule(mjg_context* ctx, int term, int* schedule);
 /* Sets the per-particle neighbour capacity of a global term's lists.  A
  * capacity below what a later rebuild needs is detected on the device, the
  * current mjg_step chunk is rolled back, the lists grow and the chunk runs

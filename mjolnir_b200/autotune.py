@@ -4,8 +4,11 @@ For every global term of an :class:`~mjolnir_b200.engine.Engine` it picks
   * the relative margin (list radius cutoff * (1 + margin), hence the cell size
     and the rebuild interval) from a candidate set, by timing whole MD steps --
     a thinner skin makes shorter lists but more frequent rebuilds;
-  * the number of threads that cooperate on one particle's list in the pair
-    kernel (1, 2, 4, 8, 16), by timing the pair kernel alone.
+  * the pair kernel's launch shape, by timing the kernel alone: the schedule
+    (one particle per group of threads, or warp-balanced over the lists of a
+    warp's 32 particles; mixed form only), the threads per particle / list
+    layout (1, 2, 4, 8, 16) and the partners each thread requests per batch
+    (1, 2, 4).
 In the mixed form neither choice changes a result: the fixed-point force sums
 do not depend on list order or length.  The engine's systems keep stepping
 while the tuner measures (the tuning run is part of the warm-up).
@@ -27,7 +30,8 @@ def _time_steps(eng, nsteps: int) -> float:
 
 
 def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
-         tpps=(1, 2, 4, 8, 16), steps: int = 60, warm: int = 20, log=None) -> dict:
+         tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1), steps: int = 60,
+         warm: int = 20, log=None) -> dict:
     present = []
     for t in terms:
         try:
@@ -40,25 +44,53 @@ def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
         best = None
         for m in margins:
             eng.set_margin(t, m)
-            best_tpp = _tune_tpp(eng, t, tpps)
-            eng.set_threads_per_particle(t, best_tpp)
+            shape = _tune_shape(eng, t, tpps, unrolls, schedules if eng.precision == "mixed" else (0,))
+            _apply(eng, t, shape)
             eng.step(warm)
             ms = _time_steps(eng, steps)
             if log:
-                log(f"autotune {t}: margin {m} tpp {best_tpp}: {ms:.4f} ms/step")
+                log(f"autotune {t}: margin {m} schedule {shape[0]} tpp {shape[1]} unroll {shape[2]}: "
+                    f"{ms:.4f} ms/step")
             if best is None or ms < best[0]:
-                best = (ms, m, best_tpp)
+                best = (ms, m, shape)
         eng.set_margin(t, best[1])
-        eng.set_threads_per_particle(t, best[2])
-        choice[t] = {"margin": best[1], "threads_per_particle": best[2], "ms_per_step": best[0]}
+        _apply(eng, t, best[2])
+        choice[t] = {"margin": best[1], "schedule": best[2][0], "threads_per_particle": best[2][1],
+                     "unroll": best[2][2], "ms_per_step": best[0]}
     return choice
 
 
-def _tune_tpp(eng, term, tpps) -> int:
+def _apply(eng, term, shape):
+    eng.set_pair_schedule(term, shape[0])
+    eng.set_threads_per_particle(term, shape[1])
+    eng.set_pair_unroll(term, shape[2])
+
+
+def _tune_shape(eng, term, tpps, unrolls, schedules):
     best = None
-    for p in tpps:
-        eng.set_threads_per_particle(term, p)
-        ms = eng.time_kernel(term, reps=10)
-        if best is None or ms < best[0]:
-            best = (ms, p)
+    for sch in schedules:
+        eng.set_pair_schedule(term, sch)
+        for p in tpps:
+            eng.set_threads_per_particle(term, p)
+            for u in unrolls:
+                eng.set_pair_unroll(term, u)
+                ms = eng.time_kernel(term, reps=10)
+                if best is None or ms < best[0]:
+                    best = (ms, (sch, p, u))
     return best[1]
+
+
+def tune_shapes(eng, terms=("exv", "dh", "lj"), tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4),
+                schedules=(0, 1)) -> dict:
+    """Launch shape only (margins as committed): for a single large system,
+    where the margin is fixed by the input."""
+    out = {}
+    for t in terms:
+        try:
+            eng.get_threads_per_particle(t)
+        except Exception:
+            continue
+        shape = _tune_shape(eng, t, tpps, unrolls, schedules if eng.precision == "mixed" else (0,))
+        _apply(eng, t, shape)
+        out[t] = {"schedule": shape[0], "threads_per_particle": shape[1], "unroll": shape[2]}
+    return out

@@ -12,12 +12,17 @@
 #include "model.hpp"
 
 #include <atomic>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace mjg {
@@ -46,17 +51,31 @@ struct Error : std::runtime_error {
 // device buffer with byte accounting
 struct DevBuf {
     void* p = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0;            // size in use
+    size_t cap = 0;              // size allocated
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() {release();}
-    void release() {if(p) {cudaFree(p); p = nullptr; bytes = 0;}}
+    void release() {if(p) {cudaFree(p); p = nullptr;} bytes = 0; cap = 0;}
     void alloc(size_t b)
     {
         release();
         if(b == 0) {return;}
         CK(cudaMalloc(&p, b));
+        bytes = cap = b;
+    }
+    // keeps the allocation when it is large enough, else grows it with a
+    // quarter of headroom (arenas that are re-packed often change size)
+    void ensure(size_t b)
+    {
+        if(b > cap)
+        {
+            release();
+            const size_t want = b + b / 4;
+            CK(cudaMalloc(&p, want));
+            cap = want;
+        }
         bytes = b;
     }
     template<typename T> T* as() const {return static_cast<T*>(p);}
@@ -116,6 +135,8 @@ struct TermDev {
     int cap_alloc = 0;           // capacity the nbr buffer was sized for
     bool tpp_fixed = false;      // threads per slot chosen by the caller
     int tpp_choice = 1;          // ... and its value (kept across commits)
+    int unroll_choice = 1;       // partner batch depth of the force launch
+    int schedule_choice = 0;     // force launch schedule (0 slot per threads, 1 warp-balanced)
     TermArrays t{};
 };
 
@@ -128,6 +149,11 @@ struct mjg_context {
     bool graphs = true;
     bool rollback = true;
     cudaStream_t stream = nullptr;
+    // branches of the step: one per global term (rebuild, gather, force) and
+    // one for the bonded terms, forked from and joined back into `stream`
+    cudaStream_t side[mjg::NGLOBAL + 1] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[mjg::NGLOBAL + 1] = {};
     std::string err;
     std::vector<mjg::HostSystem> sys;
 
@@ -138,8 +164,10 @@ struct mjg_context {
     mjg::DevBuf d_sys, d_pos, d_vel, d_force, d_coef, d_psys, d_staging, d_mol;
     mjg::DevBuf b_sys, b_pos, b_vel, b_force;   // rollback copies
     mjg::DevBuf d_force_scratch;
-    double* h_pinned = nullptr;             // page-locked host staging (commit)
+    double* h_pinned = nullptr;             // page-locked host staging (state, forces)
     size_t h_pinned_bytes = 0;
+    void* h_pack = nullptr;                 // page-locked packing buffer of commit
+    size_t h_pack_bytes = 0;
     mjg::TermDev term[mjg::NGLOBAL];
     mjg::DevBuf l_bond_idx, l_bond_k, l_bond_v0, l_bond_sys;
     mjg::DevBuf l_angle_idx, l_angle_k, l_angle_v0, l_angle_sys;
@@ -170,7 +198,7 @@ int64_t device_bytes(const mjg_context* c)
                             &c->l_angle_sys, &c->l_dihd_idx, &c->l_dihd_k, &c->l_dihd_n,
                             &c->l_dihd_v0, &c->l_dihd_sys, &c->l_win_bond, &c->l_win_angle,
                             &c->l_win_dihd, &c->l_bond_kv, &c->l_angle_kv, &c->l_dihd_p};
-    for(auto* x : bufs) {b += (int64_t)x->bytes;}
+    for(auto* x : bufs) {b += (int64_t)x->cap;}
     for(const auto& t : c->term)
     {
         const DevBuf* tb[] = {&t.part_particle, &t.part_p0, &t.part_p1, &t.part_lead, &t.part_sys,
@@ -178,7 +206,7 @@ int64_t device_bytes(const mjg_context* c)
                               &t.work, &t.part_chunks, &t.cell_chunks, &t.flagged, &t.slot_part, &t.slot_particle, &t.slot_lead,
                               &t.slot_sys, &t.slot_pd, &t.slot_p1, &t.nnb, &t.nbr, &t.max_count,
                               &t.any_rebuild, &t.ex_start, &t.ex_idx};
-        for(auto* x : tb) {b += (int64_t)x->bytes;}
+        for(auto* x : tb) {b += (int64_t)x->cap;}
     }
     return b;
 }
@@ -225,14 +253,43 @@ void enqueue_forces(mjg_context* c, const Arena& a, bool nf, bool ne)
 
 // One integrator step without its closing half-kick.  kick: open with the
 // previous step's closing half-kick (fused into the same pass).
+// The step after the integrator's first pass forks into independent
+// branches: each global term rebuilds its lists (for the flagged systems),
+// refreshes its slot coordinates and, in the mixed form, adds its forces; the
+// bonded terms run beside them.  The mixed form's force launches add with
+// integer atomics (exact in any order), so all branches may overlap; the FP64
+// form adds its pair forces after the join, one term after the other, as the
+// reference does.
 void enqueue_step_body(mjg_context* c, bool kick)
 {
     const Arena& a = c->arena;
+    cudaStream_t st = c->stream;
     TermArrays ts[NGLOBAL] = {c->term[0].t, c->term[1].t, c->term[2].t};
-    launch_integrate_first(a, c->stream, kick);
-    launch_margin(a, ts, c->stream);
-    for(int g = 0; g < NGLOBAL; ++g) {launch_rebuild(a, g, c->term[g].t, 0, c->stream);}
-    enqueue_forces(c, a, true, false);
+    launch_integrate_first(a, st, kick);
+    launch_margin(a, ts, st);
+    const bool mixed = a.precision == P_MIXED;
+    CK(cudaEventRecord(c->ev_fork, st));
+    auto branch = [&](int b, auto&& body) {
+        CK(cudaStreamWaitEvent(c->side[b], c->ev_fork, 0));
+        body(c->side[b]);
+        CK(cudaEventRecord(c->ev_join[b], c->side[b]));
+        CK(cudaStreamWaitEvent(st, c->ev_join[b], 0));
+    };
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        TermArrays& t = c->term[g].t;
+        if(!t.on || t.np == 0) {continue;}
+        branch(g, [&](cudaStream_t s) {
+            launch_rebuild(a, g, t, 0, s);
+            launch_gather(a, t, s);
+            if(mixed) {launch_pair(a, g, t, true, false, 0, s, false);}
+        });
+    }
+    branch(NGLOBAL, [&](cudaStream_t s) {launch_local(a, c->local, 7, true, false, 0, s);});
+    if(!mixed)
+    {
+        for(int g = 0; g < NGLOBAL; ++g) {launch_pair(a, g, c->term[g].t, true, false, 0, st, false);}
+    }
 }
 
 
@@ -421,10 +478,15 @@ void derive(HostSystem& s)
     s.mol_local.assign(m.begin(), m.end());
     for(int g = 0; g < NGLOBAL; ++g)
     {
-        std::vector<std::pair<int, int>> kw;
-        for(const auto& w : s.g[g].within) {kw.emplace_back(kind_id(kinds, w.first), w.second);}
         s.ex_start_local[g].assign(1, 0);
         s.ex_idx_local[g].clear();
+        if(!s.g[g].on)                   // no participant of this term: empty lists
+        {
+            s.ex_start_local[g].assign((size_t)s.n + 1, 0);
+            continue;
+        }
+        std::vector<std::pair<int, int>> kw;
+        for(const auto& w : s.g[g].within) {kw.emplace_back(kind_id(kinds, w.first), w.second);}
         exclusion_csr(topo, s.n, kw, 0, s.ex_start_local[g], s.ex_idx_local[g]);
     }
     auto order = [](HostLocal& L, int arity) {
@@ -459,14 +521,210 @@ void derive(HostSystem& s)
     s.derived = true;
 }
 
+// runs fn(i) for i in [0, n) on up to 16 host threads (work handed out one
+// index at a time); the first exception thrown is rethrown here
+template<typename F>
+void parallel_for(int64_t n, F fn)
+{
+    const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+    const int nt = (int)std::min<int64_t>(std::min<int64_t>(hw, 16), n);
+    if(nt <= 1)
+    {
+        for(int64_t i = 0; i < n; ++i) {fn(i);}
+        return;
+    }
+    std::atomic<int64_t> next{0};
+    std::exception_ptr err;
+    std::mutex m;
+    auto work = [&]() {
+        try
+        {
+            for(int64_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {fn(i);}
+        }
+        catch(...)
+        {
+            std::lock_guard<std::mutex> l(m);
+            if(!err) {err = std::current_exception();}
+            next.store(n);
+        }
+    };
+    std::vector<std::thread> th;
+    for(int t = 1; t < nt; ++t) {th.emplace_back(work);}
+    work();
+    for(auto& t : th) {t.join();}
+    if(err) {std::rethrow_exception(err);}
+}
+
+// carves typed arrays out of the context's page-locked packing buffer
+struct Carver {
+    struct Item {size_t off, bytes;};
+    size_t total = 0;
+    template<typename T> Item add(size_t count)
+    {
+        Item it{total, sizeof(T) * count};
+        total += (it.bytes + 255) / 256 * 256;
+        return it;
+    }
+};
+
+// optional per-phase timing of a commit on stderr (MJG_TRACE=1)
+struct PhaseTimer {
+    bool on;
+    std::chrono::steady_clock::time_point t;
+    std::string line;
+    PhaseTimer() : on(std::getenv("MJG_TRACE") != nullptr), t(std::chrono::steady_clock::now()) {}
+    void mark(const char* what)
+    {
+        if(!on) {return;}
+        const auto now = std::chrono::steady_clock::now();
+        line += std::string(" ") + what + "=" +
+                std::to_string(std::chrono::duration<double, std::milli>(now - t).count()).substr(0, 7) + "ms";
+        t = now;
+    }
+    ~PhaseTimer() {if(on && !line.empty()) {std::fprintf(stderr, "mjg commit:%s\n", line.c_str());}}
+};
+
+// the cell grid of term g of system s (host side of the rebuild)
+void cell_grid(const HostSystem& s, const SysDev& d, int g, GlobalParams& G)
+{
+    const HostGlobal& H = s.g[g];
+    const int64_t np = (int64_t)H.idx.size();
+    if(s.boundary == B_PERIODIC)
+    {
+        // PeriodicGridCellList::set_cutoff / initialize (:67-96, :383-395)
+        const double r = 1.0 / (G.cutoff * (1.0 + G.margin) + 1e-6);
+        long long dims[3];
+        for(int x = 0; x < 3; ++x) {dims[x] = std::max<long long>(3, (long long)std::floor(d.width[x] * r));}
+        // keep the grid within a few cells per participant (wider cells stay exact)
+        const long long limit = std::max<long long>(27, 8 * np + 64);
+        while(dims[0] * dims[1] * dims[2] > limit)
+        {
+            int big = 0;
+            for(int x = 1; x < 3; ++x) {if(dims[x] > dims[big]) {big = x;}}
+            if(dims[big] <= 3) {break;}
+            dims[big] -= 1;
+        }
+        for(int x = 0; x < 3; ++x)
+        {
+            G.dims[x] = (int)dims[x];
+            G.inv_w[x] = 1.0 / (d.width[x] / (double)dims[x]);
+            G.origin[x] = d.lower[x];
+        }
+        G.hashed = 0;
+    }
+    else
+    {
+        // unbounded space: cells of cutoff (1 + margin)(1 + 1e-6) hashed
+        // modulo a grid sized to the system's current extent
+        const double w = G.cutoff * (1 + G.margin) * (1 + 1e-6);
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for(int64_t q = 0; q < np; ++q)
+        {
+            const int64_t i = H.idx[q];
+            for(int x = 0; x < 3; ++x)
+            {
+                lo[x] = std::min(lo[x], s.pos[3 * i + x]);
+                hi[x] = std::max(hi[x], s.pos[3 * i + x]);
+            }
+        }
+        long long dims[3];
+        for(int x = 0; x < 3; ++x)
+        {
+            const double ext = np > 0 ? hi[x] - lo[x] : 0.0;
+            dims[x] = std::max<long long>(3, (long long)std::floor(ext / w) + 3);
+        }
+        const long long limit = std::max<long long>(27, 2 * np + 64);
+        while(dims[0] * dims[1] * dims[2] > limit)
+        {
+            int big = 0;
+            for(int x = 1; x < 3; ++x) {if(dims[x] > dims[big]) {big = x;}}
+            if(dims[big] <= 3) {break;}
+            dims[big] -= 1;
+        }
+        for(int x = 0; x < 3; ++x)
+        {
+            G.dims[x] = (int)dims[x];
+            G.inv_w[x] = 1.0 / w;
+            G.origin[x] = 0.0;
+        }
+        G.hashed = 1;
+    }
+    G.ncell = G.dims[0] * G.dims[1] * G.dims[2];
+}
+
+// the per-system device record: box, counters and the constants of every
+// global term (potential parameters, list radius, cell grid)
+void make_sysdev(const HostSystem& s, SysDev& d)
+{
+    std::memset(&d, 0, sizeof(SysDev));
+    d.off = s.off; d.n = s.n;
+    d.boundary = s.boundary;
+    d.integrator = s.integrator;
+    for(int x = 0; x < 3; ++x)
+    {
+        d.lower[x] = s.lower[x]; d.upper[x] = s.upper[x];
+        d.width[x] = s.upper[x] - s.lower[x];
+        d.halfw[x] = d.width[x] / 2;
+    }
+    d.seed = s.seed;
+    d.step = s.step;
+    d.frozen = s.frozen ? 1 : 0;
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        const HostGlobal& H = s.g[g];
+        GlobalParams& G = d.g[g];
+        if(!H.on) {continue;}
+        G.on = 1;
+        G.margin = H.margin;
+        G.cutoff_ratio = H.cutoff_ratio;
+        G.cutoff_ratio_sq = H.cutoff_ratio * H.cutoff_ratio;
+        G.ignore_mol = H.ignore_mol;
+        G.eps = H.eps;
+        const int64_t np = (int64_t)H.idx.size();
+        if(g == G_EXV)             // ExcludedVolumePotential.hpp:44-48,92-106
+        {
+            G.coef_at_cutoff = std::pow(1.0 / H.cutoff_ratio, 12);
+            double mr = 0;
+            for(double r : H.p0) {mr = std::max(mr, r);}
+            G.cutoff = np == 0 ? 1.0 : mr * 2 * H.cutoff_ratio;
+        }
+        else if(g == G_DH)         // DebyeHuckelPotential.hpp:126-167,245-248
+        {
+            const DHParams p = dh_params(s.T, s.I, H.cutoff_ratio);
+            G.debye = p.debye; G.inv_debye = p.inv_debye; G.abs_cutoff = p.abs_cutoff;
+            G.coef_at_cutoff = p.coef_at_cutoff; G.inv4pi = p.inv4pi;
+            G.cutoff = p.debye * H.cutoff_ratio;
+        }
+        else                       // LennardJonesPotential.hpp:36-41,75-91
+        {
+            G.coef_at_cutoff = std::pow(1.0 / H.cutoff_ratio, 12) - std::pow(1.0 / H.cutoff_ratio, 6);
+            double ms = 0;
+            for(double x : H.p0) {ms = std::max(ms, x);}
+            G.cutoff = np == 0 ? 1.0 : ms * H.cutoff_ratio;
+        }
+        const double r_c = G.cutoff * (1. + G.margin);
+        G.rl2 = r_c * r_c;
+        G.current_margin = G.cutoff * G.margin;
+        G.rebuild = 1;
+        G.rebuilds = s.rebuilds[g];
+        G.nslot = (int)np;
+        cell_grid(s, d, g, G);
+    }
+}
+
+// Packs every live system into one arena and uploads it.  Systems keep their
+// state (positions, velocities, exact forces, step counters) across commits.
+// The host work runs in parallel over systems into one page-locked buffer,
+// from which each device array is filled by a single copy.
 void commit(mjg_context* c)
 {
+    PhaseTimer tm;
     CK(cudaSetDevice(c->device));
     save_resident_state(c);
+    tm.mark("save");
     release_graph(c);
     for(auto& s : c->sys) {s.resident = false; s.arena_slot = -1;}
 
-    // ---- host packing
     std::vector<int> ids;
     for(int i = 0; i < (int)c->sys.size(); ++i)
     {
@@ -478,51 +736,100 @@ void commit(mjg_context* c)
         }
         ids.push_back(i);
     }
-    const Units u;
+    const int nsys = (int)ids.size();
+    parallel_for(nsys, [&](int64_t k) {derive(c->sys[ids[k]]);});
+    tm.mark("derive");
+
+    // ---- offsets (serial, per system)
     long long n_tot = 0;
     for(int id : ids) {c->sys[id].off = n_tot; n_tot += c->sys[id].n;}
-    const int nsys = (int)ids.size();
-
-    std::vector<double4> pos(n_tot), vel(n_tot), coef(n_tot);
-    std::vector<int> psys(n_tot), mol(n_tot);
     std::vector<SysDev> hs(nsys);
-    std::vector<long long> ex_start[NGLOBAL];
-    std::vector<int> ex_idx[NGLOBAL];
-    for(int g = 0; g < NGLOBAL; ++g) {ex_start[g].push_back(0);}
-
-    // per term participant data
-    std::vector<int> part_particle[NGLOBAL], part_sys[NGLOBAL];
+    parallel_for(nsys, [&](int64_t k) {make_sysdev(c->sys[ids[k]], hs[k]);});
+    std::vector<long long> mol_base(nsys + 1, 0), ex_off[NGLOBAL], b_off(nsys + 1, 0), a_off(nsys + 1, 0),
+                           d_off(nsys + 1, 0);
+    long long np_tot[NGLOBAL] = {0, 0, 0}, ncell[NGLOBAL] = {0, 0, 0};
     long long part_chunk_cap[NGLOBAL] = {0, 0, 0}, cell_chunk_cap[NGLOBAL] = {0, 0, 0};
-    std::vector<double> part_p0[NGLOBAL], part_p1[NGLOBAL];
-    std::vector<unsigned char> part_lead[NGLOBAL];
-    int ncell[NGLOBAL] = {0, 0, 0};
-
-    // local terms
-    std::vector<int> b_idx, b_sys, a_idx, a_sys, d_idx, d_sys, d_n;
-    std::vector<double> b_k, b_v0, a_k, a_v0, d_k, d_v0;
-
-    long long mol_base = 0;
+    for(int g = 0; g < NGLOBAL; ++g) {ex_off[g].assign(nsys + 1, 0);}
     for(int k = 0; k < nsys; ++k)
     {
         HostSystem& s = c->sys[ids[k]];
         s.resident = true;
         s.arena_slot = k;
-        SysDev& d = hs[k];
-        std::memset(&d, 0, sizeof(SysDev));
-        d.off = s.off; d.n = s.n;
-        d.boundary = s.boundary;
-        d.integrator = s.integrator;
-        for(int x = 0; x < 3; ++x)
+        int64_t nmol = 0;
+        for(const int32_t m : s.mol_local) {nmol = std::max<int64_t>(nmol, (int64_t)m + 1);}
+        mol_base[k + 1] = mol_base[k] + nmol;
+        for(int g = 0; g < NGLOBAL; ++g)
         {
-            d.lower[x] = s.lower[x]; d.upper[x] = s.upper[x];
-            d.width[x] = s.upper[x] - s.lower[x];
-            d.halfw[x] = d.width[x] / 2;
+            ex_off[g][k + 1] = ex_off[g][k] + (long long)s.ex_idx_local[g].size();
+            GlobalParams& G = hs[k].g[g];
+            if(!G.on) {continue;}
+            G.slot_off = (int)np_tot[g];
+            G.cell_off = (int)ncell[g];
+            np_tot[g] += G.nslot;
+            ncell[g] += G.ncell;
+            cell_chunk_cap[g] += (G.ncell + 255) / 256;
+            part_chunk_cap[g] += (G.nslot + 255) / 256;
         }
-        d.seed = s.seed;
-        d.step = s.step;
-        d.frozen = s.frozen ? 1 : 0;
+        b_off[k + 1] = b_off[k] + s.bond.m();
+        a_off[k + 1] = a_off[k] + s.angle.m();
+        d_off[k + 1] = d_off[k] + s.dihd.m();
+    }
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        if(np_tot[g] > INT32_MAX || ncell[g] > INT32_MAX) {throw Error(MJG_EINVAL, "arena too large");}
+    }
+    const long long nb = b_off[nsys], na = a_off[nsys], nd = d_off[nsys];
+    const int nwin = (int)((n_tot + 255) / 256);
 
-        // particles
+    // ---- layout of the page-locked packing buffer
+    Carver cv;
+    const auto c_pos = cv.add<double4>(n_tot), c_vel = cv.add<double4>(n_tot), c_coef = cv.add<double4>(n_tot);
+    const auto c_psys = cv.add<int>(n_tot), c_mol = cv.add<int>(n_tot);
+    Carver::Item c_exs[NGLOBAL], c_exi[NGLOBAL], c_pp[NGLOBAL], c_ps[NGLOBAL], c_p0[NGLOBAL], c_p1[NGLOBAL],
+                 c_pl[NGLOBAL];
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        c_exs[g] = cv.add<long long>(n_tot + 1);
+        c_exi[g] = cv.add<int>(std::max<long long>(1, ex_off[g][nsys]));
+        c_pp[g] = cv.add<int>(np_tot[g]);
+        c_ps[g] = cv.add<int>(np_tot[g]);
+        c_p0[g] = cv.add<double>(np_tot[g]);
+        c_p1[g] = cv.add<double>(np_tot[g]);
+        c_pl[g] = cv.add<unsigned char>(np_tot[g]);
+    }
+    const auto c_bidx = cv.add<int>(2 * nb), c_bk = cv.add<double>(nb), c_bv0 = cv.add<double>(nb),
+               c_bsys = cv.add<int>(nb), c_bkv = cv.add<float2>(nb);
+    const auto c_aidx = cv.add<int>(3 * na), c_ak = cv.add<double>(na), c_av0 = cv.add<double>(na),
+               c_asys = cv.add<int>(na), c_akv = cv.add<float2>(na);
+    const auto c_didx = cv.add<int>(4 * nd), c_dk = cv.add<double>(nd), c_dv0 = cv.add<double>(nd),
+               c_dsys = cv.add<int>(nd), c_dn = cv.add<int>(nd), c_dp = cv.add<float4>(nd);
+    const auto c_wb = cv.add<long long>(nwin + 1), c_wa = cv.add<long long>(nwin + 1),
+               c_wd = cv.add<long long>(nwin + 1);
+    if(cv.total > c->h_pack_bytes)
+    {
+        if(c->h_pack) {cudaFreeHost(c->h_pack); c->h_pack = nullptr; c->h_pack_bytes = 0;}
+        const size_t want = cv.total + cv.total / 4;
+        CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_pack), want));
+        c->h_pack_bytes = want;
+    }
+    char* hb = static_cast<char*>(c->h_pack);
+    auto at = [&](const Carver::Item& it) {return hb + it.off;};
+    double4* pos = (double4*)at(c_pos); double4* vel = (double4*)at(c_vel); double4* coef = (double4*)at(c_coef);
+    int* psys = (int*)at(c_psys); int* mol = (int*)at(c_mol);
+    int* b_idx = (int*)at(c_bidx); double* b_k = (double*)at(c_bk); double* b_v0 = (double*)at(c_bv0);
+    int* b_sys = (int*)at(c_bsys); float2* b_kv = (float2*)at(c_bkv);
+    int* a_idx = (int*)at(c_aidx); double* a_k = (double*)at(c_ak); double* a_v0 = (double*)at(c_av0);
+    int* a_sys = (int*)at(c_asys); float2* a_kv = (float2*)at(c_akv);
+    int* d_idx = (int*)at(c_didx); double* d_k = (double*)at(c_dk); double* d_v0 = (double*)at(c_dv0);
+    int* d_sys = (int*)at(c_dsys); int* d_n = (int*)at(c_dn); float4* d_p = (float4*)at(c_dp);
+    tm.mark("layout");
+
+    // ---- fill (parallel over systems)
+    const Units u;
+    parallel_for(nsys, [&](int64_t k) {
+        const HostSystem& s = c->sys[ids[k]];
+        const SysDev& d = hs[k];
+        const long long off = s.off;
         const double halfdt = s.dt / 2;
         const double kBT = u.kB * s.T;
         for(int64_t i = 0; i < s.n; ++i)
@@ -536,7 +843,7 @@ void commit(mjg_context* c)
                     else if(p[x] >= d.upper[x]) {p[x] -= d.width[x];}
                 }
             }
-            const long long gi = s.off + i;
+            const long long gi = off + i;
             pos[gi] = make_double4(p[0], p[1], p[2], 0.0);
             vel[gi] = make_double4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], 0.0);
             const double rmass = 1.0 / s.mass[i];
@@ -550,184 +857,111 @@ void commit(mjg_context* c)
             {
                 coef[gi] = make_double4(halfdt * rmass, 1.0, 0.0, s.dt);
             }
-            psys[gi] = k;
+            psys[gi] = (int)k;
+            mol[gi] = (int)(mol_base[k] + s.mol_local[i]);
         }
-
-        // topology-derived data, computed at the system's first commit
-        derive(s);
-        int64_t nmol = 0;
-        for(int64_t i = 0; i < s.n; ++i)
-        {
-            mol[s.off + i] = (int)(mol_base + s.mol_local[i]);
-            nmol = std::max<int64_t>(nmol, s.mol_local[i] + 1);
-        }
-        mol_base += nmol;
-
-        // global terms
         for(int g = 0; g < NGLOBAL; ++g)
         {
+            long long* exs = (long long*)at(c_exs[g]);
+            int* exi = (int*)at(c_exi[g]);
+            const long long base = ex_off[g][k];
+            const std::vector<long long>& ls = s.ex_start_local[g];
+            if(k == 0) {exs[0] = 0;}
+            for(int64_t i = 1; i <= s.n; ++i) {exs[off + i] = base + ls[i];}
+            const std::vector<int>& li = s.ex_idx_local[g];
+            for(size_t j = 0; j < li.size(); ++j) {exi[base + j] = (int)(li[j] + off);}
+            const GlobalParams& G = d.g[g];
+            if(!G.on) {continue;}
             const HostGlobal& H = s.g[g];
-            GlobalParams& G = d.g[g];
-            {
-                const long long base = (long long)ex_idx[g].size();
-                const std::vector<long long>& ls = s.ex_start_local[g];
-                for(int64_t i = 1; i <= s.n; ++i) {ex_start[g].push_back(base + ls[i]);}
-                for(const int j : s.ex_idx_local[g]) {ex_idx[g].push_back((int)(j + s.off));}
-            }
-            if(!H.on) {continue;}
-            G.on = 1;
-            G.margin = H.margin;
-            G.cutoff_ratio = H.cutoff_ratio;
-            G.cutoff_ratio_sq = H.cutoff_ratio * H.cutoff_ratio;
-            G.ignore_mol = H.ignore_mol;
-            G.eps = H.eps;
-            const int64_t np = (int64_t)H.idx.size();
-            if(g == G_EXV)             // ExcludedVolumePotential.hpp:44-48,92-106
-            {
-                G.coef_at_cutoff = std::pow(1.0 / H.cutoff_ratio, 12);
-                double mr = 0;
-                for(double r : H.p0) {mr = std::max(mr, r);}
-                G.cutoff = np == 0 ? 1.0 : mr * 2 * H.cutoff_ratio;
-            }
-            else if(g == G_DH)         // DebyeHuckelPotential.hpp:126-167,245-248
-            {
-                const DHParams p = dh_params(s.T, s.I, H.cutoff_ratio);
-                G.debye = p.debye; G.inv_debye = p.inv_debye; G.abs_cutoff = p.abs_cutoff;
-                G.coef_at_cutoff = p.coef_at_cutoff; G.inv4pi = p.inv4pi;
-                G.cutoff = p.debye * H.cutoff_ratio;
-            }
-            else                       // LennardJonesPotential.hpp:36-41,75-91
-            {
-                G.coef_at_cutoff = std::pow(1.0 / H.cutoff_ratio, 12) - std::pow(1.0 / H.cutoff_ratio, 6);
-                double ms = 0;
-                for(double x : H.p0) {ms = std::max(ms, x);}
-                G.cutoff = np == 0 ? 1.0 : ms * H.cutoff_ratio;
-            }
-            const double r_c = G.cutoff * (1. + G.margin);
-            G.rl2 = r_c * r_c;
-            G.current_margin = G.cutoff * G.margin;
-            G.rebuild = 1;
-            G.rebuilds = s.rebuilds[g];
-
-            // cell grid
-            if(s.boundary == B_PERIODIC)
-            {
-                // PeriodicGridCellList::set_cutoff / initialize (:67-96, :383-395)
-                const double r = 1.0 / (G.cutoff * (1.0 + G.margin) + 1e-6);
-                long long dims[3];
-                for(int x = 0; x < 3; ++x) {dims[x] = std::max<long long>(3, (long long)std::floor(d.width[x] * r));}
-                // keep the grid within a few cells per participant (wider cells stay exact)
-                const long long limit = std::max<long long>(27, 8 * np + 64);
-                while(dims[0] * dims[1] * dims[2] > limit)
-                {
-                    int big = 0;
-                    for(int x = 1; x < 3; ++x) {if(dims[x] > dims[big]) {big = x;}}
-                    if(dims[big] <= 3) {break;}
-                    dims[big] -= 1;
-                }
-                for(int x = 0; x < 3; ++x)
-                {
-                    G.dims[x] = (int)dims[x];
-                    G.inv_w[x] = 1.0 / (d.width[x] / (double)dims[x]);
-                    G.origin[x] = d.lower[x];
-                }
-                G.hashed = 0;
-            }
-            else
-            {
-                // unbounded space: cells of cutoff (1 + margin)(1 + 1e-6) hashed
-                // modulo a grid sized to the system's current extent
-                const double w = G.cutoff * (1 + G.margin) * (1 + 1e-6);
-                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-                for(int64_t q = 0; q < np; ++q)
-                {
-                    const int64_t i = H.idx[q];
-                    for(int x = 0; x < 3; ++x)
-                    {
-                        lo[x] = std::min(lo[x], s.pos[3 * i + x]);
-                        hi[x] = std::max(hi[x], s.pos[3 * i + x]);
-                    }
-                }
-                long long dims[3];
-                for(int x = 0; x < 3; ++x)
-                {
-                    const double ext = np > 0 ? hi[x] - lo[x] : 0.0;
-                    dims[x] = std::max<long long>(3, (long long)std::floor(ext / w) + 3);
-                }
-                const long long limit = std::max<long long>(27, 2 * np + 64);
-                while(dims[0] * dims[1] * dims[2] > limit)
-                {
-                    int big = 0;
-                    for(int x = 1; x < 3; ++x) {if(dims[x] > dims[big]) {big = x;}}
-                    if(dims[big] <= 3) {break;}
-                    dims[big] -= 1;
-                }
-                for(int x = 0; x < 3; ++x)
-                {
-                    G.dims[x] = (int)dims[x];
-                    G.inv_w[x] = 1.0 / w;
-                    G.origin[x] = 0.0;
-                }
-                G.hashed = 1;
-            }
-            G.ncell = G.dims[0] * G.dims[1] * G.dims[2];
-            G.cell_off = ncell[g];
-            ncell[g] += G.ncell;
-            cell_chunk_cap[g] += (G.ncell + 255) / 256;
-            part_chunk_cap[g] += (np + 255) / 256;
-            G.slot_off = (int)part_particle[g].size();
-            G.nslot = (int)np;
+            int* pp = (int*)at(c_pp[g]); int* ps = (int*)at(c_ps[g]);
+            double* p0 = (double*)at(c_p0[g]); double* p1 = (double*)at(c_p1[g]);
+            unsigned char* pl = (unsigned char*)at(c_pl[g]);
+            const int64_t np = G.nslot;
             for(int64_t q = 0; q < np; ++q)
             {
-                part_particle[g].push_back((int)(s.off + H.idx[q]));
-                part_sys[g].push_back(k);
-                part_p0[g].push_back(H.p0[q]);
-                part_p1[g].push_back(H.p1.empty() ? 0.0 : H.p1[q]);
-                part_lead[g].push_back(q + 1 < np ? 1 : 0);
+                const int64_t x = G.slot_off + q;
+                pp[x] = (int)(off + H.idx[q]);
+                ps[x] = (int)k;
+                p0[x] = H.p0[q];
+                p1[x] = H.p1.empty() ? 0.0 : H.p1[q];
+                pl[x] = q + 1 < np ? 1 : 0;
             }
         }
-
-        // local terms
         for(int64_t t = 0; t < s.bond.m(); ++t)
         {
-            b_idx.push_back((int)(s.off + s.bond.idx[2 * t]));
-            b_idx.push_back((int)(s.off + s.bond.idx[2 * t + 1]));
-            b_k.push_back(s.bond.k[t]); b_v0.push_back(s.bond.v0[t]); b_sys.push_back(k);
+            const long long x = b_off[k] + t;
+            b_idx[2 * x] = (int)(off + s.bond.idx[2 * t]);
+            b_idx[2 * x + 1] = (int)(off + s.bond.idx[2 * t + 1]);
+            b_k[x] = s.bond.k[t]; b_v0[x] = s.bond.v0[t]; b_sys[x] = (int)k;
+            b_kv[x] = make_float2((float)s.bond.k[t], (float)s.bond.v0[t]);
         }
         for(int64_t t = 0; t < s.angle.m(); ++t)
         {
-            for(int x = 0; x < 3; ++x) {a_idx.push_back((int)(s.off + s.angle.idx[3 * t + x]));}
-            a_k.push_back(s.angle.k[t]); a_v0.push_back(s.angle.v0[t]); a_sys.push_back(k);
+            const long long x = a_off[k] + t;
+            for(int y = 0; y < 3; ++y) {a_idx[3 * x + y] = (int)(off + s.angle.idx[3 * t + y]);}
+            a_k[x] = s.angle.k[t]; a_v0[x] = s.angle.v0[t]; a_sys[x] = (int)k;
+            a_kv[x] = make_float2((float)s.angle.k[t], (float)s.angle.v0[t]);
         }
         for(int64_t t = 0; t < s.dihd.m(); ++t)
         {
-            for(int x = 0; x < 4; ++x) {d_idx.push_back((int)(s.off + s.dihd.idx[4 * t + x]));}
-            d_k.push_back(s.dihd.k[t]); d_v0.push_back(s.dihd.v0[t]); d_n.push_back(s.dihd.n[t]);
-            d_sys.push_back(k);
+            const long long x = d_off[k] + t;
+            for(int y = 0; y < 4; ++y) {d_idx[4 * x + y] = (int)(off + s.dihd.idx[4 * t + y]);}
+            d_k[x] = s.dihd.k[t]; d_v0[x] = s.dihd.v0[t]; d_n[x] = s.dihd.n[t]; d_sys[x] = (int)k;
+            const double nv = (double)s.dihd.n[t] * s.dihd.v0[t];
+            d_p[x] = make_float4((float)s.dihd.k[t], (float)std::cos(nv), (float)std::sin(nv),
+                                 (float)s.dihd.n[t]);
         }
+    });
+    if(nsys == 0)
+    {
+        for(int g = 0; g < NGLOBAL; ++g) {((long long*)at(c_exs[g]))[0] = 0;}
     }
+    // local terms: every system keeps its terms ordered by their smallest
+    // particle and systems are packed in order, so the arena's terms are in
+    // order too; CSR of terms over 256-particle windows
+    auto windows = [&](const int* idx, int arity, long long m, long long* win) {
+        std::fill(win, win + nwin + 1, 0LL);
+        int prev = 0;
+        for(long long t = 0; t < m; ++t)
+        {
+            int mn = idx[arity * t];
+            for(int x = 1; x < arity; ++x) {mn = std::min(mn, idx[arity * t + x]);}
+            if(mn < prev) {throw Error(MJG_ESTATE, "local terms out of order");}
+            prev = mn;
+            win[mn / 256 + 1] += 1;
+        }
+        for(int w = 0; w < nwin; ++w) {win[w + 1] += win[w];}
+    };
+    windows(b_idx, 2, nb, (long long*)at(c_wb));
+    windows(a_idx, 3, na, (long long*)at(c_wa));
+    windows(d_idx, 4, nd, (long long*)at(c_wd));
+    tm.mark("fill");
 
-    // ---- device upload
+    // ---- device upload (buffers keep their capacity across commits)
     cudaStream_t st = c->stream;
+    auto put = [&](DevBuf& dst, const Carver::Item& it) {
+        dst.ensure(it.bytes);
+        if(it.bytes) {CK(cudaMemcpyAsync(dst.p, at(it), it.bytes, cudaMemcpyHostToDevice, st));}
+    };
     c->n_tot = n_tot;
     c->arena_ids = ids;
     c->h_sys = hs;
-    c->d_sys.alloc(sizeof(SysDev) * std::max(nsys, 1));
+    c->d_sys.ensure(sizeof(SysDev) * std::max(nsys, 1));
     upload_sys(c);
-    upload(c->d_pos, pos, st);
-    upload(c->d_vel, vel, st);
-    upload(c->d_coef, coef, st);
-    upload(c->d_psys, psys, st);
-    upload(c->d_mol, mol, st);
-    c->d_force.alloc(32 * (size_t)std::max<long long>(n_tot, 1));
-    c->d_force_scratch.alloc(32 * (size_t)std::max<long long>(n_tot, 1));
-    c->d_staging.alloc(sizeof(double) * 3 * (size_t)std::max<long long>(n_tot, 1));
+    put(c->d_pos, c_pos);
+    put(c->d_vel, c_vel);
+    put(c->d_coef, c_coef);
+    put(c->d_psys, c_psys);
+    put(c->d_mol, c_mol);
+    c->d_force.ensure(32 * (size_t)std::max<long long>(n_tot, 1));
+    c->d_force_scratch.ensure(32 * (size_t)std::max<long long>(n_tot, 1));
+    c->d_staging.ensure(sizeof(double) * 3 * (size_t)std::max<long long>(n_tot, 1));
     if(c->rollback)
     {
-        c->b_sys.alloc(c->d_sys.bytes);
-        c->b_pos.alloc(c->d_pos.bytes);
-        c->b_vel.alloc(c->d_vel.bytes);
-        c->b_force.alloc(c->d_force.bytes);
+        c->b_sys.ensure(c->d_sys.bytes);
+        c->b_pos.ensure(c->d_pos.bytes);
+        c->b_vel.ensure(c->d_vel.bytes);
+        c->b_force.ensure(c->d_force.bytes);
     }
     else
     {
@@ -751,18 +985,18 @@ void commit(mjg_context* c)
     for(int g = 0; g < NGLOBAL; ++g)
     {
         TermDev& T = c->term[g];
-        upload(T.ex_start, ex_start[g], st);
-        if(ex_idx[g].empty()) {ex_idx[g].push_back(0);}
-        upload(T.ex_idx, ex_idx[g], st);
+        put(T.ex_start, c_exs[g]);
+        put(T.ex_idx, c_exi[g]);
         a.ex_start[g] = T.ex_start.as<long long>();
         a.ex_idx[g] = T.ex_idx.as<int>();
 
         TermArrays& t = T.t;
+        const int prev_tpp = t.tpp > 0 ? t.tpp : 1;
         t = TermArrays{};
-        const long long np = (long long)part_particle[g].size();
+        const long long np = np_tot[g];
         t.on = np > 0 ? 1 : 0;
         t.np = np;
-        t.ncell = ncell[g];
+        t.ncell = (int)ncell[g];
         if(!t.on)
         {
             DevBuf* bufs[] = {&T.part_particle, &T.part_p0, &T.part_p1, &T.part_lead, &T.part_sys,
@@ -771,40 +1005,41 @@ void commit(mjg_context* c)
                               &T.slot_sys, &T.slot_pd, &T.slot_p1, &T.nnb, &T.nbr,
                               &T.max_count, &T.any_rebuild};
             for(auto* b : bufs) {b->release();}
+            T.cap_alloc = 0;
             continue;
         }
-        upload(T.part_particle, part_particle[g], st);
-        upload(T.part_p0, part_p0[g], st);
-        upload(T.part_p1, part_p1[g], st);
-        upload(T.part_lead, part_lead[g], st);
-        upload(T.part_sys, part_sys[g], st);
-        T.part_cell.alloc(sizeof(int) * np);
-        T.cell_count.alloc(sizeof(int) * t.ncell);
-        T.cell_fill.alloc(sizeof(int) * t.ncell);
-        T.cell_start.alloc(sizeof(int) * (t.ncell + 1));
+        put(T.part_particle, c_pp[g]);
+        put(T.part_p0, c_p0[g]);
+        put(T.part_p1, c_p1[g]);
+        put(T.part_lead, c_pl[g]);
+        put(T.part_sys, c_ps[g]);
+        T.part_cell.ensure(sizeof(int) * np);
+        T.cell_count.ensure(sizeof(int) * t.ncell);
+        T.cell_fill.ensure(sizeof(int) * t.ncell);
+        T.cell_start.ensure(sizeof(int) * (t.ncell + 1));
         // rebuild work lists (sized for every system flagged at once)
-        T.work.alloc(sizeof(int) * 4);
+        T.work.ensure(sizeof(int) * 4);
         CK(cudaMemsetAsync(T.work.p, 0, T.work.bytes, st));
-        T.part_chunks.alloc(sizeof(int4) * std::max<long long>(1, part_chunk_cap[g]));
-        T.cell_chunks.alloc(sizeof(int4) * std::max<long long>(1, cell_chunk_cap[g]));
-        T.flagged.alloc(sizeof(int) * std::max(1, nsys));
+        T.part_chunks.ensure(sizeof(int4) * std::max<long long>(1, part_chunk_cap[g]));
+        T.cell_chunks.ensure(sizeof(int4) * std::max<long long>(1, cell_chunk_cap[g]));
+        T.flagged.ensure(sizeof(int) * std::max(1, nsys));
         {
-            std::vector<int> last(1, (int)np);   // cell_start[ncell] = total slots
-            CK(cudaMemcpyAsync(T.cell_start.as<int>() + t.ncell, last.data(), sizeof(int),
+            const int last = (int)np;        // cell_start[ncell] = total slots
+            CK(cudaMemcpyAsync(T.cell_start.as<int>() + t.ncell, &last, sizeof(int),
                                cudaMemcpyHostToDevice, st));
             CK(cudaStreamSynchronize(st));
         }
         CK(cudaMemsetAsync(T.cell_count.p, 0, T.cell_count.bytes, st));
         CK(cudaMemsetAsync(T.cell_fill.p, 0, T.cell_fill.bytes, st));
-        T.slot_part.alloc(sizeof(int) * np);
-        T.slot_particle.alloc(sizeof(int) * np);
-        T.slot_lead.alloc(np);
-        T.slot_sys.alloc(sizeof(int) * np);
-        T.slot_pd.alloc(sizeof(double4) * np);
-        T.slot_p1.alloc(sizeof(double) * np);
-        T.nnb.alloc(sizeof(int) * np);
-        T.max_count.alloc(sizeof(int));
-        T.any_rebuild.alloc(sizeof(int));
+        T.slot_part.ensure(sizeof(int) * np);
+        T.slot_particle.ensure(sizeof(int) * np);
+        T.slot_lead.ensure(np);
+        T.slot_sys.ensure(sizeof(int) * np);
+        T.slot_pd.ensure(sizeof(double4) * np);
+        T.slot_p1.ensure(sizeof(double) * np);
+        T.nnb.ensure(sizeof(int) * np);
+        T.max_count.ensure(sizeof(int));
+        T.any_rebuild.ensure(sizeof(int));
         CK(cudaMemsetAsync(T.any_rebuild.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(T.nnb.p, 0, T.nnb.bytes, st));
         t.part_particle = T.part_particle.as<int>();
@@ -829,86 +1064,44 @@ void commit(mjg_context* c)
         t.nnb = T.nnb.as<int>();
         t.max_count = T.max_count.as<int>();
         t.any_rebuild = T.any_rebuild.as<int>();
-        t.cap = 0;
         t.tpp = T.tpp_fixed ? T.tpp_choice : 1;
+        t.unroll = T.unroll_choice;
+        t.schedule = T.schedule_choice;
         t.any_periodic = 0;
         for(int id : ids)
         {
             if(c->sys[id].g[g].on && c->sys[id].boundary == B_PERIODIC) {t.any_periodic = 1;}
         }
-        T.nbr.release();
-        t.nbr = nullptr;
-        alloc_lists(c, g, 0);
+        // keep the list capacity of the previous arena when the buffer still
+        // holds it; rebuild_all grows it where needed
+        const int keep = T.cap_alloc;
+        if(keep > 0 && T.nbr.cap >= sizeof(int) * (size_t)keep * (size_t)np)
+        {
+            T.nbr.bytes = sizeof(int) * (size_t)keep * (size_t)np;
+            t.nbr = T.nbr.as<int>();
+            t.cap = keep;
+            if(!T.tpp_fixed) {t.tpp = prev_tpp;}
+        }
+        else
+        {
+            t.nbr = nullptr;
+            t.cap = 0;
+            alloc_lists(c, g, 0);
+        }
     }
 
-    // local: terms sorted by their smallest particle, CSR over 256-particle windows
-    const int nwin = (int)((n_tot + 255) / 256);
-    auto sort_terms = [&](std::vector<int>& idx, int arity, std::vector<double>& kk,
-                          std::vector<double>& v0, std::vector<int>& sysv, std::vector<int>* nn,
-                          std::vector<long long>& win) {
-        const size_t m = kk.size();
-        std::vector<int> key(m);
-        for(size_t t = 0; t < m; ++t)
-        {
-            int mn = idx[arity * t];
-            for(int x = 1; x < arity; ++x) {mn = std::min(mn, idx[arity * t + x]);}
-            key[t] = mn;
-        }
-        win.assign((size_t)nwin + 1, 0);
-        if(std::is_sorted(key.begin(), key.end()))      // every system's terms are kept in order
-        {
-            for(size_t t = 0; t < m; ++t) {win[(size_t)key[t] / 256 + 1] += 1;}
-            for(int w = 0; w < nwin; ++w) {win[w + 1] += win[w];}
-            return;
-        }
-        std::vector<size_t> perm(m);
-        for(size_t t = 0; t < m; ++t) {perm[t] = t;}
-        std::stable_sort(perm.begin(), perm.end(), [&](size_t x, size_t y) {return key[x] < key[y];});
-        std::vector<int> idx2(idx.size()), sys2(m), n2(nn ? m : 0);
-        std::vector<double> k2(m), v2(m);
-        for(size_t t = 0; t < m; ++t)
-        {
-            const size_t p = perm[t];
-            for(int x = 0; x < arity; ++x) {idx2[arity * t + x] = idx[arity * p + x];}
-            k2[t] = kk[p]; v2[t] = v0[p]; sys2[t] = sysv[p];
-            if(nn) {n2[t] = (*nn)[p];}
-        }
-        idx.swap(idx2); kk.swap(k2); v0.swap(v2); sysv.swap(sys2);
-        if(nn) {nn->swap(n2);}
-        for(size_t t = 0; t < m; ++t) {win[(size_t)key[perm[t]] / 256 + 1] += 1;}
-        for(int w = 0; w < nwin; ++w) {win[w + 1] += win[w];}
-    };
-    std::vector<long long> w_bond, w_angle, w_dihd;
-    sort_terms(b_idx, 2, b_k, b_v0, b_sys, nullptr, w_bond);
-    sort_terms(a_idx, 3, a_k, a_v0, a_sys, nullptr, w_angle);
-    sort_terms(d_idx, 4, d_k, d_v0, d_sys, &d_n, w_dihd);
-    {
-        std::vector<float2> bkv(b_k.size()), akv(a_k.size());
-        std::vector<float4> dp(d_k.size());
-        for(size_t t = 0; t < b_k.size(); ++t) {bkv[t] = make_float2((float)b_k[t], (float)b_v0[t]);}
-        for(size_t t = 0; t < a_k.size(); ++t) {akv[t] = make_float2((float)a_k[t], (float)a_v0[t]);}
-        for(size_t t = 0; t < d_k.size(); ++t)
-        {
-            const double nv = (double)d_n[t] * d_v0[t];
-            dp[t] = make_float4((float)d_k[t], (float)std::cos(nv), (float)std::sin(nv), (float)d_n[t]);
-        }
-        upload(c->l_bond_kv, bkv, st);
-        upload(c->l_angle_kv, akv, st);
-        upload(c->l_dihd_p, dp, st);
-    }
-    upload(c->l_win_bond, w_bond, st);
-    upload(c->l_win_angle, w_angle, st);
-    upload(c->l_win_dihd, w_dihd, st);
-    upload(c->l_bond_idx, b_idx, st);  upload(c->l_bond_k, b_k, st);
-    upload(c->l_bond_v0, b_v0, st);    upload(c->l_bond_sys, b_sys, st);
-    upload(c->l_angle_idx, a_idx, st); upload(c->l_angle_k, a_k, st);
-    upload(c->l_angle_v0, a_v0, st);   upload(c->l_angle_sys, a_sys, st);
-    upload(c->l_dihd_idx, d_idx, st);  upload(c->l_dihd_k, d_k, st);
-    upload(c->l_dihd_n, d_n, st);      upload(c->l_dihd_v0, d_v0, st);
-    upload(c->l_dihd_sys, d_sys, st);
     LocalArrays& l = c->local;
     l = LocalArrays{};
-    l.nbond = (long long)b_k.size(); l.nangle = (long long)a_k.size(); l.ndihd = (long long)d_k.size();
+    put(c->l_bond_kv, c_bkv); put(c->l_angle_kv, c_akv); put(c->l_dihd_p, c_dp);
+    put(c->l_win_bond, c_wb); put(c->l_win_angle, c_wa); put(c->l_win_dihd, c_wd);
+    put(c->l_bond_idx, c_bidx);  put(c->l_bond_k, c_bk);
+    put(c->l_bond_v0, c_bv0);    put(c->l_bond_sys, c_bsys);
+    put(c->l_angle_idx, c_aidx); put(c->l_angle_k, c_ak);
+    put(c->l_angle_v0, c_av0);   put(c->l_angle_sys, c_asys);
+    put(c->l_dihd_idx, c_didx);  put(c->l_dihd_k, c_dk);
+    put(c->l_dihd_n, c_dn);      put(c->l_dihd_v0, c_dv0);
+    put(c->l_dihd_sys, c_dsys);
+    l.nbond = nb; l.nangle = na; l.ndihd = nd;
     l.bond_idx = c->l_bond_idx.as<int>();   l.bond_k = c->l_bond_k.as<double>();
     l.bond_v0 = c->l_bond_v0.as<double>();  l.bond_sys = c->l_bond_sys.as<int>();
     l.angle_idx = c->l_angle_idx.as<int>(); l.angle_k = c->l_angle_k.as<double>();
@@ -923,9 +1116,11 @@ void commit(mjg_context* c)
     l.win_bond = c->l_win_bond.as<long long>();
     l.win_angle = c->l_win_angle.as<long long>();
     l.win_dihd = c->l_win_dihd.as<long long>();
+    tm.mark("upload");
 
     c->committed = true;
     rebuild_all(c);
+    tm.mark("rebuild");
     compute_initial_forces(c);
     // systems that were resident keep their exact force array: one upload,
     // then one conversion per run of consecutive such systems
@@ -939,10 +1134,13 @@ void commit(mjg_context* c)
         if(any)
         {
             double* h = pinned(c, sizeof(double) * 3 * (size_t)n_tot);
-            for(int k = 0; k < nsys; ++k)
-            {
-                if(keeps(k)) {const HostSystem& s = c->sys[ids[k]]; std::copy(s.force.begin(), s.force.end(), h + 3 * s.off);}
-            }
+            parallel_for(nsys, [&](int64_t k) {
+                if(keeps((int)k))
+                {
+                    const HostSystem& s = c->sys[ids[k]];
+                    std::copy(s.force.begin(), s.force.end(), h + 3 * s.off);
+                }
+            });
             double* stg = c->d_staging.as<double>();
             CK(cudaMemcpyAsync(stg, h, sizeof(double) * 3 * (size_t)n_tot, cudaMemcpyHostToDevice, st));
             for(int k = 0; k < nsys;)
@@ -959,6 +1157,7 @@ void commit(mjg_context* c)
     }
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
+    tm.mark("forces");
 }
 
 // ------------------------------------------------------------------ step
@@ -1065,10 +1264,18 @@ int mjg_context_create(int device, int precision, mjg_context** out)
     if(!c) {return MJG_ENOMEM;}
     c->device = device;
     c->precision = precision;
-    if(cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    bool ok = cudaSetDevice(device) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for(int b = 0; ok && b <= mjg::NGLOBAL; ++b)
+    {
+        ok = cudaStreamCreateWithFlags(&c->side[b], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&c->ev_join[b], cudaEventDisableTiming) == cudaSuccess;
+    }
+    if(!ok)
     {
         cudaGetLastError();
-        delete c;
+        mjg_context_destroy(c);
         return MJG_ECUDA;
     }
     *out = c;
@@ -1091,6 +1298,13 @@ void mjg_context_destroy(mjg_context* c)
         for(auto* b : bufs) {b->release();}
     }
     if(c->h_pinned) {cudaFreeHost(c->h_pinned);}
+    if(c->h_pack) {cudaFreeHost(c->h_pack);}
+    for(int b = 0; b <= mjg::NGLOBAL; ++b)
+    {
+        if(c->side[b]) {cudaStreamSynchronize(c->side[b]); cudaStreamDestroy(c->side[b]);}
+        if(c->ev_join[b]) {cudaEventDestroy(c->ev_join[b]);}
+    }
+    if(c->ev_fork) {cudaEventDestroy(c->ev_fork);}
     if(c->stream) {cudaStreamDestroy(c->stream);}
     delete c;
 }
@@ -1637,6 +1851,52 @@ int mjg_set_threads_per_particle(mjg_context* c, int term, int tpp)
         rebuild_all(c);
         CK(cudaStreamSynchronize(c->stream));
     }
+    ABI_END(c)
+}
+
+int mjg_set_pair_unroll(mjg_context* c, int term, int unroll)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "the batch depth applies to global terms");}
+    if(unroll != 1 && unroll != 2 && unroll != 4) {throw Error(MJG_EINVAL, "unroll must be 1, 2 or 4");}
+    TermDev& T = c->term[term - MJG_TERM_EXV];
+    T.unroll_choice = unroll;
+    if(T.t.unroll != unroll)
+    {
+        T.t.unroll = unroll;    // same lists, another kernel: recapture the step
+        release_graph(c);
+    }
+    ABI_END(c)
+}
+
+int mjg_set_pair_schedule(mjg_context* c, int term, int schedule)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "the schedule applies to global terms");}
+    if(schedule != 0 && schedule != 1) {throw Error(MJG_EINVAL, "schedule must be 0 or 1");}
+    TermDev& T = c->term[term - MJG_TERM_EXV];
+    T.schedule_choice = schedule;
+    if(T.t.schedule != schedule)
+    {
+        T.t.schedule = schedule;
+        release_graph(c);
+    }
+    ABI_END(c)
+}
+
+int mjg_get_pair_schedule(mjg_context* c, int term, int* schedule)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !schedule) {throw Error(MJG_EINVAL, "bad query");}
+    *schedule = c->term[term - MJG_TERM_EXV].schedule_choice;
+    ABI_END(c)
+}
+
+int mjg_get_pair_unroll(mjg_context* c, int term, int* unroll)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !unroll) {throw Error(MJG_EINVAL, "bad query");}
+    *unroll = c->term[term - MJG_TERM_EXV].unroll_choice;
     ABI_END(c)
 }
 

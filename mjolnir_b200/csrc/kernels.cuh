@@ -31,6 +31,8 @@ struct TermArrays {
     int        ncell;           // total cells over all systems
     int        cap;             // neighbour capacity per slot (a multiple of tpp)
     int        tpp;             // threads per slot of the pair kernel (1, 2, 4, 8, 16)
+    int        unroll;          // partners requested per batch by the force launch (1, 2, 4)
+    int        schedule;        // force launch: 0 = slot per tpp threads, 1 = warp-balanced (mixed)
     int        any_periodic;    // some system with this term has a periodic box
     const int* part_particle;   // [np] global particle index
     const double* part_p0;      // [np] radius / charge / sigma
@@ -70,8 +72,11 @@ void launch_integrate_last(const Arena& a, cudaStream_t s);
 void launch_zero_force(const Arena& a, cudaStream_t s);
 
 void launch_rebuild(const Arena& a, int gterm, TermArrays& t, int force_all, cudaStream_t s);
+// slot coordinates of a term's participants (before its force launch)
+void launch_gather(const Arena& a, TermArrays& t, cudaStream_t s);
+// gather: refresh the slot coordinates first
 void launch_pair(const Arena& a, int gterm, TermArrays& t, bool need_force, bool need_energy,
-                 int calc_energy_form, cudaStream_t s);
+                 int calc_energy_form, cudaStream_t s, bool gather = true);
 
 struct LocalArrays {
     long long nbond, nangle, ndihd;

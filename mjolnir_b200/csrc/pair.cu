@@ -75,18 +75,149 @@ template<> struct Acc<P_MIXED>
         y += __shfl_xor_sync(0xffffffffu, y, o);
         z += __shfl_xor_sync(0xffffffffu, z, o);
     }
+    // integer atomics: exact and order independent, so the force launches of
+    // different terms and the bonded launch may run concurrently
     __device__ __forceinline__ void store(void* force, long long i) const
     {
-        longlong4* f = static_cast<longlong4*>(force) + i;
-        longlong4 v = *f;
-        v.x += x; v.y += y; v.z += z;
-        *f = v;
+        unsigned long long* f = reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(force) + i);
+        if(x) {atomicAdd(f + 0, (unsigned long long)x);}
+        if(y) {atomicAdd(f + 1, (unsigned long long)y);}
+        if(z) {atomicAdd(f + 2, (unsigned long long)z);}
     }
 };
 
-// PER: some system of the arena is periodic (the minimum image is applied
-// where the system asks for it); without it the image code is compiled out.
-template<int PREC, int G, bool NF, bool NE, int TPP, bool PER>
+// Constants of one slot's pair evaluations and the evaluation of one pair
+// (slot s, partner q).  PER: some system of the arena is periodic (the
+// minimum image is applied where the system asks for it); without it the
+// image code is compiled out.
+template<int PREC, int G, bool NF, bool NE, bool PER>
+struct PairEval {
+    const SysDev* S;
+    double4 pi;
+    long long s;
+    bool periodic;
+    double crsq, coefc, eps, eps12, debye, inv_debye, abs_cut_sq, qi, inv4pi, epsi;
+    float eps12f, epsf, coefcf, debf, invdf;
+    const double* slot_p1;
+
+    __device__ __forceinline__ PairEval(const Arena& a, const TermArrays& t, long long slot, int sys)
+    {
+        s = slot;
+        S = &a.sys[sys];
+        const GlobalParams& P = S->g[G];
+        periodic = PER && S->boundary == B_PERIODIC;
+        pi = t.slot_pd[slot];
+        crsq  = P.cutoff_ratio_sq;
+        coefc = P.coef_at_cutoff;
+        eps   = P.eps;
+        eps12 = eps * 12;
+        debye = P.debye; inv_debye = P.inv_debye;
+        abs_cut_sq = P.abs_cutoff * P.abs_cutoff;
+        qi = pi.w; inv4pi = P.inv4pi;
+        slot_p1 = t.slot_p1;
+        epsi  = (G == G_LJ) ? t.slot_p1[slot] : 0.0;
+        eps12f = (float)eps12; epsf = (float)eps; coefcf = (float)coefc;
+        debf = (float)debye; invdf = (float)inv_debye;
+    }
+
+    __device__ __forceinline__ void operator()(const double4& pj, const int q, Acc<PREC>& acc,
+                                               double& energy, bool& ovf) const
+    {
+        double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+        if(PER && periodic)
+        {
+            dx = min_image(dx, S->halfw[0], S->width[0]);
+            dy = min_image(dy, S->halfw[1], S->width[1]);
+            dz = min_image(dz, S->halfw[2], S->width[2]);
+        }
+        const double l2 = fma(dz, dz, fma(dy, dy, dx * dx));
+        const bool count_e = NE && (s < q);
+        if(G == G_EXV)
+        {
+            const double sigma = pi.w + pj.w;
+            const double sigma_sq = sigma * sigma;
+            const bool in = !(sigma_sq * crsq < l2);
+            if(PREC == P_FP64)
+            {
+                if(!in) {return;}
+                const double rcp = 1.0 / l2;
+                const double s2 = sigma_sq * rcp;
+                const double s6 = s2 * s2 * s2;
+                if(NF) {acc.add(-eps12 * s6 * s6 * rcp, dx, dy, dz, ovf);}
+                if(count_e) {energy += eps * (s6 * s6 - coefc);}
+            }
+            else
+            {
+                // branch-free: every lane evaluates, pairs outside the
+                // cutoff add an exact zero
+                const float rcp = __frcp_rn((float)l2);
+                const float s2 = (float)sigma_sq * rcp;
+                const float s6 = s2 * s2 * s2;
+                const float cf = in ? -eps12f * s6 * s6 * rcp : 0.0f;
+                if(NF) {acc.add((double)cf, dx, dy, dz, ovf);}
+                if(count_e && in) {energy += (double)(epsf * (s6 * s6 - coefcf));}
+            }
+        }
+        else if(G == G_DH)
+        {
+            const bool in = l2 < abs_cut_sq;
+            if(PREC == P_FP64)
+            {
+                if(!in) {return;}
+                const double qq = (qi * pj.w) * inv4pi;     // symmetric in i, j
+                const double rl = rsqrt(l2);
+                const double l  = l2 * rl;
+                const double ex = exp(-l * inv_debye);
+                if(NF) {acc.add(-qq * (debye + l) * inv_debye / (l * l) * ex * rl, dx, dy, dz, ovf);}
+                if(count_e) {energy += qq * (ex / l - coefc);}
+            }
+            else
+            {
+                // branch-free like ExcludedVolume: outside the cutoff the
+                // distance is replaced by the cutoff and the force is zero
+                const float qq = (float)((qi * pj.w) * inv4pi);
+                const float l2f = in ? (float)l2 : (float)abs_cut_sq;
+                const float rl = rsqrtf(l2f);
+                const float l  = l2f * rl;
+                const float ex = __expf(-l * invdf);
+                const float cf = in ? -qq * (debf + l) * invdf * (rl * rl) * ex * rl : 0.0f;
+                if(NF) {acc.add((double)cf, dx, dy, dz, ovf);}
+                if(count_e && in) {energy += (double)(qq * (ex * rl - coefcf));}
+            }
+        }
+        else   // G_LJ
+        {
+            const double sigma = (pi.w + pj.w) / 2;
+            const double epsj = slot_p1[q];
+            const double epsilon = (epsi == epsj) ? epsi : sqrt(epsi * epsj);
+            const double sigma_sq = sigma * sigma;
+            if(sigma_sq * crsq < l2) {return;}
+            if(PREC == P_FP64)
+            {
+                const double rcp = 1.0 / l2;
+                const double s2 = sigma_sq * rcp;
+                const double s6 = s2 * s2 * s2;
+                if(NF) {acc.add(24 * epsilon * (s6 - 2 * s6 * s6) * rcp, dx, dy, dz, ovf);}
+                if(count_e) {energy += 4 * epsilon * (s6 * s6 - s6 - coefc);}
+            }
+            else
+            {
+                const float rcp = __frcp_rn((float)l2);
+                const float s2 = (float)sigma_sq * rcp;
+                const float s6 = s2 * s2 * s2;
+                const float ef = (float)epsilon;
+                if(NF) {acc.add((double)(24.0f * ef * (s6 - 2.0f * s6 * s6) * rcp), dx, dy, dz, ovf);}
+                if(count_e) {energy += (double)(4.0f * ef * (s6 * s6 - s6 - coefcf));}
+            }
+        }
+    }
+};
+
+// One slot per TPP consecutive threads.  UNR: partners requested per batch.
+// 1 keeps one partner in flight ahead of the pair being evaluated; 2 and 4
+// issue the batch's list words, then its coordinates, before evaluating any
+// of them (more loads in flight per thread, more registers).
+template<int PREC, int G, bool NF, bool NE, int TPP, bool PER, int UNR>
 __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
 {
     // TPP consecutive threads share one slot; lane lg walks partners lg,
@@ -101,127 +232,47 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
     Acc<PREC> acc;
     if(active)
     {
-        const SysDev& S = a.sys[sys];
-        const GlobalParams& P = S.g[G];
-        const bool periodic = PER && S.boundary == B_PERIODIC;
-        const double4 pi = t.slot_pd[s];
+        const PairEval<PREC, G, NF, NE, PER> eval(a, t, s, sys);
         const long long np = t.np;
-        const int n = S.frozen ? 0 : t.nnb[s];       // a frozen system keeps its forces
-
-        // potential constants
-        const double crsq  = P.cutoff_ratio_sq;
-        const double coefc = P.coef_at_cutoff;
-        const double eps   = P.eps;
-        const double eps12 = eps * 12;
-        const double debye = P.debye, inv_debye = P.inv_debye, abs_cut = P.abs_cutoff;
-        const double abs_cut_sq = abs_cut * abs_cut;
-        const double qi = pi.w, inv4pi = P.inv4pi;
-        const double epsi  = (G == G_LJ) ? t.slot_p1[s] : 0.0;
-        const float  eps12f = (float)eps12, epsf = (float)eps, coefcf = (float)coefc;
-        const float  debf = (float)debye, invdf = (float)inv_debye;
+        const int n = eval.S->frozen ? 0 : t.nnb[s];       // a frozen system keeps its forces
         const int* __restrict__ nbr = t.nbr + s * TPP + lg;
         const double4* __restrict__ pd = t.slot_pd;
-
-        // software pipeline: the next partner's index and coordinates are
-        // requested before the current pair is evaluated
-        int k = lg;
-        int q = 0;
-        double4 pj = make_double4(0.0, 0.0, 0.0, 0.0);
-        if(k < n) {q = __ldg(nbr + (long long)(k / TPP) * np * TPP); pj = pd[q];}
-        for(; k < n; k += TPP)
+        if(UNR == 1)
         {
-            const int kn = k + TPP;
-            int qn = q;
-            double4 pn = pj;
-            if(kn < n) {qn = __ldg(nbr + (long long)(kn / TPP) * np * TPP); pn = pd[qn];}
-            do {
-            double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-            if(PER && periodic)
+            // software pipeline: the next partner's index and coordinates are
+            // requested before the current pair is evaluated
+            int k = lg;
+            int q = 0;
+            double4 pj = make_double4(0.0, 0.0, 0.0, 0.0);
+            if(k < n) {q = __ldg(nbr + (long long)(k / TPP) * np * TPP); pj = pd[q];}
+            for(; k < n; k += TPP)
             {
-                dx = min_image(dx, S.halfw[0], S.width[0]);
-                dy = min_image(dy, S.halfw[1], S.width[1]);
-                dz = min_image(dz, S.halfw[2], S.width[2]);
+                const int kn = k + TPP;
+                int qn = q;
+                double4 pn = pj;
+                if(kn < n) {qn = __ldg(nbr + (long long)(kn / TPP) * np * TPP); pn = pd[qn];}
+                eval(pj, q, acc, energy, ovf);
+                q = qn;
+                pj = pn;
             }
-            const double l2 = fma(dz, dz, fma(dy, dy, dx * dx));
-            const bool count_e = NE && (s < q);
-            if(G == G_EXV)
+        }
+        else
+        {
+            for(int k = lg; k < n; k += UNR * TPP)
             {
-                const double sigma = pi.w + pj.w;
-                const double sigma_sq = sigma * sigma;
-                const bool in = !(sigma_sq * crsq < l2);
-                if(PREC == P_FP64)
+                int qv[UNR];
+                double4 pv[UNR];
+#pragma unroll
+                for(int u = 0; u < UNR; ++u)
                 {
-                    if(!in) {break;}
-                    const double rcp = 1.0 / l2;
-                    const double s2 = sigma_sq * rcp;
-                    const double s6 = s2 * s2 * s2;
-                    if(NF) {acc.add(-eps12 * s6 * s6 * rcp, dx, dy, dz, ovf);}
-                    if(count_e) {energy += eps * (s6 * s6 - coefc);}
+                    const int kk = k + u * TPP;
+                    qv[u] = kk < n ? __ldg(nbr + (long long)(kk / TPP) * np * TPP) : -1;
                 }
-                else
-                {
-                    // branch-free: every lane evaluates, pairs outside the
-                    // cutoff add an exact zero
-                    const float rcp = __frcp_rn((float)l2);
-                    const float s2 = (float)sigma_sq * rcp;
-                    const float s6 = s2 * s2 * s2;
-                    const float cf = in ? -eps12f * s6 * s6 * rcp : 0.0f;
-                    if(NF) {acc.add((double)cf, dx, dy, dz, ovf);}
-                    if(count_e && in) {energy += (double)(epsf * (s6 * s6 - coefcf));}
-                }
+#pragma unroll
+                for(int u = 0; u < UNR; ++u) {pv[u] = qv[u] >= 0 ? pd[qv[u]] : eval.pi;}
+#pragma unroll
+                for(int u = 0; u < UNR; ++u) {if(qv[u] >= 0) {eval(pv[u], qv[u], acc, energy, ovf);}}
             }
-            else if(G == G_DH)
-            {
-                if(!(l2 < abs_cut_sq)) {break;}
-                if(PREC == P_FP64)
-                {
-                    const double qq = (qi * pj.w) * inv4pi;     // symmetric in i, j
-                    const double rl = rsqrt(l2);
-                    const double l  = l2 * rl;
-                    const double ex = exp(-l * inv_debye);
-                    if(NF) {acc.add(-qq * (debye + l) * inv_debye / (l * l) * ex * rl, dx, dy, dz, ovf);}
-                    if(count_e) {energy += qq * (ex / l - coefc);}
-                }
-                else
-                {
-                    const float qq = (float)((qi * pj.w) * inv4pi);
-                    const float l2f = (float)l2;
-                    const float rl = rsqrtf(l2f);
-                    const float l  = l2f * rl;
-                    const float ex = __expf(-l * invdf);
-                    if(NF) {acc.add((double)(-qq * (debf + l) * invdf * (rl * rl) * ex * rl), dx, dy, dz, ovf);}
-                    if(count_e) {energy += (double)(qq * (ex * rl - coefcf));}
-                }
-            }
-            else   // G_LJ
-            {
-                const double sigma = (pi.w + pj.w) / 2;
-                const double epsj = t.slot_p1[q];
-                const double epsilon = (epsi == epsj) ? epsi : sqrt(epsi * epsj);
-                const double sigma_sq = sigma * sigma;
-                if(sigma_sq * crsq < l2) {break;}
-                if(PREC == P_FP64)
-                {
-                    const double rcp = 1.0 / l2;
-                    const double s2 = sigma_sq * rcp;
-                    const double s6 = s2 * s2 * s2;
-                    if(NF) {acc.add(24 * epsilon * (s6 - 2 * s6 * s6) * rcp, dx, dy, dz, ovf);}
-                    if(count_e) {energy += 4 * epsilon * (s6 * s6 - s6 - coefc);}
-                }
-                else
-                {
-                    const float rcp = __frcp_rn((float)l2);
-                    const float s2 = (float)sigma_sq * rcp;
-                    const float s6 = s2 * s2 * s2;
-                    const float ef = (float)epsilon;
-                    if(NF) {acc.add((double)(24.0f * ef * (s6 - 2.0f * s6 * s6) * rcp), dx, dy, dz, ovf);}
-                    if(count_e) {energy += (double)(4.0f * ef * (s6 * s6 - s6 - coefcf));}
-                }
-            }
-            } while(0);
-            q = qn;
-            pj = pn;
-
         }
     }
     // group reduction: exact in fixed point, fixed order in FP64
@@ -245,6 +296,93 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
         {
             atomicAdd(&a.sys[sys].energy[T_EXV + G], energy);
         }
+    }
+}
+
+// Warp-balanced schedule of the mixed form's force launch: a warp owns 32
+// consecutive slots and splits the concatenation of their lists into 32 equal
+// contiguous chunks, one per lane, so every lane evaluates the same number of
+// pairs whatever the list lengths (one slot per thread leaves the lanes of
+// short lists idle).  A lane sums the pairs of one slot in registers and adds
+// the sum to the particle's fixed-point force with integer atomics when its
+// chunk leaves that slot; integer sums are exact, so the result does not
+// depend on where the chunks start.
+template<int G, bool PER, int UNR>
+__global__ void __launch_bounds__(TPB) k_pair_warp(Arena a, TermArrays t)
+{
+    __shared__ int seg[TPB / 32][33];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const long long gt = (long long)blockIdx.x * TPB + threadIdx.x;
+    const long long s0 = gt - lane;                  // first slot of this warp
+    int n_my = 0;
+    if(gt < t.np)
+    {
+        const int sys = t.slot_sys[gt];
+        n_my = a.sys[sys].frozen ? 0 : t.nnb[gt];    // a frozen system keeps its forces
+    }
+    int incl = n_my;
+#pragma unroll
+    for(int o = 1; o < 32; o <<= 1)
+    {
+        const int y = __shfl_up_sync(full, incl, o);
+        if(lane >= o) {incl += y;}
+    }
+    seg[wl][lane] = incl - n_my;                     // first entry of slot s0 + lane
+    if(lane == 31) {seg[wl][32] = incl;}
+    __syncwarp();
+    const int total = seg[wl][32];
+    const int per = (total + 31) >> 5;
+    int e = min(lane * per, total);
+    const int e_end = min(e + per, total);
+    if(e >= e_end) {return;}
+    // slot of entry e: the last j with seg[j] <= e (seg is non-decreasing)
+    int j = 0;
+#pragma unroll
+    for(int b = 16; b > 0; b >>= 1) {if(j + b < 32 && seg[wl][j + b] <= e) {j += b;}}
+
+    const long long np = t.np;
+    const int tpp = t.tpp;
+    const int lt = __ffs(tpp) - 1;                   // tpp is a power of two
+    const int* __restrict__ nbr = t.nbr;
+    const double4* __restrict__ pd = t.slot_pd;
+    while(e < e_end)
+    {
+        const long long s = s0 + j;
+        const int b = seg[wl][j];
+        const int kend = min(seg[wl][j + 1], e_end) - b;
+        const int sys = t.slot_sys[s];
+        const PairEval<P_MIXED, G, true, false, PER> eval(a, t, s, sys);
+        Acc<P_MIXED> acc;
+        double energy = 0.0;
+        bool ovf = false;
+        for(int k = e - b; k < kend; k += UNR)
+        {
+            int qv[UNR];
+            double4 pv[UNR];
+#pragma unroll
+            for(int u = 0; u < UNR; ++u)
+            {
+                const int kk = k + u;
+                qv[u] = kk < kend ? __ldg(nbr + (((long long)(kk >> lt) * np + s) << lt) + (kk & (tpp - 1))) : -1;
+            }
+#pragma unroll
+            for(int u = 0; u < UNR; ++u) {pv[u] = qv[u] >= 0 ? pd[qv[u]] : eval.pi;}
+#pragma unroll
+            for(int u = 0; u < UNR; ++u) {if(qv[u] >= 0) {eval(pv[u], qv[u], acc, energy, ovf);}}
+        }
+        if(acc.x | acc.y | acc.z)
+        {
+            unsigned long long* f =
+                reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(a.force) + t.slot_particle[s]);
+            atomicAdd(f + 0, (unsigned long long)acc.x);
+            atomicAdd(f + 1, (unsigned long long)acc.y);
+            atomicAdd(f + 2, (unsigned long long)acc.z);
+        }
+        if(ovf) {atomicOr(&a.sys[sys].status, ST_FIXED_OVERFLOW);}
+        e = b + kend;
+        ++j;
+        while(j < 32 && seg[wl][j + 1] == seg[wl][j]) {++j;}     // skip empty lists
     }
 }
 
@@ -289,9 +427,22 @@ template<int PREC, int G, int TPP, bool PER>
 void dispatch_per(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
 {
     const unsigned nb = (unsigned)((t.np * TPP + TPB - 1) / TPB);
-    if(nf && ne)  {k_pair<PREC, G, true,  true,  TPP, PER><<<nb, TPB, 0, s>>>(a, t);}
-    else if(nf)   {k_pair<PREC, G, true,  false, TPP, PER><<<nb, TPB, 0, s>>>(a, t);}
-    else if(ne)   {k_pair<PREC, G, false, true,  TPP, PER><<<nb, TPB, 0, s>>>(a, t);}
+    if(nf && ne)  {k_pair<PREC, G, true,  true,  TPP, PER, 1><<<nb, TPB, 0, s>>>(a, t);}
+    else if(nf)
+    {
+        // the per-step force launch: schedule and partner batch depth are tunable
+        if(PREC == P_MIXED && t.schedule == 1)
+        {
+            const unsigned nw = (unsigned)((t.np + TPB - 1) / TPB);
+            if(t.unroll == 4)      {k_pair_warp<G, PER, 4><<<nw, TPB, 0, s>>>(a, t);}
+            else if(t.unroll == 2) {k_pair_warp<G, PER, 2><<<nw, TPB, 0, s>>>(a, t);}
+            else                   {k_pair_warp<G, PER, 1><<<nw, TPB, 0, s>>>(a, t);}
+        }
+        else if(t.unroll == 4) {k_pair<PREC, G, true, false, TPP, PER, 4><<<nb, TPB, 0, s>>>(a, t);}
+        else if(t.unroll == 2) {k_pair<PREC, G, true, false, TPP, PER, 2><<<nb, TPB, 0, s>>>(a, t);}
+        else                   {k_pair<PREC, G, true, false, TPP, PER, 1><<<nb, TPB, 0, s>>>(a, t);}
+    }
+    else if(ne)   {k_pair<PREC, G, false, true,  TPP, PER, 1><<<nb, TPB, 0, s>>>(a, t);}
 }
 
 template<int PREC, int G, int TPP>
@@ -316,12 +467,19 @@ void dispatch(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
 
 }  // namespace
 
-void launch_pair(const Arena& a, int g, TermArrays& t, bool need_force, bool need_energy,
-                 int /*calc_energy_form*/, cudaStream_t s)
+void launch_gather(const Arena& a, TermArrays& t, cudaStream_t s)
 {
     if(!t.on || t.np == 0) {return;}
     k_gather<<<(unsigned)((t.np + 255) / 256), 256, 0, s>>>(a, t);
-    note_launches(2);
+    note_launches(1);
+}
+
+void launch_pair(const Arena& a, int g, TermArrays& t, bool need_force, bool need_energy,
+                 int /*calc_energy_form*/, cudaStream_t s, bool gather)
+{
+    if(!t.on || t.np == 0) {return;}
+    if(gather) {launch_gather(a, t, s);}
+    note_launches(1);
     if(a.precision == P_FP64)
     {
         if(g == G_EXV)     {dispatch<P_FP64, G_EXV>(a, t, need_force, need_energy, s);}

@@ -237,6 +237,26 @@ class Engine:
             raise A.MjgError(A.EINVAL, f"term {term} not present")
         return v.value
 
+    def set_pair_unroll(self, term, unroll: int):
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        self._c(self.lib.mjg_set_pair_unroll(self.ctx, t, int(unroll)))
+
+    def get_pair_unroll(self, term) -> int:
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        v = C.c_int()
+        self._c(self.lib.mjg_get_pair_unroll(self.ctx, t, C.byref(v)))
+        return v.value
+
+    def set_pair_schedule(self, term, schedule: int):
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        self._c(self.lib.mjg_set_pair_schedule(self.ctx, t, int(schedule)))
+
+    def get_pair_schedule(self, term) -> int:
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        v = C.c_int()
+        self._c(self.lib.mjg_get_pair_schedule(self.ctx, t, C.byref(v)))
+        return v.value
+
     def set_margin(self, term, margin: float):
         t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
         self._c(self.lib.mjg_set_margin(self.ctx, t, float(margin)))

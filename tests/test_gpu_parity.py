@@ -225,3 +225,37 @@ def test_fixed_point_newton_third_law():
         f, _ = e.term_force(sid, t)
         assert np.abs(f.sum(axis=0)).max() <= 1e-9
     e.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_launch_shapes_give_the_same_trajectory(precision):
+    """Every threads-per-slot and partner-batch choice of the autotuner gives
+    the same dynamics: bit for bit in the mixed form, within rounding of the
+    summation order in FP64."""
+    descs = [S.polymer_melt(nchains=4, nbeads=60, radius=45.0, seed=41),
+             S.bead_fluid(n=3000, density=0.003, seed=42, dt=0.3),
+             S.lj_fluid(n=512, seed=43)]
+    ref = None
+    shapes = [(0, tpp, unr) for tpp in (1, 2, 4, 8, 16) for unr in (1, 2, 4)]
+    if precision == "mixed":
+        shapes += [(1, tpp, unr) for tpp in (1, 16) for unr in (1, 2, 4)]
+    for sch, tpp, unr in shapes:
+        e = Engine(precision)
+        ids = [e.add_system(d) for d in descs]
+        e.commit()
+        for term in ("exv", "dh", "lj"):
+            e.set_pair_schedule(term, sch)
+            e.set_threads_per_particle(term, tpp)
+            e.set_pair_unroll(term, unr)
+            assert (e.get_pair_schedule(term), e.get_pair_unroll(term)) == (sch, unr)
+        e.step(30)
+        got = [e.state(sid)[0] for sid in ids]
+        e.close()
+        if ref is None:
+            ref = got
+            continue
+        for a, b in zip(got, ref):
+            if precision == "mixed":
+                assert np.array_equal(a, b), (sch, tpp, unr)
+            else:
+                assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max(), (sch, tpp, unr)
