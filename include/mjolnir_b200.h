@@ -221,11 +221,13 @@ MJG_API int mjg_set_margin(mjg_context* ctx, int term, double margin);
  * no result.  No counterpart in the reference. */
 MJG_API int mjg_set_pair_unroll(mjg_context* ctx, int term, int unroll);
 MJG_API int mjg_get_pair_unroll(mjg_context* ctx, int term, int* unroll);
-/* Schedule of a global term's force launch in the mixed form: 0 = one
- * particle per group of threads-per-particle threads; 1 = warp-balanced, a
- * warp splits the combined lists of its 32 particles evenly over its lanes
- * and adds each partial sum with integer atomics (exact, so the forces are
- * identical).  The FP64 form always uses 0.  No counterpart in the reference. */
+/* Schedule of a global term's force launch: 0 = one particle per group of
+ * threads-per-particle threads; 1 (mixed form only) = warp-balanced, a warp
+ * splits the combined lists of its 32 particles evenly over its lanes and adds
+ * each partial sum with integer atomics (exact, so the forces are identical);
+ * 2 = one thread per particle reading its list in blocks of
+ * threads-per-particle words with vector loads (with threads-per-particle 1
+ * it is schedule 0).  No counterpart in the reference. */
 MJG_API int mjg_set_pair_schedule(mjg_context* ctx, int term, int schedule);
 MJG_API int mjg_get_pair_schedule(mjg_context* ctx, int term, int* schedule);
 /* Sets the per-particle neighbour capacity of a global term's lists.  A

@@ -5,9 +5,10 @@ For every global term of an :class:`~mjolnir_b200.engine.Engine` it picks
     and the rebuild interval) from a candidate set, by timing whole MD steps --
     a thinner skin makes shorter lists but more frequent rebuilds;
   * the pair kernel's launch shape, by timing the kernel alone: the schedule
-    (one particle per group of threads, or warp-balanced over the lists of a
-    warp's 32 particles; mixed form only), the threads per particle / list
-    layout (1, 2, 4, 8, 16) and the partners each thread requests per batch
+    (one particle per group of threads; warp-balanced over the lists of a
+    warp's 32 particles, mixed form only; or one thread per particle reading
+    its list in blocks with vector loads), the threads per particle / list
+    block (1, 2, 4, 8, 16) and the partners each thread requests per batch
     (1, 2, 4).
 In the mixed form neither choice changes a result: the fixed-point force sums
 do not depend on list order or length.  The engine's systems keep stepping
@@ -30,7 +31,7 @@ def _time_steps(eng, nsteps: int) -> float:
 
 
 def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
-         tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1), steps: int = 60,
+         tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1, 2), steps: int = 60,
          warm: int = 20, log=None) -> dict:
     present = []
     for t in terms:
@@ -44,7 +45,8 @@ def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
         best = None
         for m in margins:
             eng.set_margin(t, m)
-            shape = _tune_shape(eng, t, tpps, unrolls, schedules if eng.precision == "mixed" else (0,))
+            shape = _tune_shape(eng, t, tpps, unrolls,
+                                tuple(x for x in schedules if eng.precision == "mixed" or x != 1))
             _apply(eng, t, shape)
             eng.step(warm)
             ms = _time_steps(eng, steps)
@@ -71,8 +73,10 @@ def _tune_shape(eng, term, tpps, unrolls, schedules):
     for sch in schedules:
         eng.set_pair_schedule(term, sch)
         for p in tpps:
+            if sch == 2 and p == 1:
+                continue                  # the same launch as schedule 0
             eng.set_threads_per_particle(term, p)
-            for u in unrolls:
+            for u in (unrolls if sch != 2 else (1,)):
                 eng.set_pair_unroll(term, u)
                 ms = eng.time_kernel(term, reps=10)
                 if best is None or ms < best[0]:
@@ -81,7 +85,7 @@ def _tune_shape(eng, term, tpps, unrolls, schedules):
 
 
 def tune_shapes(eng, terms=("exv", "dh", "lj"), tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4),
-                schedules=(0, 1)) -> dict:
+                schedules=(0, 1, 2)) -> dict:
     """Launch shape only (margins as committed): for a single large system,
     where the margin is fixed by the input."""
     out = {}
@@ -90,7 +94,8 @@ def tune_shapes(eng, terms=("exv", "dh", "lj"), tpps=(1, 2, 4, 8, 16), unrolls=(
             eng.get_threads_per_particle(t)
         except Exception:
             continue
-        shape = _tune_shape(eng, t, tpps, unrolls, schedules if eng.precision == "mixed" else (0,))
+        shape = _tune_shape(eng, t, tpps, unrolls,
+                            tuple(x for x in schedules if eng.precision == "mixed" or x != 1))
         _apply(eng, t, shape)
         out[t] = {"schedule": shape[0], "threads_per_particle": shape[1], "unroll": shape[2]}
     return out

@@ -87,8 +87,10 @@ __global__ void __launch_bounds__(TPB) k_cells_assign(Arena a, int g, TermArrays
     }
 }
 
-// exclusive scan of one flagged system's cells per block; cell_start of the
-// system's first cell is its first slot
+// exclusive scan of one flagged system's cells per block (SCAN_ITEMS cells
+// per thread and pass); cell_start of the system's first cell is its first
+// slot
+constexpr int SCAN_ITEMS = 4;
 __global__ void __launch_bounds__(SCAN_TPB) k_scan_sys(Arena a, int g, TermArrays t)
 {
     const int nf = t.work[2];
@@ -100,11 +102,18 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan_sys(Arena a, int g, TermArray
         const GlobalParams& G = a.sys[t.flagged[f]].g[g];
         if(threadIdx.x == 0) {carry = G.slot_off;}
         __syncthreads();
-        for(int base = 0; base < G.ncell; base += SCAN_TPB)
+        for(int base = 0; base < G.ncell; base += SCAN_TPB * SCAN_ITEMS)
         {
-            const int cell = G.cell_off + base + threadIdx.x;
-            const int v = base + threadIdx.x < G.ncell ? t.cell_count[cell] : 0;
-            int incl = v;
+            const int first = base + threadIdx.x * SCAN_ITEMS;     // this thread's cells
+            int v[SCAN_ITEMS];
+            int sum = 0;
+#pragma unroll
+            for(int q = 0; q < SCAN_ITEMS; ++q)
+            {
+                v[q] = first + q < G.ncell ? t.cell_count[G.cell_off + first + q] : 0;
+                sum += v[q];
+            }
+            int incl = sum;
 #pragma unroll
             for(int o = 1; o < 32; o <<= 1)
             {
@@ -126,10 +135,15 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan_sys(Arena a, int g, TermArray
                 warp_tot[lane] = xi - x;
             }
             __syncthreads();
-            const int excl = carry + warp_tot[w] + incl - v;
-            if(base + threadIdx.x < G.ncell) {t.cell_start[cell] = excl;}
+            int run = carry + warp_tot[w] + incl - sum;
+#pragma unroll
+            for(int q = 0; q < SCAN_ITEMS; ++q)
+            {
+                if(first + q < G.ncell) {t.cell_start[G.cell_off + first + q] = run;}
+                run += v[q];
+            }
             __syncthreads();
-            if(threadIdx.x == SCAN_TPB - 1) {carry = excl + v;}
+            if(threadIdx.x == SCAN_TPB - 1) {carry = run;}
             __syncthreads();
         }
     }
@@ -149,24 +163,47 @@ __global__ void __launch_bounds__(TPB) k_cells_scatter(TermArrays t, int* slot_t
     }
 }
 
-// one warp per cell: rank sort of the members by participant index, so that
-// the slot order depends only on the cell assignment
+// rank sort of each cell's members by participant index, so that the slot
+// order depends only on the cell assignment.  A warp takes 32 cells: each
+// lane sorts a small cell (up to SMALL members) by itself, then the warp sorts
+// the larger ones together, one after the other.
+constexpr int SMALL = 8;
 __global__ void __launch_bounds__(TPB) k_cells_sort(TermArrays t, const int* slot_tmp)
 {
     const int n = t.work[1];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned full = 0xffffffffu;
     for(int c = blockIdx.x; c < n; c += gridDim.x)
     {
         const int4 w = t.cell_chunks[c];
-        for(int cell = w.y + wid; cell < w.z; cell += TPB / 32)
+        for(int cb = w.y + wid * 32; cb < w.z; cb += TPB)
         {
-            const int b = t.cell_start[cell], m = t.cell_count[cell];
-            for(int e = lane; e < m; e += 32)
+            const int cell = cb + lane;
+            int b = 0, m = 0;
+            if(cell < w.z) {b = t.cell_start[cell]; m = t.cell_count[cell];}
+            if(m <= SMALL)
             {
-                const int v = slot_tmp[b + e];
-                int rank = 0;
-                for(int u = 0; u < m; ++u) {rank += slot_tmp[b + u] < v ? 1 : 0;}
-                t.slot_part[b + rank] = v;
+                for(int e = 0; e < m; ++e)
+                {
+                    const int v = slot_tmp[b + e];
+                    int rank = 0;
+                    for(int u = 0; u < m; ++u) {rank += slot_tmp[b + u] < v ? 1 : 0;}
+                    t.slot_part[b + rank] = v;
+                }
+            }
+            unsigned big = __ballot_sync(full, m > SMALL);
+            while(big)
+            {
+                const int src = __ffs(big) - 1;
+                big &= big - 1;
+                const int bb = __shfl_sync(full, b, src), mm = __shfl_sync(full, m, src);
+                for(int e = lane; e < mm; e += 32)
+                {
+                    const int v = slot_tmp[bb + e];
+                    int rank = 0;
+                    for(int u = 0; u < mm; ++u) {rank += slot_tmp[bb + u] < v ? 1 : 0;}
+                    t.slot_part[bb + rank] = v;
+                }
             }
         }
     }
@@ -184,6 +221,7 @@ __global__ void __launch_bounds__(TPB) k_slots_setup(Arena a, TermArrays t)
         const int i = t.part_particle[p];
         const double4 r = a.pos[i];
         t.slot_particle[s] = i;
+        t.slot_of[i]       = s;
         t.slot_lead[s]     = t.part_lead[p];
         t.slot_sys[s]      = w.x;
         t.slot_pd[s]       = make_double4(r.x, r.y, r.z, t.part_p0[p]);

@@ -129,14 +129,14 @@ struct HostSystem {
 struct TermDev {
     DevBuf part_particle, part_p0, part_p1, part_lead, part_sys, part_cell;
     DevBuf cell_count, cell_start, cell_fill, work, part_chunks, cell_chunks, flagged;
-    DevBuf slot_part, slot_particle, slot_lead, slot_sys, slot_pd, slot_p1;
+    DevBuf slot_part, slot_particle, slot_lead, slot_sys, slot_pd, slot_p1, slot_of;
     DevBuf nnb, nbr, max_count, any_rebuild;
     DevBuf ex_start, ex_idx;
     int cap_alloc = 0;           // capacity the nbr buffer was sized for
     bool tpp_fixed = false;      // threads per slot chosen by the caller
     int tpp_choice = 1;          // ... and its value (kept across commits)
     int unroll_choice = 1;       // partner batch depth of the force launch
-    int schedule_choice = 0;     // force launch schedule (0 slot per threads, 1 warp-balanced)
+    int schedule_choice = 0;     // force launch schedule (0 slot per threads, 1 warp-balanced, 2 block-vector)
     TermArrays t{};
 };
 
@@ -149,8 +149,8 @@ struct mjg_context {
     bool graphs = true;
     bool rollback = true;
     cudaStream_t stream = nullptr;
-    // branches of the step: one per global term (rebuild, gather, force) and
-    // one for the bonded terms, forked from and joined back into `stream`
+    // branches of the step: one per global term (rebuild, forces) and one for
+    // the bonded terms, forked from and joined back into `stream`
     cudaStream_t side[mjg::NGLOBAL + 1] = {};
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[mjg::NGLOBAL + 1] = {};
@@ -204,7 +204,7 @@ int64_t device_bytes(const mjg_context* c)
         const DevBuf* tb[] = {&t.part_particle, &t.part_p0, &t.part_p1, &t.part_lead, &t.part_sys,
                               &t.part_cell, &t.cell_count, &t.cell_start, &t.cell_fill,
                               &t.work, &t.part_chunks, &t.cell_chunks, &t.flagged, &t.slot_part, &t.slot_particle, &t.slot_lead,
-                              &t.slot_sys, &t.slot_pd, &t.slot_p1, &t.nnb, &t.nbr, &t.max_count,
+                              &t.slot_sys, &t.slot_pd, &t.slot_p1, &t.slot_of, &t.nnb, &t.nbr, &t.max_count,
                               &t.any_rebuild, &t.ex_start, &t.ex_idx};
         for(auto* x : tb) {b += (int64_t)x->cap;}
     }
@@ -253,13 +253,13 @@ void enqueue_forces(mjg_context* c, const Arena& a, bool nf, bool ne)
 
 // One integrator step without its closing half-kick.  kick: open with the
 // previous step's closing half-kick (fused into the same pass).
-// The step after the integrator's first pass forks into independent
-// branches: each global term rebuilds its lists (for the flagged systems),
-// refreshes its slot coordinates and, in the mixed form, adds its forces; the
-// bonded terms run beside them.  The mixed form's force launches add with
-// integer atomics (exact in any order), so all branches may overlap; the FP64
-// form adds its pair forces after the join, one term after the other, as the
-// reference does.
+// The step after the integrator's first pass (which also refreshes every
+// term's slot coordinates) forks into independent branches: each global term
+// rebuilds its lists (for the flagged systems) and, in the mixed form, adds
+// its forces; the bonded terms run beside them.  The mixed form's force
+// launches add with integer atomics (exact in any order), so all branches may
+// overlap; the FP64 form adds its pair forces after the join, one term after
+// the other.
 void enqueue_step_body(mjg_context* c, bool kick)
 {
     const Arena& a = c->arena;
@@ -281,7 +281,6 @@ void enqueue_step_body(mjg_context* c, bool kick)
         if(!t.on || t.np == 0) {continue;}
         branch(g, [&](cudaStream_t s) {
             launch_rebuild(a, g, t, 0, s);
-            launch_gather(a, t, s);
             if(mixed) {launch_pair(a, g, t, true, false, 0, s, false);}
         });
     }
@@ -1002,7 +1001,7 @@ void commit(mjg_context* c)
             DevBuf* bufs[] = {&T.part_particle, &T.part_p0, &T.part_p1, &T.part_lead, &T.part_sys,
                               &T.part_cell, &T.cell_count, &T.cell_start, &T.cell_fill,
                               &T.work, &T.part_chunks, &T.cell_chunks, &T.flagged, &T.slot_part, &T.slot_particle, &T.slot_lead,
-                              &T.slot_sys, &T.slot_pd, &T.slot_p1, &T.nnb, &T.nbr,
+                              &T.slot_sys, &T.slot_pd, &T.slot_p1, &T.slot_of, &T.nnb, &T.nbr,
                               &T.max_count, &T.any_rebuild};
             for(auto* b : bufs) {b->release();}
             T.cap_alloc = 0;
@@ -1037,6 +1036,8 @@ void commit(mjg_context* c)
         T.slot_sys.ensure(sizeof(int) * np);
         T.slot_pd.ensure(sizeof(double4) * np);
         T.slot_p1.ensure(sizeof(double) * np);
+        T.slot_of.ensure(sizeof(int) * (size_t)std::max<long long>(n_tot, 1));
+        CK(cudaMemsetAsync(T.slot_of.p, 0xff, T.slot_of.bytes, st));      // -1: no slot
         T.nnb.ensure(sizeof(int) * np);
         T.max_count.ensure(sizeof(int));
         T.any_rebuild.ensure(sizeof(int));
@@ -1061,6 +1062,9 @@ void commit(mjg_context* c)
         t.slot_sys = T.slot_sys.as<int>();
         t.slot_pd = T.slot_pd.as<double4>();
         t.slot_p1 = T.slot_p1.as<double>();
+        t.slot_of = T.slot_of.as<int>();
+        a.slot_pd[g] = t.slot_pd;
+        a.slot_of[g] = t.slot_of;
         t.nnb = T.nnb.as<int>();
         t.max_count = T.max_count.as<int>();
         t.any_rebuild = T.any_rebuild.as<int>();
@@ -1293,7 +1297,7 @@ void mjg_context_destroy(mjg_context* c)
         DevBuf* bufs[] = {&t.part_particle, &t.part_p0, &t.part_p1, &t.part_lead, &t.part_sys,
                           &t.part_cell, &t.cell_count, &t.cell_start, &t.cell_fill, &t.work, &t.part_chunks, &t.cell_chunks, &t.flagged,
                           &t.slot_part, &t.slot_particle, &t.slot_lead, &t.slot_sys, &t.slot_pd,
-                          &t.slot_p1, &t.nnb, &t.nbr, &t.max_count, &t.any_rebuild, &t.ex_start,
+                          &t.slot_p1, &t.slot_of, &t.nnb, &t.nbr, &t.max_count, &t.any_rebuild, &t.ex_start,
                           &t.ex_idx};
         for(auto* b : bufs) {b->release();}
     }
@@ -1873,7 +1877,7 @@ int mjg_set_pair_schedule(mjg_context* c, int term, int schedule)
 {
     ABI_BEGIN(c)
     if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "the schedule applies to global terms");}
-    if(schedule != 0 && schedule != 1) {throw Error(MJG_EINVAL, "schedule must be 0 or 1");}
+    if(schedule < 0 || schedule > 2) {throw Error(MJG_EINVAL, "schedule must be 0, 1 or 2");}
     TermDev& T = c->term[term - MJG_TERM_EXV];
     T.schedule_choice = schedule;
     if(T.t.schedule != schedule)

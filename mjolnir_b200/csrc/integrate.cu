@@ -102,6 +102,22 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
         }
         a.pos[i] = p;
         a.vel[i] = v;
+        // the pair kernels read coordinates in slot order: keep every term's
+        // copy current (a rebuild later in the step renumbers its systems'
+        // slots and rewrites them)
+#pragma unroll
+        for(int g = 0; g < NGLOBAL; ++g)
+        {
+            if(a.slot_of[g])
+            {
+                const int so = a.slot_of[g][i];
+                if(so >= 0)
+                {
+                    double* d = reinterpret_cast<double*>(a.slot_pd[g] + so);
+                    d[0] = p.x; d[1] = p.y; d[2] = p.z;
+                }
+            }
+        }
         zero_force<PREC>(a.force, i);
         d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
         if(!(d2 == d2) || d2 > 1e300) {atomicOr(&a.sys[s].status, ST_NONFINITE); d2 = 0.0;}

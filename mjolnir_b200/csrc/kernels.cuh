@@ -22,6 +22,10 @@ struct Arena {
     const long long* ex_start[NGLOBAL];
     const int*       ex_idx[NGLOBAL];
     const int*       mol;       // molecule id per particle (global numbering)
+    // slot coordinates of every global term, written by the integrator
+    // through the particle -> slot map (nullptr: term off)
+    double4*         slot_pd[NGLOBAL];
+    const int*       slot_of[NGLOBAL];
 };
 
 // Per global term arrays (participants grouped by system, input order inside).
@@ -32,7 +36,8 @@ struct TermArrays {
     int        cap;             // neighbour capacity per slot (a multiple of tpp)
     int        tpp;             // threads per slot of the pair kernel (1, 2, 4, 8, 16)
     int        unroll;          // partners requested per batch by the force launch (1, 2, 4)
-    int        schedule;        // force launch: 0 = slot per tpp threads, 1 = warp-balanced (mixed)
+    int        schedule;        // force launch: 0 = slot per tpp threads, 1 = warp-balanced (mixed),
+                                // 2 = one thread per slot reading tpp-word blocks of its list
     int        any_periodic;    // some system with this term has a periodic box
     const int* part_particle;   // [np] global particle index
     const double* part_p0;      // [np] radius / charge / sigma
@@ -52,7 +57,8 @@ struct TermArrays {
     unsigned char* slot_lead;   // [np]
     int*       slot_sys;        // [np]
     float4*    slot_pf;         // [np] packed per-slot parameters (mixed)
-    double4*   slot_pd;         // [np] x, y, z, p0 gathered each step
+    double4*   slot_pd;         // [np] x, y, z, p0 (kept current by the integrator)
+    int*       slot_of;         // [n] slot of each particle of the arena, -1 if none
     double*    slot_p1;         // [np] LJ epsilon per slot
     int*       nnb;             // [np] partners per slot
     int*       nbr;             // [cap * np] column-major
@@ -74,7 +80,8 @@ void launch_zero_force(const Arena& a, cudaStream_t s);
 void launch_rebuild(const Arena& a, int gterm, TermArrays& t, int force_all, cudaStream_t s);
 // slot coordinates of a term's participants (before its force launch)
 void launch_gather(const Arena& a, TermArrays& t, cudaStream_t s);
-// gather: refresh the slot coordinates first
+// gather: refresh the slot coordinates first (the step's launches rely on
+// the integrator and the rebuild having done so)
 void launch_pair(const Arena& a, int gterm, TermArrays& t, bool need_force, bool need_energy,
                  int calc_energy_form, cudaStream_t s, bool gather = true);
 

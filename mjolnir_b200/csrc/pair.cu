@@ -299,6 +299,68 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
     }
 }
 
+// Block-vector schedule: one thread per slot reads its list L words at a
+// time with one vector load (the blocked layout with L = tpp stores a slot's
+// words k .. k + L - 1 next to each other, 4 L bytes aligned), the next block
+// of words is requested before the current one is evaluated, and up to four
+// partner coordinates are requested together.  A slot's list then costs one
+// list latency per L partners instead of one per partner.
+template<int L>
+__device__ __forceinline__ void load_block(const int* __restrict__ p, int (&q)[L])
+{
+    if(L == 2)
+    {
+        const int2 v = __ldg(reinterpret_cast<const int2*>(p));
+        q[0] = v.x; q[1] = v.y;
+    }
+    else
+    {
+#pragma unroll
+        for(int c = 0; c < L / 4; ++c)
+        {
+            const int4 v = __ldg(reinterpret_cast<const int4*>(p) + c);
+            q[4 * c] = v.x; q[4 * c + 1] = v.y; q[4 * c + 2] = v.z; q[4 * c + 3] = v.w;
+        }
+    }
+}
+
+template<int PREC, int G, bool PER, int L>
+__global__ void __launch_bounds__(TPB) k_pair_vec(Arena a, TermArrays t)
+{
+    const long long s = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(s >= t.np) {return;}
+    const int sys = t.slot_sys[s];
+    double energy = 0.0;
+    bool ovf = false;
+    Acc<PREC> acc;
+    const PairEval<PREC, G, true, false, PER> eval(a, t, s, sys);
+    const long long np = t.np;
+    const int n = eval.S->frozen ? 0 : t.nnb[s];       // a frozen system keeps its forces
+    const double4* __restrict__ pd = t.slot_pd;
+    constexpr int W = L < 4 ? L : 4;                 // partners requested together
+    int q[L];
+    if(n > 0) {load_block<L>(t.nbr + s * L, q);}
+    for(int k = 0; k < n; k += L)
+    {
+        int qn[L];
+        if(k + L < n) {load_block<L>(t.nbr + ((long long)(k / L + 1) * np + s) * L, qn);}
+        const int m = min(L, n - k);
+#pragma unroll
+        for(int u0 = 0; u0 < L; u0 += W)
+        {
+            double4 pv[W];
+#pragma unroll
+            for(int u = 0; u < W; ++u) {pv[u] = u0 + u < m ? pd[q[u0 + u]] : eval.pi;}
+#pragma unroll
+            for(int u = 0; u < W; ++u) {if(u0 + u < m) {eval(pv[u], q[u0 + u], acc, energy, ovf);}}
+        }
+#pragma unroll
+        for(int u = 0; u < L; ++u) {q[u] = qn[u];}
+    }
+    acc.store(a.force, t.slot_particle[s]);
+    if(ovf) {atomicOr(&a.sys[sys].status, ST_FIXED_OVERFLOW);}
+}
+
 // Warp-balanced schedule of the mixed form's force launch: a warp owns 32
 // consecutive slots and splits the concatenation of their lists into 32 equal
 // contiguous chunks, one per lane, so every lane evaluates the same number of
@@ -431,6 +493,15 @@ void dispatch_per(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t 
     else if(nf)
     {
         // the per-step force launch: schedule and partner batch depth are tunable
+        if constexpr(TPP > 1)
+        {
+            if(t.schedule == 2)
+            {
+                const unsigned nv = (unsigned)((t.np + TPB - 1) / TPB);
+                k_pair_vec<PREC, G, PER, TPP><<<nv, TPB, 0, s>>>(a, t);
+                return;
+            }
+        }
         if(PREC == P_MIXED && t.schedule == 1)
         {
             const unsigned nw = (unsigned)((t.np + TPB - 1) / TPB);
