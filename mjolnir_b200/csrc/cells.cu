@@ -377,9 +377,22 @@ __global__ void k_rebuild_done(Arena a, int g, TermArrays t, int forced)
     if(s == 0) {t.work[0] = 0; t.work[1] = 0; t.work[2] = 0; *t.any_rebuild = 0;}
 }
 
+__global__ void k_scatter_param(TermArrays t, double* w)
+{
+    const long long p = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(p < t.np) {w[t.part_particle[p]] = t.part_p0[p];}
+}
+
 inline unsigned blocks(long long n, int tpb = TPB) {return (unsigned)((n + tpb - 1) / tpb);}
 
 }  // namespace
+
+void launch_scatter_param(const TermArrays& t, double* w, cudaStream_t s)
+{
+    if(!t.on || t.np == 0) {return;}
+    k_scatter_param<<<blocks(t.np), TPB, 0, s>>>(t, w);
+    note_launches(1);
+}
 
 void launch_rebuild(const Arena& a, int g, TermArrays& t, int force_all, cudaStream_t s)
 {

@@ -111,11 +111,7 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
             if(a.slot_of[g])
             {
                 const int so = a.slot_of[g][i];
-                if(so >= 0)
-                {
-                    double* d = reinterpret_cast<double*>(a.slot_pd[g] + so);
-                    d[0] = p.x; d[1] = p.y; d[2] = p.z;
-                }
+                if(so >= 0) {a.slot_pd[g][so] = make_double4(p.x, p.y, p.z, a.slot_w[g][i]);}   // whole 32 B
             }
         }
         zero_force<PREC>(a.force, i);

@@ -26,6 +26,7 @@ struct Arena {
     // through the particle -> slot map (nullptr: term off)
     double4*         slot_pd[NGLOBAL];
     const int*       slot_of[NGLOBAL];
+    const double*    slot_w[NGLOBAL];   // [n] the term's parameter of each particle (slot_pd.w)
 };
 
 // Per global term arrays (participants grouped by system, input order inside).
@@ -78,6 +79,8 @@ void launch_integrate_last(const Arena& a, cudaStream_t s);
 void launch_zero_force(const Arena& a, cudaStream_t s);
 
 void launch_rebuild(const Arena& a, int gterm, TermArrays& t, int force_all, cudaStream_t s);
+// w[particle] = the term's parameter of each participant (radius, charge, sigma)
+void launch_scatter_param(const TermArrays& t, double* w, cudaStream_t s);
 // slot coordinates of a term's participants (before its force launch)
 void launch_gather(const Arena& a, TermArrays& t, cudaStream_t s);
 // gather: refresh the slot coordinates first (the step's launches rely on
