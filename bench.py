@@ -351,10 +351,21 @@ def run_b200(args, ws, rank, local, pg):
     kern = pair_kernels(eng, descs, -1, "mixed")
     dom = max(kern, key=lambda k: kern[k]["ms"])
     k = kern[dom]
+    # DRAM bytes (read + write) of one launch from the ncu capture summarised
+    # in profiles/k_pair_batch256_mixed.md, per slot of the captured launch,
+    # scaled to this launch by its slots
+    ncu_bytes_per_slot = {"exv": 177.8e6 / 1563757, "dh": 117.3e6 / 312662}
+    traffic = ncu_bytes_per_slot[dom] * k["slots"] if dom in ncu_bytes_per_slot else None
     local_ms = {t: eng.time_kernel(t, reps=20) for t in ("bond", "angle", "dihedral")}
-    roofline = {"bound": "hbm", "kernel": f"k_pair<{dom}> (+ its slot gather)", "achieved": k["gbs"],
-                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": k["gbs"] / peak,
-                "traffic": None, "ms_per_launch": k["ms"], "pairs_in_cutoff": k["pcut"],
+    shape = eng.get_pair_schedule(dom), eng.get_threads_per_particle(dom), eng.get_pair_unroll(dom)
+    roofline = {"bound": "hbm", "kernel": f"pair force kernel of {dom} (schedule {shape[0]}, "
+                f"{shape[1]} threads or words per slot, {shape[2]} partners per batch)",
+                "achieved": k["gbs"], "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": k["gbs"] / peak, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                  "profiles/k_pair_batch256_mixed.md, scaled by slots",
+                "timing": "CUDA events per launch on the library stream, L2 evicted before each launch",
+                "ms_per_launch": k["ms"], "pairs_in_cutoff": k["pcut"],
                 "algorithmic_bytes": k["bytes"], "other": {t: kern[t] for t in kern if t != dom},
                 "local_ms_per_launch": local_ms}
 
