@@ -393,6 +393,40 @@ void compute_initial_forces(mjg_context* c)
 
 // ------------------------------------------------------------- commit
 
+// runs fn(i) for i in [0, n) on up to 16 host threads (work handed out one
+// index at a time); the first exception thrown is rethrown here
+template<typename F>
+void parallel_for(int64_t n, F fn)
+{
+    const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+    const int nt = (int)std::min<int64_t>(std::min<int64_t>(hw, 16), n);
+    if(nt <= 1)
+    {
+        for(int64_t i = 0; i < n; ++i) {fn(i);}
+        return;
+    }
+    std::atomic<int64_t> next{0};
+    std::exception_ptr err;
+    std::mutex m;
+    auto work = [&]() {
+        try
+        {
+            for(int64_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {fn(i);}
+        }
+        catch(...)
+        {
+            std::lock_guard<std::mutex> l(m);
+            if(!err) {err = std::current_exception();}
+            next.store(n);
+        }
+    };
+    std::vector<std::thread> th;
+    for(int t = 1; t < nt; ++t) {th.emplace_back(work);}
+    work();
+    for(auto& t : th) {t.join();}
+    if(err) {std::rethrow_exception(err);}
+}
+
 int kind_id(std::map<std::string, int>& kinds, const std::string& k)
 {
     auto it = kinds.find(k);
@@ -438,14 +472,13 @@ void save_resident_state(mjg_context* c)
         launch_pack_state(c->arena, st, field, 0, c->n_tot, c->stream);
         CK(cudaMemcpyAsync(h, st, sizeof(double) * per, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        for(size_t k = 0; k < c->arena_ids.size(); ++k)
-        {
+        parallel_for((int64_t)c->arena_ids.size(), [&](int64_t k) {
             HostSystem& s = c->sys[c->arena_ids[k]];
-            if(!s.alive) {continue;}
+            if(!s.alive) {return;}
             std::vector<double>& dst = field == 0 ? s.pos : field == 1 ? s.vel : s.force;
             dst.assign(h + 3 * s.off, h + 3 * (s.off + s.n));
             if(field == 2) {s.force_valid = true;}
-        }
+        });
     }
 }
 
@@ -518,40 +551,6 @@ void derive(HostSystem& s)
     order(s.angle, 3);
     order(s.dihd, 4);
     s.derived = true;
-}
-
-// runs fn(i) for i in [0, n) on up to 16 host threads (work handed out one
-// index at a time); the first exception thrown is rethrown here
-template<typename F>
-void parallel_for(int64_t n, F fn)
-{
-    const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
-    const int nt = (int)std::min<int64_t>(std::min<int64_t>(hw, 16), n);
-    if(nt <= 1)
-    {
-        for(int64_t i = 0; i < n; ++i) {fn(i);}
-        return;
-    }
-    std::atomic<int64_t> next{0};
-    std::exception_ptr err;
-    std::mutex m;
-    auto work = [&]() {
-        try
-        {
-            for(int64_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {fn(i);}
-        }
-        catch(...)
-        {
-            std::lock_guard<std::mutex> l(m);
-            if(!err) {err = std::current_exception();}
-            next.store(n);
-        }
-    };
-    std::vector<std::thread> th;
-    for(int t = 1; t < nt; ++t) {th.emplace_back(work);}
-    work();
-    for(auto& t : th) {t.join();}
-    if(err) {std::rethrow_exception(err);}
 }
 
 // carves typed arrays out of the context's page-locked packing buffer

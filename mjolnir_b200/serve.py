@@ -274,7 +274,7 @@ def poisson_workload(rate: float, duration: float, seed: int = 7, nmin: int = 20
 
 def serve_poisson(duration: float = 60.0, rate: float = 200.0, chunk: int = 2000, seed: int = 7,
                   precision: str = "mixed", max_particles: int = 2_000_000,
-                  chunk_seconds: float = 0.5, min_commit_interval: float = 0.5) -> dict:
+                  chunk_seconds: float = 1.0, min_commit_interval: float = 1.0) -> dict:
     """Replays a Poisson stream in real time for `duration` seconds and
     reports completion latency, queue depth and aggregate throughput."""
     jobs = poisson_workload(rate, duration, seed=seed)
