@@ -87,6 +87,19 @@ MJG_API int mjg_system_set_attributes(mjg_context* ctx, int sys, double temperat
  * (forcefield/local/DummyInteraction.hpp). */
 MJG_API int mjg_system_add_connections(mjg_context* ctx, int sys, const char* kind,
                                int64_t m, const int64_t* pairs);
+/* Changes a system's temperature at any time: the Langevin noise coefficients
+ * of its particles take the new value from the next step on, as
+ * BAOABLangevinIntegrator::update does after SimulatedAnnealingSimulator sets
+ * the temperature attribute (core/SimulatedAnnealingSimulator.hpp:144-154,
+ * core/BAOABLangevinIntegrator.hpp:47-58).  DebyeHuckel keeps the Debye
+ * length of the committed temperature, as the reference's annealing does. */
+MJG_API int mjg_system_set_temperature(mjg_context* ctx, int sys, double temperature);
+/* Sets the integrator's step counter of a system before its first commit
+ * (default 0).  The Langevin noise of particle i at step t is Philox keyed by
+ * (seed, i, t), so a system restored from a checkpoint with the step it had
+ * continues the same noise stream.  The reference keeps its mt19937 state in
+ * the checkpoint's _rng.msg instead (core/MsgPackSaver.hpp:66-87). */
+MJG_API int mjg_system_set_step(mjg_context* ctx, int sys, uint64_t step);
 /* Freezes (1) or releases (0) a system: while frozen it does not advance in
  * mjg_step and its forces, energies and state stay as they are (its terms are
  * not evaluated), so a finished job can wait in the arena until the next

@@ -8,7 +8,8 @@ the per-term energies and the kinetic energy to ``<path>/<prefix>.ene`` and a
 frame of positions to ``<path>/<prefix>.xyz`` (the quantities the reference's
 EnergyObserver and XYZObserver write; core/EnergyObserver.hpp:89-153).
 ``precision = "double"`` in the input selects the FP64 form unless
-``--precision`` says otherwise.
+``--precision`` says otherwise.  A ``SimulatedAnnealing`` input follows its
+linear temperature schedule (:mod:`mjolnir_b200.anneal`).
 """
 from __future__ import annotations
 
@@ -19,6 +20,7 @@ import time
 
 import numpy as np
 
+from .anneal import current
 from .engine import Engine
 from .input import load
 
@@ -55,21 +57,28 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
     sid = eng.add_system(d)
     eng.commit()
     t0 = time.perf_counter()
+    anneal = inp.schedule                    # SimulatedAnnealing: (first, last, each_step)
+    r_total = 1.0 / total if total else 0.0
     with open(ene_path, "w") as ene, open(xyz_path, "w") as xyz:
         ene.write("# timestep " + " ".join(TERM_LABEL[t] for t in terms) + " kinetic_energy\n")
         done = 0
         while True:
-            e = eng.energies(sid)
-            p, v, _ = eng.state(sid)
-            kin = 0.5 * float(np.sum(d.mass[:, None] * v * v))
-            ene.write(f"{done} " + " ".join(f"{e[t]:.10e}" for t in terms) + f" {kin:.10e}\n")
-            xyz.write(f"{d.n}\nstep = {done}\n")
-            xyz.write("".join(f"X {x:.6f} {y:.6f} {z:.6f}\n" for x, y, z in p))
+            if done % save == 0 or done >= total:
+                e = eng.energies(sid)
+                p, v, _ = eng.state(sid)
+                kin = 0.5 * float(np.sum(d.mass[:, None] * v * v))
+                ene.write(f"{done} " + " ".join(f"{e[t]:.10e}" for t in terms) + f" {kin:.10e}\n")
+                xyz.write(f"{d.n}\nstep = {done}\n")
+                xyz.write("".join(f"X {x:.6f} {y:.6f} {z:.6f}\n" for x, y, z in p))
             if done >= total:
                 break
-            k = min(save, total - done)
+            k = min(save - done % save, total - done)
+            if anneal:
+                k = min(k, anneal[2] - done % anneal[2])
             eng.step(k)
             done += k
+            if anneal and done % anneal[2] == 0:    # core/SimulatedAnnealingSimulator.hpp:144-154
+                eng.set_temperature(sid, current(anneal[0], anneal[1], done * r_total))
     wall = time.perf_counter() - t0
     eng.close()
     res = {"steps": total, "particles": d.n, "precision": prec, "wall_s": wall,

@@ -36,6 +36,8 @@ SIGNATURES = {
     "mjg_system_set_attributes": (C.c_int, [_ctx, C.c_int, C.c_double, C.c_double]),
     "mjg_system_add_connections": (C.c_int, [_ctx, C.c_int, C.c_char_p, C.c_int64, _i64p]),
     "mjg_system_remove": (C.c_int, [_ctx, C.c_int]),
+    "mjg_system_set_step": (C.c_int, [_ctx, C.c_int, C.c_uint64]),
+    "mjg_system_set_temperature": (C.c_int, [_ctx, C.c_int, C.c_double]),
     "mjg_system_freeze": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "mjg_exv_set": (C.c_int, [_ctx, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int64, _i64p, _f64p]),
     "mjg_dh_set": (C.c_int, [_ctx, C.c_int, C.c_double, C.c_double, C.c_int64, _i64p, _f64p]),

@@ -1362,6 +1362,31 @@ int mjg_system_create(mjg_context* c, int64_t n, int boundary, const double* low
     ABI_END(c)
 }
 
+int mjg_system_set_temperature(mjg_context* c, int sys, double T)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(!(T > 0)) {throw Error(MJG_EINVAL, "temperature must be positive");}
+    s.T = T;
+    if(!c->committed || !s.resident || s.integrator != I_BAOAB) {return MJG_OK;}
+    // BAOABLangevinIntegrator::update -> reset_parameters (:47-58, :73-99): the
+    // noise coefficients of the system's particles, computed as at commit
+    const Units u;
+    const double kBT = u.kB * s.T;
+    std::vector<double> z((size_t)s.n);
+    for(int64_t i = 0; i < s.n; ++i)
+    {
+        const double gamma_dt = -1 * s.gamma[i] * s.dt;
+        z[i] = std::sqrt(kBT * (1 - std::exp(2 * gamma_dt)) * (1.0 / s.mass[i]));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    double* stg = c->d_staging.as<double>();
+    CK(cudaMemcpyAsync(stg, z.data(), sizeof(double) * s.n, cudaMemcpyHostToDevice, c->stream));
+    launch_set_noise(c->arena, stg, s.off, s.n, c->stream);
+    CK(cudaStreamSynchronize(c->stream));
+    ABI_END(c)
+}
+
 int mjg_system_set_attributes(mjg_context* c, int sys, double T, double I)
 {
     ABI_BEGIN(c)
@@ -1384,6 +1409,15 @@ int mjg_system_add_connections(mjg_context* c, int sys, const char* kind, int64_
         if(i < 0 || j < 0 || i >= s.n || j >= s.n) {throw Error(MJG_EINVAL, "connection index out of range");}
         s.connections.push_back({kind, {i, j}});
     }
+    ABI_END(c)
+}
+
+int mjg_system_set_step(mjg_context* c, int sys, uint64_t step)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "the step counter is set before the first commit");}
+    s.step = step;
     ABI_END(c)
 }
 

@@ -227,6 +227,12 @@ __global__ void k_set_force(Arena a, const double* src, long long first, long lo
     }
 }
 
+__global__ void k_set_noise(Arena a, const double* src, long long first, long long count)
+{
+    const long long k = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(k < count) {a.coef[first + k].z = src[k];}
+}
+
 __global__ void k_clear_energy(Arena a)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -300,6 +306,14 @@ void launch_clear_energy(const Arena& a, cudaStream_t s)
 {
     if(a.nsys == 0) {return;}
     k_clear_energy<<<(a.nsys + 127) / 128, 128, 0, s>>>(a);
+    note_launches(1);
+}
+
+void launch_set_noise(const Arena& a, const double* noise, long long first, long long count,
+                      cudaStream_t s)
+{
+    if(count == 0) {return;}
+    k_set_noise<<<blocks(count), TPB, 0, s>>>(a, noise, first, count);
     note_launches(1);
 }
 

@@ -111,6 +111,9 @@ void launch_local(const Arena& a, const LocalArrays& l, int which_mask, bool nee
 void launch_clear_energy(const Arena& a, cudaStream_t s);
 void launch_count_cut(const Arena& a, int g, TermArrays& t, int sys, unsigned long long* out,
                       cudaStream_t s);
+// coef[first + k].z = noise[k] (the Langevin noise coefficient) for k < count
+void launch_set_noise(const Arena& a, const double* noise, long long first, long long count,
+                      cudaStream_t s);
 // writes host-layout forces [3 count] (staging) into the arena's force array
 void launch_set_force(const Arena& a, const double* src, long long first, long long count,
                       cudaStream_t s);

@@ -115,11 +115,17 @@ class Engine:
         kind = A.VELOCITY_VERLET if d.integrator == "VelocityVerlet" else A.BAOAB
         gam = _arr(d.gamma if d.gamma is not None else np.zeros(d.n), np.float64)
         self._c(L.mjg_integrator_set(self.ctx, s, kind, float(d.dt), A.f64(gam), int(d.seed) & ((1 << 64) - 1)))
+        if d.start_step:
+            self._c(L.mjg_system_set_step(self.ctx, s, int(d.start_step)))
         return s
 
     def remove_system(self, sid: int):
         self._c(self.lib.mjg_system_remove(self.ctx, sid))
         self.n_of.pop(sid, None)
+
+    def set_temperature(self, sid: int, temperature: float):
+        """Langevin temperature from the next step on (simulated annealing)."""
+        self._c(self.lib.mjg_system_set_temperature(self.ctx, sid, float(temperature)))
 
     def freeze(self, sid: int, frozen: bool = True):
         self._c(self.lib.mjg_system_freeze(self.ctx, sid, 1 if frozen else 0))

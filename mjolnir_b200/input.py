@@ -12,14 +12,16 @@ ready for :meth:`Engine.add_system`:
   (input/read_table_from_file.hpp:38-91);
 * ``[units]``: ``length = "angstrom"`` and ``energy = "kcal/mol"`` only (the
   constants of input/read_units.hpp:32-91 for those units are built in);
-* ``[simulator]``: ``type = "MolecularDynamics"``, ``boundary_type``,
+* ``[simulator]``: ``type = "MolecularDynamics"`` or ``"SimulatedAnnealing"``
+  (``schedule = {type = "linear", begin, end}``, ``each_step``), ``boundary_type``,
   ``precision``, ``parallelism``, ``seed`` (or the deprecated
   ``integrator.seed``), ``delta_t``, ``total_step``, ``save_step``,
   ``integrator.type`` = ``"BAOABLangevin"`` (``gammas`` or the deprecated
   ``parameters``, input/read_integrator.hpp:120-187) or ``"VelocityVerlet"``;
 * ``[[systems]]`` (the first): ``attributes``, ``boundary_shape``,
   ``particles`` with ``mass|m``, ``position|pos``, ``velocity|vel``, ``name``,
-  ``group`` (input/read_system.hpp:93-290);
+  ``group`` (input/read_system.hpp:93-290), or ``file_name = "x.msg"``, a
+  checkpoint in the reference's MsgPack layout (:mod:`mjolnir_b200.checkpoint`);
 * ``[[forcefields]]`` (the first): ``[[forcefields.local]]`` BondLength /
   BondAngle with Harmonic (``k``, ``v0``) and DihedralAngle with Cosine
   (``k``, ``n``, ``v0``), ``indices`` plus an optional ``offset``
@@ -65,7 +67,7 @@ class InputError(ValueError):
 @dataclasses.dataclass
 class Input:
     desc: SystemDesc
-    simulator: str
+    simulator: str                  # "MolecularDynamics" | "SimulatedAnnealing"
     precision: str                  # "double" | "float"
     parallelism: str
     total_step: int
@@ -75,6 +77,7 @@ class Input:
     output_path: str
     output_format: str
     input_path: str
+    schedule: Optional[tuple] = None   # SimulatedAnnealing: (first, last, each_step)
 
 
 # ------------------------------------------------------------------ helpers
@@ -186,12 +189,15 @@ def _units(root):
 
 
 def _simulator(sim):
-    _check_keys(sim, {"type", "boundary_type", "precision", "parallelism", "seed", "total_step",
-                      "save_step", "checkpoint_step", "delta_t", "integrator", "forcefields", "env"},
-                "[simulator]")
     typ = sim.get("type")
-    if typ != "MolecularDynamics":
-        raise InputError(f'[simulator] type "{typ}": only "MolecularDynamics" is supported')
+    keys = {"type", "boundary_type", "precision", "parallelism", "seed", "total_step",
+            "save_step", "checkpoint_step", "delta_t", "integrator", "forcefields", "env"}
+    if typ == "SimulatedAnnealing":                 # input/read_simulator.hpp:84-160
+        keys |= {"schedule", "each_step"}
+    elif typ != "MolecularDynamics":
+        raise InputError(f'[simulator] type "{typ}": only "MolecularDynamics" and '
+                         '"SimulatedAnnealing" are supported')
+    _check_keys(sim, keys, "[simulator]")
     bt = sim.get("boundary_type")
     if bt not in ("Unlimited", "Periodic", "PeriodicCuboid"):
         raise InputError(f'[simulator] boundary_type "{bt}" is not one of Unlimited, PeriodicCuboid')
@@ -413,8 +419,22 @@ def load(path: str) -> Input:
     systems = root.get("systems")
     if not systems:
         raise InputError("[[systems]] is required")
-    sysd = _from_file(systems[0], "systems", input_path, base_dir)
-    pos, vel, mass, has_vel, attrs, lower, upper = _system(sysd, boundary)
+    first = systems[0]
+    if isinstance(first, dict) and str(first.get("file_name", "")).endswith(".msg"):
+        # a checkpoint (input/read_system.hpp:105-131): state, box and
+        # attributes from the MsgPack file
+        from .checkpoint import CheckpointError, read_system
+        try:
+            ck = read_system(_resolve(input_path, first["file_name"], base_dir))
+        except CheckpointError as e:
+            raise InputError(str(e)) from None
+        if ck["periodic"] != (boundary == "PeriodicCuboid"):
+            raise InputError("the checkpoint's boundary does not match [simulator] boundary_type")
+        pos, vel, mass, has_vel = ck["pos"], ck["vel"], ck["mass"], True
+        attrs, lower, upper = ck["attributes"], ck["lower"], ck["upper"]
+    else:
+        sysd = _from_file(first, "systems", input_path, base_dir)
+        pos, vel, mass, has_vel, attrs, lower, upper = _system(sysd, boundary)
     n = pos.shape[0]
     temperature = float(attrs.get("temperature", 300.0))
     ionic = float(attrs.get("ionic_strength", 0.1))
@@ -428,6 +448,18 @@ def load(path: str) -> Input:
     if pairs and not has_vel and "temperature" not in attrs:
         raise InputError("generating velocities needs systems.attributes.temperature")
     integrator, gamma = _integrator(integ, n)
+    schedule = None
+    if sim["type"] == "SimulatedAnnealing":
+        sch = sim.get("schedule")
+        if not isinstance(sch, dict) or "each_step" not in sim:
+            raise InputError("SimulatedAnnealing needs [simulator] schedule and each_step")
+        _check_keys(sch, {"type", "begin", "end", "each_step"}, "[simulator.schedule]")
+        if sch.get("type") != "linear":
+            raise InputError('schedule.type: only "linear" is supported')
+        if integrator != "BAOAB":
+            raise InputError("SimulatedAnnealing needs a Langevin integrator")
+        schedule = (float(sch["begin"]), float(sch["end"]), int(sim["each_step"]))
+        temperature = schedule[0]                   # current(0), set before initialisation
     if boundary == "PeriodicCuboid":              # System::initialize wraps positions
         lo, up = np.array(lower), np.array(upper)
         w = up - lo
@@ -456,7 +488,7 @@ def load(path: str) -> Input:
     if "DihedralAngle" in locs:
         topo, idx, k, v0, nn = locs["DihedralAngle"]
         desc.dihedrals, desc.dihedral_topology = (idx, k, nn, v0), topo
-    return Input(desc=desc, simulator="MolecularDynamics", precision=prec, parallelism=par,
+    return Input(desc=desc, simulator=sim["type"], schedule=schedule, precision=prec, parallelism=par,
                  total_step=int(sim["total_step"]), save_step=int(sim["save_step"]), seed=seed,
                  output_prefix=str(out.get("prefix", "mjolnir")), output_path=str(out.get("path", "./")),
                  output_format=str(out.get("format", "xyz")), input_path=input_path)

@@ -62,6 +62,7 @@ class SystemDesc:
     dt: float = 0.01
     gamma: Optional[np.ndarray] = None
     seed: int = 12345
+    start_step: int = 0                # noise step counter to resume from (checkpoints)
 
     @property
     def n(self) -> int:

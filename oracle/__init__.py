@@ -186,6 +186,7 @@ def _oracle_lib():
         lib.orc_term_energy.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p]
         lib.orc_init_dynamics.argtypes = [C.c_void_p]
         lib.orc_run.argtypes = [C.c_void_p, C.c_int64]
+        lib.orc_set_temperature.argtypes = [C.c_void_p, C.c_double]
         lib.orc_get_state.argtypes = [C.c_void_p, _f64p, _f64p, _f64p]
         lib.orc_rebuild_count.restype = C.c_int64
         lib.orc_rebuild_count.argtypes = [C.c_void_p, C.c_int]
@@ -266,6 +267,9 @@ class Oracle(_Common):
     def run(self, nsteps):
         self.lib.orc_run(self._h, int(nsteps))
 
+    def set_temperature(self, T):
+        self.lib.orc_set_temperature(self._h, float(T))
+
     def state(self):
         p, v, f = (np.empty((self.n, 3)) for _ in range(3))
         self.lib.orc_get_state(self._h, _ptr(p, C.c_double), _ptr(v, C.c_double), _ptr(f, C.c_double))
@@ -344,6 +348,11 @@ def _ref_lib():
         lib.ref_total_energy.restype = C.c_double
         lib.ref_total_energy.argtypes = [C.c_void_p]
         lib.ref_max_threads.restype = C.c_int
+        lib.ref_save_msgpack.restype = C.c_int
+        lib.ref_save_msgpack.argtypes = [C.c_void_p, C.c_char_p]
+        lib.ref_load_msgpack.restype = C.c_longlong
+        lib.ref_load_msgpack.argtypes = [C.c_char_p, C.c_int, C.c_longlong, _f64p, _f64p, _f64p, _f64p,
+                                         _f64p, _f64p, _f64p, _f64p]
         _rlib = lib
     return _rlib
 
@@ -406,6 +415,28 @@ class Reference(_Common):
 
     def total_energy(self):
         return self.lib.ref_total_energy(self._h)
+
+    def save_msgpack(self, prefix: str):
+        """The reference's MsgPackSaver on the current state: writes
+        prefix + "_system.msg"."""
+        if self.lib.ref_save_msgpack(self._h, prefix.encode()):
+            raise RuntimeError("ref_save_msgpack: " + self.lib.ref_last_error().decode())
+
+    @staticmethod
+    def load_msgpack(path: str, periodic: bool, n_max: int = 1 << 22) -> dict:
+        """The reference's MsgPackLoader::load_system on a file."""
+        lib = _ref_lib()
+        pos, vel, force = (np.empty((n_max, 3)) for _ in range(3))
+        mass = np.empty(n_max)
+        lo, up = np.zeros(3), np.zeros(3)
+        t, i = C.c_double(0), C.c_double(0)
+        n = lib.ref_load_msgpack(path.encode(), 1 if periodic else 0, n_max, _ptr(pos, C.c_double),
+                                 _ptr(vel, C.c_double), _ptr(force, C.c_double), _ptr(mass, C.c_double),
+                                 _ptr(lo, C.c_double), _ptr(up, C.c_double), C.byref(t), C.byref(i))
+        if n < 0:
+            raise RuntimeError("ref_load_msgpack: " + lib.ref_last_error().decode())
+        return {"pos": pos[:n], "vel": vel[:n], "force": force[:n], "mass": mass[:n], "lower": lo,
+                "upper": up, "temperature": t.value, "ionic_strength": i.value}
 
     @staticmethod
     def max_threads():

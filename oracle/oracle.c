@@ -1034,6 +1034,23 @@ int orc_init_dynamics(orc_state* st)
     return 0;
 }
 
+/* BAOABLangevinIntegrator::update (:47-58) after the system's temperature
+ * attribute changed (SimulatedAnnealingSimulator::step,
+ * core/SimulatedAnnealingSimulator.hpp:144-154): reset_parameters with the new
+ * temperature.  The DebyeHuckel parameters keep the old temperature, as in the
+ * reference. */
+void orc_set_temperature(orc_state* st, double T)
+{
+    st->T = T;
+    const double kBT = st->kB * st->T;
+    for(int64_t i=0; i<st->n; ++i)
+    {
+        const double gamma_dt = -1 * st->gamma[i] * st->dt;
+        st->exp_gamma_dt[i] = exp(gamma_dt);
+        st->noise_coeff[i]  = sqrt(kBT * (1 - exp(2 * gamma_dt)) * st->rmass[i]);
+    }
+}
+
 /* GlobalPairInteraction::reduce_margin -> ...GridCellList::reduce_margin */
 static void reduce_margin(orc_state* st, double dmargin)
 {

@@ -23,6 +23,8 @@
 #include <mjolnir/core/System.hpp>
 #include <mjolnir/core/ForceField.hpp>
 #include <mjolnir/core/Unit.hpp>
+#include <mjolnir/core/MsgPackSaver.hpp>
+#include <mjolnir/core/MsgPackLoader.hpp>
 #include <mjolnir/core/BAOABLangevinIntegrator.hpp>
 #include <mjolnir/core/VelocityVerletIntegrator.hpp>
 #include <mjolnir/core/PeriodicGridCellList.hpp>
@@ -88,6 +90,7 @@ struct RefSimBase
     virtual void get_state(double* pos, double* vel, double* force) = 0;
     virtual void total_force(double* force) = 0;
     virtual double total_energy() = 0;
+    virtual void save_msgpack(const std::string& prefix) = 0;
 };
 
 template<typename coordT>
@@ -413,6 +416,13 @@ struct RefSim final : public RefSimBase
                          : vv->step(time, *sys, ff, rng);
         }
     }
+    // MsgPackSaver::save(System) writes prefix + "_system.msg"
+    void save_msgpack(const std::string& prefix) override
+    {
+        MsgPackSaver<traitsT> saver(prefix);
+        saver.save(*sys);
+    }
+
     void get_state(double* pos, double* vel, double* force) override
     {
         for(std::size_t i=0; i<sys->size(); ++i)
@@ -444,6 +454,27 @@ RefSimBase* make_sim(const orc_spec& s)
         return new RefSim<traitsT<double, CuboidalPeriodicBoundary>, Seq>(s);
     }
     return new RefSim<traitsT<double, UnlimitedBoundary>, Seq>(s);
+}
+
+template<typename sysT>
+long long copy_system(const sysT& sys, long long cap, double* pos, double* vel, double* force,
+                      double* mass, double* temperature, double* ionic_strength)
+{
+    const long long n = (long long)sys.size();
+    for(long long i = 0; i < n && i < cap; ++i)
+    {
+        for(int x = 0; x < 3; ++x)
+        {
+            pos[3 * i + x]   = sys.position(i)[x];
+            vel[3 * i + x]   = sys.velocity(i)[x];
+            force[3 * i + x] = sys.force(i)[x];
+        }
+        mass[i] = sys.mass(i);
+    }
+    const auto& at = sys.attributes();
+    *temperature    = at.count("temperature")    ? at.at("temperature")    : 0.0;
+    *ionic_strength = at.count("ionic_strength") ? at.at("ionic_strength") : 0.0;
+    return n;
 }
 
 } // anonymous
@@ -505,6 +536,53 @@ void ref_get_state(void* h, double* pos, double* vel, double* force)
 }
 void ref_total_force(void* h, double* force) {static_cast<RefSimBase*>(h)->total_force(force);}
 double ref_total_energy(void* h) {return static_cast<RefSimBase*>(h)->total_energy();}
+
+// The reference's checkpoint writer on the current system state.
+int ref_save_msgpack(void* h, const char* prefix)
+{
+    try
+    {
+        static_cast<RefSimBase*>(h)->save_msgpack(prefix);
+        return 0;
+    }
+    catch(const std::exception& e)
+    {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// The reference's checkpoint reader (MsgPackLoader::load_system): copies out
+// what it read.  periodic selects the boundary type the file must hold.
+// Returns the number of particles, or -1 (ref_last_error) on failure; copies
+// at most cap particles.
+long long ref_load_msgpack(const char* file, int periodic, long long cap, double* pos,
+                           double* vel, double* force, double* mass, double* lower,
+                           double* upper, double* temperature, double* ionic_strength)
+{
+    try
+    {
+        if(periodic)
+        {
+            MsgPackLoader<SimulatorTraits<double, CuboidalPeriodicBoundary>> loader;
+            const auto sys = loader.load_system(file);
+            for(int x = 0; x < 3; ++x)
+            {
+                lower[x] = sys.boundary().lower_bound()[x];
+                upper[x] = sys.boundary().upper_bound()[x];
+            }
+            return copy_system(sys, cap, pos, vel, force, mass, temperature, ionic_strength);
+        }
+        MsgPackLoader<SimulatorTraits<double, UnlimitedBoundary>> loader;
+        const auto sys = loader.load_system(file);
+        return copy_system(sys, cap, pos, vel, force, mass, temperature, ionic_strength);
+    }
+    catch(const std::exception& e)
+    {
+        g_error = e.what();
+        return -1;
+    }
+}
 
 int ref_max_threads(void)
 {

@@ -260,3 +260,26 @@ def test_launch_shapes_give_the_same_trajectory(precision):
                 assert np.array_equal(a, b), (sch, tpp, unr)
             else:
                 assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max(), (sch, tpp, unr)
+
+
+def test_simulated_annealing_matches_oracle():
+    """A linear annealing schedule (temperature updated every 25 steps) on the
+    GPU follows the oracle driven by the same Philox stream and schedule."""
+    from mjolnir_b200 import anneal
+    d = S.polymer_melt(nchains=6, nbeads=60, radius=60.0, seed=6)
+    first, last, total, each = 400.0, 250.0, 100, 25
+    d.temperature = first
+    o = oracle.Oracle(d)
+    o.init_dynamics()
+    done = 0
+    while done < total:
+        o.run(each)
+        done += each
+        o.set_temperature(anneal.current(first, last, done * (1.0 / total)))
+    po, vo, _ = o.state()
+    e, sid = engine_for(d, "fp64")
+    anneal.run(e, {sid: (first, last)}, total, each)
+    p, v, _ = e.state(sid)
+    assert np.abs(p - po).max() <= 1e-9
+    assert np.abs(v - vo).max() <= 1e-8
+    e.close()

@@ -212,3 +212,21 @@ parameters = [{index = 0, charge = 1.0}, {index = 3, charge = -1.0}]
     assert d.dh.cutoff == 5.5
     with pytest.raises(NotImplementedError):
         oracle.make_spec(d)
+
+
+def test_simulated_annealing_input(tmp_path):
+    text = HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF
+    text = text.replace('type          = "MolecularDynamics"', 'type          = "SimulatedAnnealing"')
+    text = text.replace('save_step     = 10', 'save_step     = 10\neach_step     = 5\n'
+                        'schedule = {type = "linear", begin = 350.0, end = 280.0}')
+    inp = I.load(_write(tmp_path, "anneal.toml", text))
+    assert inp.simulator == "SimulatedAnnealing" and inp.schedule == (350.0, 280.0, 5)
+    assert inp.desc.temperature == 350.0            # current(0) before initialisation
+    with pytest.raises(I.InputError, match="linear"):
+        I.load(_write(tmp_path, "bad.toml", text.replace('"linear"', '"exponential"')))
+
+
+def test_linear_schedule_matches_reference_formula():
+    from mjolnir_b200.anneal import current
+    assert current(350.0, 280.0, 0.0) == 350.0 and current(350.0, 280.0, 1.0) == 280.0
+    assert current(300.0, 100.0, 0.25) == 300.0 * 0.75 + 100.0 * 0.25
