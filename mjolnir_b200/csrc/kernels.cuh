@@ -57,7 +57,6 @@ struct TermArrays {
     int*       slot_particle;   // [np] global particle of slot
     unsigned char* slot_lead;   // [np]
     int*       slot_sys;        // [np]
-    float4*    slot_pf;         // [np] packed per-slot parameters (mixed)
     double4*   slot_pd;         // [np] x, y, z, p0 (kept current by the integrator)
     int*       slot_of;         // [n] slot of each particle of the arena, -1 if none
     double*    slot_p1;         // [np] LJ epsilon per slot
