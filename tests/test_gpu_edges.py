@@ -37,6 +37,7 @@ def test_edges_against_oracle(name, precision):
             assert np.abs(f).max() == 0
         assert abs(en - eo) <= FORCE_TOL[precision] * max(abs(eo), 1e-12), (name, t, en, eo)
     e.step(200)
+    e.rebuild()                                  # lists at the current coordinates
     p, v, f = e.state(sid)
     assert np.all(np.isfinite(p)) and np.all(np.isfinite(v))
     for t in ("exv", "dh", "lj"):
