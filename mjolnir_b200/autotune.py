@@ -7,7 +7,8 @@ For every global term of an :class:`~mjolnir_b200.engine.Engine` it picks
   * the pair kernel's launch shape, by timing the kernel alone: the schedule
     (one particle per group of threads; warp-balanced over the lists of a
     warp's 32 particles, mixed form only; or one thread per particle reading
-    its list in blocks with vector loads), the threads per particle / list
+    its list in blocks with vector loads, optionally with each block's
+    threads ordered by list length), the threads per particle / list
     block (1, 2, 4, 8, 16) and the partners each thread requests per batch
     (1, 2, 4).
 In the mixed form neither choice changes a result: the fixed-point force sums
@@ -31,7 +32,7 @@ def _time_steps(eng, nsteps: int) -> float:
 
 
 def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
-         tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1, 2), steps: int = 60,
+         tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1, 2, 3), steps: int = 60,
          warm: int = 20, log=None) -> dict:
     present = []
     for t in terms:
@@ -73,10 +74,10 @@ def _tune_shape(eng, term, tpps, unrolls, schedules):
     for sch in schedules:
         eng.set_pair_schedule(term, sch)
         for p in tpps:
-            if sch == 2 and p == 1:
+            if sch in (2, 3) and p == 1:
                 continue                  # the same launch as schedule 0
             eng.set_threads_per_particle(term, p)
-            for u in (unrolls if sch != 2 else (1,)):
+            for u in (unrolls if sch not in (2, 3) else (1,)):
                 eng.set_pair_unroll(term, u)
                 ms = eng.time_kernel(term, reps=10)
                 if best is None or ms < best[0]:
@@ -85,7 +86,7 @@ def _tune_shape(eng, term, tpps, unrolls, schedules):
 
 
 def tune_shapes(eng, terms=("exv", "dh", "lj"), tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4),
-                schedules=(0, 1, 2)) -> dict:
+                schedules=(0, 1, 2, 3)) -> dict:
     """Launch shape only (margins as committed): for a single large system,
     where the margin is fixed by the input."""
     out = {}

@@ -136,7 +136,8 @@ struct TermDev {
     bool tpp_fixed = false;      // threads per slot chosen by the caller
     int tpp_choice = 1;          // ... and its value (kept across commits)
     int unroll_choice = 1;       // partner batch depth of the force launch
-    int schedule_choice = 0;     // force launch schedule (0 slot per threads, 1 warp-balanced, 2 block-vector)
+    int schedule_choice = 0;     // force launch schedule (0 slot per threads, 1 warp-balanced,
+                                 // 2 block-vector, 3 block-vector with length-sorted threads)
     TermArrays t{};
 };
 
@@ -1925,7 +1926,7 @@ int mjg_set_pair_schedule(mjg_context* c, int term, int schedule)
 {
     ABI_BEGIN(c)
     if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "the schedule applies to global terms");}
-    if(schedule < 0 || schedule > 2) {throw Error(MJG_EINVAL, "schedule must be 0, 1 or 2");}
+    if(schedule < 0 || schedule > 3) {throw Error(MJG_EINVAL, "schedule must be 0, 1, 2 or 3");}
     TermDev& T = c->term[term - MJG_TERM_EXV];
     T.schedule_choice = schedule;
     if(T.t.schedule != schedule)

@@ -324,10 +324,44 @@ __device__ __forceinline__ void load_block(const int* __restrict__ p, int (&q)[L
     }
 }
 
-template<int PREC, int G, bool PER, int L>
+// SORT: the block's threads take its 256 slots in order of their number of
+// list blocks (a counting sort in shared memory), so that the lanes of a warp
+// walk lists of about the same length; the slots themselves, and with them
+// the spatial order of the partners, stay where they are.
+template<int PREC, int G, bool PER, int L, bool SORT>
 __global__ void __launch_bounds__(TPB) k_pair_vec(Arena a, TermArrays t)
 {
-    const long long s = (long long)blockIdx.x * TPB + threadIdx.x;
+    long long s = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(SORT)
+    {
+        constexpr int NB = 32;                       // bins: list blocks 0 .. 31+
+        __shared__ int bin_count[NB];
+        __shared__ int perm[TPB];
+        if(threadIdx.x < NB) {bin_count[threadIdx.x] = 0;}
+        __syncthreads();
+        int nb = 0;
+        if(s < t.np && !a.sys[t.slot_sys[s]].frozen) {nb = (t.nnb[s] + L - 1) / L;}
+        const int bin = nb < NB - 1 ? nb : NB - 1;
+        const int rank = atomicAdd(&bin_count[bin], 1);
+        __syncthreads();
+        if(threadIdx.x < 32)
+        {
+            // exclusive scan of the 32 bin counts by the first warp
+            const int v = bin_count[threadIdx.x];
+            int incl = v;
+#pragma unroll
+            for(int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if((int)threadIdx.x >= o) {incl += y;}
+            }
+            bin_count[threadIdx.x] = incl - v;
+        }
+        __syncthreads();
+        perm[bin_count[bin] + rank] = threadIdx.x;
+        __syncthreads();
+        s = (long long)blockIdx.x * TPB + perm[threadIdx.x];
+    }
     if(s >= t.np) {return;}
     const int sys = t.slot_sys[s];
     double energy = 0.0;
@@ -495,10 +529,11 @@ void dispatch_per(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t 
         // the per-step force launch: schedule and partner batch depth are tunable
         if constexpr(TPP > 1)
         {
-            if(t.schedule == 2)
+            if(t.schedule == 2 || t.schedule == 3)
             {
                 const unsigned nv = (unsigned)((t.np + TPB - 1) / TPB);
-                k_pair_vec<PREC, G, PER, TPP><<<nv, TPB, 0, s>>>(a, t);
+                if(t.schedule == 3) {k_pair_vec<PREC, G, PER, TPP, true ><<<nv, TPB, 0, s>>>(a, t);}
+                else                {k_pair_vec<PREC, G, PER, TPP, false><<<nv, TPB, 0, s>>>(a, t);}
                 return;
             }
         }

@@ -237,7 +237,7 @@ def test_launch_shapes_give_the_same_trajectory(precision):
              S.lj_fluid(n=512, seed=43)]
     ref = None
     shapes = [(0, tpp, unr) for tpp in (1, 2, 4, 8, 16) for unr in (1, 2, 4)]
-    shapes += [(2, tpp, 1) for tpp in (2, 4, 8, 16)]
+    shapes += [(sch, tpp, 1) for sch in (2, 3) for tpp in (2, 4, 8, 16)]
     if precision == "mixed":
         shapes += [(1, tpp, unr) for tpp in (1, 16) for unr in (1, 2, 4)]
     for sch, tpp, unr in shapes:
