@@ -242,8 +242,9 @@ MJG_API int mjg_get_pair_unroll(mjg_context* ctx, int term, int* unroll);
  * 2 = one thread per particle reading its list in blocks of
  * threads-per-particle words with vector loads (with threads-per-particle 1
  * it is schedule 0); 3 = as 2, with the threads of each 256-particle block
- * handed its particles in order of list length.  No counterpart in the
- * reference. */
+ * handed its particles in order of list length; 4 = as 0, with the thread
+ * groups of each block handed its particles in order of list length.  No
+ * counterpart in the reference. */
 MJG_API int mjg_set_pair_schedule(mjg_context* ctx, int term, int schedule);
 MJG_API int mjg_get_pair_schedule(mjg_context* ctx, int term, int* schedule);
 /* Sets the per-particle neighbour capacity of a global term's lists.  A

@@ -7,8 +7,8 @@ For every global term of an :class:`~mjolnir_b200.engine.Engine` it picks
   * the pair kernel's launch shape, by timing the kernel alone: the schedule
     (one particle per group of threads; warp-balanced over the lists of a
     warp's 32 particles, mixed form only; or one thread per particle reading
-    its list in blocks with vector loads, optionally with each block's
-    threads ordered by list length), the threads per particle / list
+    its list in blocks with vector loads; the first and last optionally with
+    each block's threads ordered by list length), the threads per particle / list
     block (1, 2, 4, 8, 16) and the partners each thread requests per batch
     (1, 2, 4).
 In the mixed form neither choice changes a result: the fixed-point force sums
@@ -32,7 +32,7 @@ def _time_steps(eng, nsteps: int) -> float:
 
 
 def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
-         tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1, 2, 3), steps: int = 60,
+         tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1, 2, 3, 4), steps: int = 60,
          warm: int = 20, log=None) -> dict:
     present = []
     for t in terms:
@@ -86,7 +86,7 @@ def _tune_shape(eng, term, tpps, unrolls, schedules):
 
 
 def tune_shapes(eng, terms=("exv", "dh", "lj"), tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4),
-                schedules=(0, 1, 2, 3)) -> dict:
+                schedules=(0, 1, 2, 3, 4)) -> dict:
     """Launch shape only (margins as committed): for a single large system,
     where the margin is fixed by the input."""
     out = {}

@@ -137,7 +137,8 @@ struct TermDev {
     int tpp_choice = 1;          // ... and its value (kept across commits)
     int unroll_choice = 1;       // partner batch depth of the force launch
     int schedule_choice = 0;     // force launch schedule (0 slot per threads, 1 warp-balanced,
-                                 // 2 block-vector, 3 block-vector with length-sorted threads)
+                                 // 2 block-vector, 3 block-vector with length-sorted threads,
+                                 // 4 slot per threads with length-sorted groups)
     TermArrays t{};
 };
 
@@ -1926,7 +1927,7 @@ int mjg_set_pair_schedule(mjg_context* c, int term, int schedule)
 {
     ABI_BEGIN(c)
     if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "the schedule applies to global terms");}
-    if(schedule < 0 || schedule > 3) {throw Error(MJG_EINVAL, "schedule must be 0, 1, 2 or 3");}
+    if(schedule < 0 || schedule > 4) {throw Error(MJG_EINVAL, "schedule must be 0 .. 4");}
     TermDev& T = c->term[term - MJG_TERM_EXV];
     T.schedule_choice = schedule;
     if(T.t.schedule != schedule)

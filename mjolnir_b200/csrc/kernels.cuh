@@ -39,7 +39,8 @@ struct TermArrays {
     int        unroll;          // partners requested per batch by the force launch (1, 2, 4)
     int        schedule;        // force launch: 0 = slot per tpp threads, 1 = warp-balanced (mixed),
                                 // 2 = one thread per slot reading tpp-word blocks of its list,
-                                // 3 = as 2 with a block's threads ordered by list length
+                                // 3 = as 2 with a block's threads ordered by list length,
+                                // 4 = as 0 with a block's thread groups ordered by list length
     int        any_periodic;    // some system with this term has a periodic box
     const int* part_particle;   // [np] global particle index
     const double* part_p0;      // [np] radius / charge / sigma

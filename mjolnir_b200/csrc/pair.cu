@@ -217,14 +217,57 @@ struct PairEval {
 // 1 keeps one partner in flight ahead of the pair being evaluated; 2 and 4
 // issue the batch's list words, then its coordinates, before evaluating any
 // of them (more loads in flight per thread, more registers).
-template<int PREC, int G, bool NF, bool NE, int TPP, bool PER, int UNR>
+// Counting sort of a block's slots by their list length (in units of `per`
+// partners, 32 bins): returns the block-local index of the slot this group of
+// threads takes.  Slot numbering is unchanged; only which threads walk which
+// list.  Every thread of the block must call it.
+template<int GROUPS>
+__device__ __forceinline__ int sorted_group(const Arena& a, const TermArrays& t, long long first_slot,
+                                            int group, bool leader, int per)
+{
+    constexpr int NB = 32;
+    __shared__ int bin_count[NB];
+    __shared__ int perm[GROUPS];
+    if(threadIdx.x < NB) {bin_count[threadIdx.x] = 0;}
+    __syncthreads();
+    const long long s = first_slot + group;
+    int nb = 0;
+    if(leader && s < t.np && !a.sys[t.slot_sys[s]].frozen) {nb = (t.nnb[s] + per - 1) / per;}
+    const int bin = nb < NB - 1 ? nb : NB - 1;
+    const int rank = leader ? atomicAdd(&bin_count[bin], 1) : 0;
+    __syncthreads();
+    if(threadIdx.x < 32)
+    {
+        const int v = bin_count[threadIdx.x];
+        int incl = v;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1)
+        {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if((int)threadIdx.x >= o) {incl += y;}
+        }
+        bin_count[threadIdx.x] = incl - v;
+    }
+    __syncthreads();
+    if(leader) {perm[bin_count[bin] + rank] = group;}
+    __syncthreads();
+    return perm[group];
+}
+
+template<int PREC, int G, bool NF, bool NE, int TPP, bool PER, int UNR, bool SORT = false>
 __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
 {
     // TPP consecutive threads share one slot; lane lg walks partners lg,
-    // lg + TPP, ... which the blocked list layout stores next to each other
+    // lg + TPP, ... which the blocked list layout stores next to each other.
+    // SORT: the block's groups take its slots in order of list length.
     const long long gt = (long long)blockIdx.x * TPB + threadIdx.x;
-    const long long s = gt / TPP;
+    long long s = gt / TPP;
     const int lg = (int)(threadIdx.x % TPP);
+    if(SORT)
+    {
+        const long long first = (long long)blockIdx.x * (TPB / TPP);
+        s = first + sorted_group<TPB / TPP>(a, t, first, (int)(threadIdx.x / TPP), lg == 0, TPP * UNR);
+    }
     const bool active = s < t.np;
     const int sys = active ? t.slot_sys[s] : 0;
     double energy = 0.0;
@@ -334,33 +377,8 @@ __global__ void __launch_bounds__(TPB) k_pair_vec(Arena a, TermArrays t)
     long long s = (long long)blockIdx.x * TPB + threadIdx.x;
     if(SORT)
     {
-        constexpr int NB = 32;                       // bins: list blocks 0 .. 31+
-        __shared__ int bin_count[NB];
-        __shared__ int perm[TPB];
-        if(threadIdx.x < NB) {bin_count[threadIdx.x] = 0;}
-        __syncthreads();
-        int nb = 0;
-        if(s < t.np && !a.sys[t.slot_sys[s]].frozen) {nb = (t.nnb[s] + L - 1) / L;}
-        const int bin = nb < NB - 1 ? nb : NB - 1;
-        const int rank = atomicAdd(&bin_count[bin], 1);
-        __syncthreads();
-        if(threadIdx.x < 32)
-        {
-            // exclusive scan of the 32 bin counts by the first warp
-            const int v = bin_count[threadIdx.x];
-            int incl = v;
-#pragma unroll
-            for(int o = 1; o < 32; o <<= 1)
-            {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if((int)threadIdx.x >= o) {incl += y;}
-            }
-            bin_count[threadIdx.x] = incl - v;
-        }
-        __syncthreads();
-        perm[bin_count[bin] + rank] = threadIdx.x;
-        __syncthreads();
-        s = (long long)blockIdx.x * TPB + perm[threadIdx.x];
+        const long long first = (long long)blockIdx.x * TPB;
+        s = first + sorted_group<TPB>(a, t, first, (int)threadIdx.x, true, L);
     }
     if(s >= t.np) {return;}
     const int sys = t.slot_sys[s];
@@ -543,6 +561,12 @@ void dispatch_per(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t 
             if(t.unroll == 4)      {k_pair_warp<G, PER, 4><<<nw, TPB, 0, s>>>(a, t);}
             else if(t.unroll == 2) {k_pair_warp<G, PER, 2><<<nw, TPB, 0, s>>>(a, t);}
             else                   {k_pair_warp<G, PER, 1><<<nw, TPB, 0, s>>>(a, t);}
+        }
+        else if(t.schedule == 4)
+        {
+            if(t.unroll == 4)      {k_pair<PREC, G, true, false, TPP, PER, 4, true><<<nb, TPB, 0, s>>>(a, t);}
+            else if(t.unroll == 2) {k_pair<PREC, G, true, false, TPP, PER, 2, true><<<nb, TPB, 0, s>>>(a, t);}
+            else                   {k_pair<PREC, G, true, false, TPP, PER, 1, true><<<nb, TPB, 0, s>>>(a, t);}
         }
         else if(t.unroll == 4) {k_pair<PREC, G, true, false, TPP, PER, 4><<<nb, TPB, 0, s>>>(a, t);}
         else if(t.unroll == 2) {k_pair<PREC, G, true, false, TPP, PER, 2><<<nb, TPB, 0, s>>>(a, t);}
