@@ -416,7 +416,8 @@ def run_b200(args, ws, rank, local, pg):
     serving = None
     if args.serve > 0 and rank == 0 and ws == 1:
         from mjolnir_b200.serve import serve_poisson
-        serving = serve_poisson(duration=args.serve, rate=200.0)
+        serving = serve_poisson(duration=args.serve, rate=200.0, tuned=tuned)
+        serving["tuned"] = tuned is not None
         serving["note"] = ("offered load far above one GPU: most arrivals stay queued; "
                            "latency is over completed jobs")
 

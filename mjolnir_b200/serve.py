@@ -66,8 +66,14 @@ class Server:
     def __init__(self, precision: str = "mixed", chunk: int = 500, hbm_fraction: float = 0.8,
                  device: int = 0, bytes_per_particle: float = 2048.0, min_commit_interval: float = 0.0,
                  keep_results: bool = True, builders: int = 4, max_particles: int = 2_000_000,
-                 chunk_seconds: Optional[float] = None, lookahead: int = 64):
+                 chunk_seconds: Optional[float] = None, lookahead: int = 64,
+                 tuned: Optional[dict] = None):
         self.eng = Engine(precision, device=device)
+        # per global term: {"margin", "schedule", "threads_per_particle", "unroll"}
+        # as :func:`mjolnir_b200.autotune.tune` returns them; the margin
+        # replaces each admitted job's, the launch shape is set after every
+        # commit (it changes no result in the mixed form)
+        self.tuned = tuned or {}
         self.chunk = int(chunk)
         self.chunk_seconds = chunk_seconds
         self.keep_results = keep_results
@@ -144,6 +150,10 @@ class Server:
                     break
                 self.queue.popleft()
                 job.n = n
+                for key, cfg in self.tuned.items():
+                    term = getattr(job.desc, key, None)
+                    if term is not None and "margin" in cfg:
+                        term.margin = cfg["margin"]
                 job.sid = self.eng.add_system(job.desc)
                 job.admitted = self.now()
                 if not self.keep_results:
@@ -160,6 +170,17 @@ class Server:
             self.eng.remove_system(sid)
         self.retiring = []
         self.eng.commit()
+        for key, cfg in self.tuned.items():
+            try:
+                self.eng.get_threads_per_particle(key)
+            except Exception:
+                continue                         # term not in the arena now
+            if self.eng.get_pair_schedule(key) != cfg.get("schedule", 0):
+                self.eng.set_pair_schedule(key, cfg.get("schedule", 0))
+            if self.eng.get_threads_per_particle(key) != cfg.get("threads_per_particle", 1):
+                self.eng.set_threads_per_particle(key, cfg.get("threads_per_particle", 1))
+            if self.eng.get_pair_unroll(key) != cfg.get("unroll", 1):
+                self.eng.set_pair_unroll(key, cfg.get("unroll", 1))
         self.commits += 1
         self.commit_s += time.perf_counter() - t
         self.last_commit = self.now()
@@ -274,13 +295,15 @@ def poisson_workload(rate: float, duration: float, seed: int = 7, nmin: int = 20
 
 def serve_poisson(duration: float = 60.0, rate: float = 200.0, chunk: int = 2000, seed: int = 7,
                   precision: str = "mixed", max_particles: int = 2_000_000,
-                  chunk_seconds: float = 1.0, min_commit_interval: float = 1.0) -> dict:
+                  chunk_seconds: float = 1.0, min_commit_interval: float = 1.0,
+                  tuned: Optional[dict] = None) -> dict:
     """Replays a Poisson stream in real time for `duration` seconds and
-    reports completion latency, queue depth and aggregate throughput."""
+    reports completion latency, queue depth and aggregate throughput.
+    `tuned`: margins and launch shapes to serve with (autotuner output)."""
     jobs = poisson_workload(rate, duration, seed=seed)
     srv = Server(precision=precision, chunk=chunk, keep_results=False,
                  min_commit_interval=min_commit_interval, max_particles=max_particles,
-                 chunk_seconds=chunk_seconds)
+                 chunk_seconds=chunk_seconds, tuned=tuned)
     srv.t0 = time.perf_counter()
     i = 0
     while srv.now() < duration:
