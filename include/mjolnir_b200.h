@@ -130,6 +130,18 @@ MJG_API int mjg_dh_set(mjg_context* ctx, int sys, double cutoff_ratio, double ma
  * (forcefield/global/LennardJonesPotential.hpp:15-110, ParameterList.hpp:185-329). */
 MJG_API int mjg_lj_set(mjg_context* ctx, int sys, double cutoff_ratio, double margin,
                int64_t np, const int64_t* idx, const double* sigma, const double* epsilon);
+/* The third global term with any potential of the Lennard-Jones family, by
+ * the name the reference's input uses: "LennardJones" (as mjg_lj_set),
+ * "WCA" (forcefield/global/WCAPotential.hpp; its cutoff is fixed at
+ * 2^(1/6) sigma and cutoff_ratio is ignored, as input/read_global_potential.hpp
+ * warns), "LennardJonesAttractive" (LennardJonesAttractivePotential.hpp) or
+ * "UniformLennardJones" (UniformLennardJonesPotential.hpp; every participant
+ * must carry the same sigma and epsilon).  The last three run through the
+ * generic GlobalPairInteraction loop (GlobalPairInteraction.hpp:148-213) with
+ * the Lorentz-Berthelot rule (ParameterList.hpp:240-251). */
+MJG_API int mjg_pair_set(mjg_context* ctx, int sys, const char* potential, double cutoff_ratio,
+                         double margin, int64_t np, const int64_t* idx, const double* sigma,
+                         const double* epsilon);
 /* The ignore rules of one global term: ignore.molecule and
  * ignore.particles_within (input/read_global_potential.hpp:29-90,168-190;
  * core/ExclusionList.hpp:56-234).  kinds[k] / within[k] for nk connection

@@ -39,6 +39,12 @@ constexpr double FX_INV_SCALE = 1.0 / 268435456.0;
 constexpr double FX_LIMIT     = 1125899906842624.0;     // 2^50
 constexpr double FX_MAGIC     = 6755399441055744.0;     // 1.5 * 2^52
 
+// potential of the third global term: LennardJones (its own interaction,
+// forcefield/global/GlobalPairLennardJonesInteraction.hpp) or a potential of
+// the family through the generic pair loop (GlobalPairInteraction.hpp:148-213)
+enum LjKind { LJ_PLAIN = 0, LJ_WCA = 1, LJ_ATTRACTIVE = 2, LJ_UNIFORM = 3 };
+constexpr double SIXTH_ROOT_OF_TWO = 1.12246204831;   // WCAPotential.hpp default_cutoff
+
 struct GlobalParams {       // per system, per global term
     double cutoff;          // max_cutoff_length
     double margin;          // relative skin
@@ -62,6 +68,7 @@ struct GlobalParams {       // per system, per global term
     int    ignore_mol;      // IgnoreMol
     int    rebuild;         // set by the margin kernel, cleared after a rebuild
     int    rebuilds;        // rebuild counter
+    int    kind;            // third term's potential (LjKind)
     int    on;
 };
 

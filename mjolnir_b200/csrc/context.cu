@@ -83,6 +83,7 @@ struct DevBuf {
 
 struct HostGlobal {
     bool on = false;
+    int kind = LJ_PLAIN;         // third term: potential of the Lennard-Jones family
     double eps = 0.0, cutoff_ratio = 0.0, margin = 0.5;
     std::vector<int64_t> idx;
     std::vector<double> p0, p1;
@@ -695,9 +696,11 @@ void make_sysdev(const HostSystem& s, SysDev& d)
             G.coef_at_cutoff = p.coef_at_cutoff; G.inv4pi = p.inv4pi;
             G.cutoff = p.debye * H.cutoff_ratio;
         }
-        else                       // LennardJonesPotential.hpp:36-41,75-91
+        else                       // LennardJonesPotential.hpp:36-41,75-91 and the family
         {
-            G.coef_at_cutoff = std::pow(1.0 / H.cutoff_ratio, 12) - std::pow(1.0 / H.cutoff_ratio, 6);
+            G.kind = H.kind;
+            G.coef_at_cutoff = H.kind == LJ_WCA ? 0.0 :          // WCAPotential.hpp: no shift
+                std::pow(1.0 / H.cutoff_ratio, 12) - std::pow(1.0 / H.cutoff_ratio, 6);
             double ms = 0;
             for(double x : H.p0) {ms = std::max(ms, x);}
             G.cutoff = np == 0 ? 1.0 : ms * H.cutoff_ratio;
@@ -1503,7 +1506,42 @@ int mjg_lj_set(mjg_context* c, int sys, double cutoff_ratio, double margin, int6
     check_idx(s, np, idx);
     if(!(cutoff_ratio > 0) || !(margin >= 0) || (np > 0 && (!sigma || !epsilon))) {throw Error(MJG_EINVAL, "bad LennardJones parameters");}
     HostGlobal& g = s.g[G_LJ];
-    g.on = true; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
+    g.on = true; g.kind = LJ_PLAIN; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
+    g.idx.assign(idx, idx + np); g.p0.assign(sigma, sigma + np); g.p1.assign(epsilon, epsilon + np);
+    ABI_END(c)
+}
+
+int mjg_pair_set(mjg_context* c, int sys, const char* potential, double cutoff_ratio, double margin,
+                 int64_t np, const int64_t* idx, const double* sigma, const double* epsilon)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "interactions are fixed once committed");}
+    if(!potential) {throw Error(MJG_EINVAL, "potential name is NULL");}
+    const std::string name(potential);
+    int kind;
+    if(name == "LennardJones")                {kind = LJ_PLAIN;}
+    else if(name == "WCA")                    {kind = LJ_WCA; cutoff_ratio = SIXTH_ROOT_OF_TWO;}
+    else if(name == "LennardJonesAttractive") {kind = LJ_ATTRACTIVE;}
+    else if(name == "UniformLennardJones")    {kind = LJ_UNIFORM;}
+    else {throw Error(MJG_EINVAL, "unknown pair potential: " + name);}
+    check_idx(s, np, idx);
+    if(!(cutoff_ratio > 0) || !(margin >= 0) || (np > 0 && (!sigma || !epsilon)))
+    {
+        throw Error(MJG_EINVAL, "bad " + name + " parameters");
+    }
+    if(kind == LJ_UNIFORM)
+    {
+        for(int64_t k = 1; k < np; ++k)
+        {
+            if(sigma[k] != sigma[0] || epsilon[k] != epsilon[0])
+            {
+                throw Error(MJG_EINVAL, "UniformLennardJones takes one sigma and one epsilon");
+            }
+        }
+    }
+    HostGlobal& g = s.g[G_LJ];
+    g.on = true; g.kind = kind; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
     g.idx.assign(idx, idx + np); g.p0.assign(sigma, sigma + np); g.p1.assign(epsilon, epsilon + np);
     ABI_END(c)
 }

@@ -19,6 +19,8 @@
 //           so the sum does not depend on list order or launch shape.
 #include "kernels.cuh"
 
+#include <type_traits>
+
 namespace mjg {
 
 namespace {
@@ -96,8 +98,9 @@ struct PairEval {
     double4 pi;
     long long s;
     bool periodic;
-    double crsq, coefc, eps, eps12, debye, inv_debye, abs_cut_sq, qi, inv4pi, epsi;
+    double crsq, coefc, eps, eps12, debye, inv_debye, abs_cut_sq, qi, inv4pi, epsi, cr;
     float eps12f, epsf, coefcf, debf, invdf;
+    int kind;
     const double* slot_p1;
 
     __device__ __forceinline__ PairEval(const Arena& a, const TermArrays& t, long long slot, int sys)
@@ -108,6 +111,8 @@ struct PairEval {
         periodic = PER && S->boundary == B_PERIODIC;
         pi = t.slot_pd[slot];
         crsq  = P.cutoff_ratio_sq;
+        cr    = P.cutoff_ratio;
+        kind  = P.kind;
         coefc = P.coef_at_cutoff;
         eps   = P.eps;
         eps12 = eps * 12;
@@ -118,6 +123,88 @@ struct PairEval {
         epsi  = (G == G_LJ) ? t.slot_p1[slot] : 0.0;
         eps12f = (float)eps12; epsf = (float)eps; coefcf = (float)coefc;
         debf = (float)debye; invdf = (float)inv_debye;
+    }
+
+    // WCA, LennardJonesAttractive and UniformLennardJones through the generic
+    // pair loop: f = r_ij (f_mag / |r|) with f_mag = potential.derivative(|r|),
+    // a pair with f_mag = 0 skipped in the force pass; the energy-only pass
+    // (calc_energy) sums potential(|r|) over every listed pair.  Formulas of
+    // WCAPotential.hpp:37-58, LennardJonesAttractivePotential.hpp:36-70,
+    // UniformLennardJonesPotential.hpp:41-61 (uniform sigma and epsilon are
+    // equal per-slot values, which the Lorentz-Berthelot rule keeps as is).
+    template<typename T>
+    __device__ __forceinline__ static T fam_derivative(int kind, T r, T sigma, T epsilon, T cutoff_ratio)
+    {
+        if(kind == LJ_WCA)
+        {
+            if(sigma * T(SIXTH_ROOT_OF_TWO) < r) {return T(0);}
+            const T rinv = T(1) / r;
+            const T r1s1 = sigma * rinv;
+            const T r3s3 = r1s1 * r1s1 * r1s1;
+            const T r6s6 = r3s3 * r3s3;
+            return T(24) * epsilon * (r6s6 * (T(1) - T(2) * r6s6)) * rinv;
+        }
+        if(kind == LJ_ATTRACTIVE)
+        {
+            if(r < sigma * T(SIXTH_ROOT_OF_TWO) || sigma * cutoff_ratio < r) {return T(0);}
+            const T rinv = T(1) / r;
+            const T sr1 = sigma * rinv;
+            const T sr3 = sr1 * sr1 * sr1;
+            const T sr6 = sr3 * sr3;
+            return T(24) * epsilon * (sr6 - T(2) * sr6 * sr6) * rinv;
+        }
+        if(sigma * cutoff_ratio < r) {return T(0);}
+        const T rinv = T(1) / r;
+        const T sr1 = sigma * rinv;
+        const T sr3 = sr1 * sr1 * sr1;
+        const T sr6 = sr3 * sr3;
+        return (epsilon * T(24)) * sr6 * (T(1) - T(2) * sr6) * rinv;
+    }
+    template<typename T>
+    __device__ __forceinline__ static T fam_potential(int kind, T r, T sigma, T epsilon, T cutoff_ratio, T coefc)
+    {
+        if(kind == LJ_WCA)
+        {
+            if(sigma * T(SIXTH_ROOT_OF_TWO) < r) {return T(0);}
+            const T r1s1 = sigma / r;
+            const T r3s3 = r1s1 * r1s1 * r1s1;
+            const T r6s6 = r3s3 * r3s3;
+            return T(4) * epsilon * (r6s6 * (r6s6 - T(1)) + T(0.25));
+        }
+        if(kind == LJ_ATTRACTIVE)
+        {
+            if(r < sigma * T(SIXTH_ROOT_OF_TWO)) {return -epsilon;}
+            if(sigma * cutoff_ratio < r) {return T(0);}
+            const T sr1 = sigma / r;
+            const T sr3 = sr1 * sr1 * sr1;
+            const T sr6 = sr3 * sr3;
+            return T(4) * epsilon * (sr6 * (sr6 - T(1)) - coefc);
+        }
+        if(sigma * cutoff_ratio < r) {return T(0);}
+        const T sr1 = sigma / r;
+        const T sr3 = sr1 * sr1 * sr1;
+        const T sr6 = sr3 * sr3;
+        return (epsilon * T(4)) * (sr6 * (sr6 - T(1)) - coefc);
+    }
+    __device__ __forceinline__ void family(int k, double sigma, double epsilon, double l2, double dx,
+                                           double dy, double dz, bool count_e, Acc<PREC>& acc,
+                                           double& energy, bool& ovf) const
+    {
+        using T = typename std::conditional<PREC == P_FP64, double, float>::type;
+        if(NF)
+        {
+            const T rl = PREC == P_FP64 ? T(rsqrt(l2)) : T(rsqrtf((float)l2));
+            const T l  = T(l2) * rl;
+            const T f_mag = fam_derivative<T>(k, l, T(sigma), T(epsilon), T(cr));
+            if(f_mag == T(0)) {return;}
+            acc.add((double)(f_mag * rl), dx, dy, dz, ovf);
+            if(count_e) {energy += (double)fam_potential<T>(k, l, T(sigma), T(epsilon), T(cr), T(coefc));}
+        }
+        else if(count_e)
+        {
+            const T l = PREC == P_FP64 ? T(sqrt(l2)) : sqrtf((float)l2);
+            energy += (double)fam_potential<T>(k, l, T(sigma), T(epsilon), T(cr), T(coefc));
+        }
     }
 
     __device__ __forceinline__ void operator()(const double4& pj, const int q, Acc<PREC>& acc,
@@ -190,6 +277,11 @@ struct PairEval {
             const double sigma = (pi.w + pj.w) / 2;
             const double epsj = slot_p1[q];
             const double epsilon = (epsi == epsj) ? epsi : sqrt(epsi * epsj);
+            if(kind != LJ_PLAIN)
+            {
+                family(kind, sigma, epsilon, l2, dx, dy, dz, count_e, acc, energy, ovf);
+                return;
+            }
             const double sigma_sq = sigma * sigma;
             if(sigma_sq * crsq < l2) {return;}
             if(PREC == P_FP64)

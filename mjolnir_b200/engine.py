@@ -93,10 +93,14 @@ class Engine:
             elif term == A.TERM_DH:
                 self._c(L.mjg_dh_set(self.ctx, s, float(t.cutoff), float(t.margin), len(idx),
                                      A.i64(idx), A.f64(p0)))
-            else:
+            elif t.kind == "LennardJones":
                 p1 = _arr(t.param1, np.float64)
                 self._c(L.mjg_lj_set(self.ctx, s, float(t.cutoff), float(t.margin), len(idx),
                                      A.i64(idx), A.f64(p0), A.f64(p1)))
+            else:                                   # WCA, LennardJonesAttractive, UniformLennardJones
+                p1 = _arr(t.param1, np.float64)
+                self._c(L.mjg_pair_set(self.ctx, s, t.kind.encode(), float(t.cutoff), float(t.margin),
+                                       len(idx), A.i64(idx), A.f64(p0), A.f64(p1)))
             kinds = (C.c_char_p * max(1, len(within)))(*[k.encode() for k, _ in within])
             vals = _arr([w for _, w in within] or [0], np.int32)
             self._c(L.mjg_ignore_set(self.ctx, s, term, ign, len(within), kinds, A.i32(vals)))

@@ -26,9 +26,11 @@ ready for :meth:`Engine.add_system`:
   BondAngle with Harmonic (``k``, ``v0``) and DihedralAngle with Cosine
   (``k``, ``n``, ``v0``), ``indices`` plus an optional ``offset``
   (input/read_local_potential.hpp:473-522); ``[[forcefields.global]]`` Pair
-  with ExcludedVolume (``epsilon``, ``radius``), DebyeHuckel (``charge``) or
-  LennardJones (``sigma|σ``, ``epsilon|ε``), ``cutoff`` (defaults 2.0 / 5.5 /
-  2.5), ``spatial_partition = {type = "CellList"|"VerletList", margin}``,
+  with ExcludedVolume (``epsilon``, ``radius``), DebyeHuckel (``charge``),
+  LennardJones, WCA or LennardJonesAttractive (``sigma|σ``, ``epsilon|ε``) or
+  UniformLennardJones (global ``sigma``, ``epsilon``; ``parameters`` optional),
+  ``cutoff`` (defaults 2.0 / 5.5 / 2.5; WCA's is fixed at 2^(1/6)),
+  ``spatial_partition = {type = "CellList"|"VerletList", margin}``,
   ``ignore.molecule`` and ``ignore.particles_within``
   (input/read_global_potential.hpp:32-300,360-470,660-705).
 
@@ -55,7 +57,9 @@ import numpy as np
 
 from .systems import KB_KCAL, PairTerm, SystemDesc
 
-DEFAULT_CUTOFF = {"ExcludedVolume": 2.0, "DebyeHuckel": 5.5, "LennardJones": 2.5}
+DEFAULT_CUTOFF = {"ExcludedVolume": 2.0, "DebyeHuckel": 5.5, "LennardJones": 2.5,
+                  "WCA": 1.12246204831, "LennardJonesAttractive": 2.5, "UniformLennardJones": 2.5}
+LJ_FAMILY = ("LennardJones", "WCA", "LennardJonesAttractive", "UniformLennardJones")
 LOCAL_FORMS = {("BondLength", "Harmonic"): 2, ("BondAngle", "Harmonic"): 3,
                ("DihedralAngle", "Cosine"): 4}
 
@@ -298,11 +302,13 @@ def _global(g, n, where):
     inter = g.get("interaction")
     pot = g.get("potential")
     if inter != "Pair" or pot not in DEFAULT_CUTOFF:
-        raise InputError(f'{where}: "{inter}" / "{pot}" is not run here '
-                         "(Pair with ExcludedVolume, DebyeHuckel or LennardJones)")
+        raise InputError(f'{where}: "{inter}" / "{pot}" is not run here (Pair with ExcludedVolume, '
+                         "DebyeHuckel, LennardJones, WCA, LennardJonesAttractive or UniformLennardJones)")
     allowed = {"interaction", "potential", "ignore", "spatial_partition", "parameters", "env", "cutoff"}
-    if pot == "ExcludedVolume":
+    if pot in ("ExcludedVolume", "UniformLennardJones"):
         allowed |= {"epsilon"}
+    if pot == "UniformLennardJones":
+        allowed |= {"sigma"}
     if "table" in g:
         raise InputError(f"{where}: parameter tables are not supported")
     _check_keys(g, allowed, where)
@@ -311,12 +317,16 @@ def _global(g, n, where):
         raise InputError(f'{where}: spatial_partition.type must be "CellList" or "VerletList"')
     margin = float(sp["margin"])
     env = g.get("env")
-    items = g.get("parameters", [])
+    if pot == "UniformLennardJones" and "parameters" not in g:
+        items = [{"index": i} for i in range(n)]   # every particle (EmptyCombinationRule)
+    else:
+        items = g.get("parameters", [])
     idx = np.array([_index(it, env, where) for it in items], dtype=np.int64)
     _no_overlap(idx.tolist(), where)
     if idx.size and (idx.min() < 0 or idx.max() >= n):
         raise InputError(f"{where}: participant index out of range")
-    cutoff = float(g.get("cutoff", DEFAULT_CUTOFF[pot]))
+    # WCA's cutoff is fixed (input/read_global_potential.hpp warns and ignores it)
+    cutoff = DEFAULT_CUTOFF[pot] if pot == "WCA" else float(g.get("cutoff", DEFAULT_CUTOFF[pot]))
     mol, within = _ignore(g, where)
     if pot == "ExcludedVolume":
         p0 = np.array([float(_param(it, env, "radius", where=where)) for it in items])
@@ -324,6 +334,13 @@ def _global(g, n, where):
     elif pot == "DebyeHuckel":
         p0 = np.array([float(_param(it, env, "charge", where=where)) for it in items])
         term = PairTerm(pot, idx, p0, cutoff=cutoff, margin=margin)
+    elif pot == "UniformLennardJones":
+        for k in ("sigma", "epsilon"):
+            if k not in g:
+                raise InputError(f"{where}: UniformLennardJones needs {k}")
+        p0 = np.full(len(idx), float(g["sigma"]))
+        p1 = np.full(len(idx), float(g["epsilon"]))
+        term = PairTerm(pot, idx, p0, p1, cutoff=cutoff, margin=margin)
     else:
         p0 = np.array([float(_param(it, env, "sigma", "σ", where=where)) for it in items])
         p1 = np.array([float(_param(it, env, "epsilon", "ε", where=where)) for it in items])
@@ -379,9 +396,10 @@ def _forcefield(ff, n, input_path, base_dir):
     for i, g in enumerate(ff.get("global", [])):
         g = _from_file(g, "global", input_path, base_dir)
         t = _global(g, n, f"forcefields.global[{i}]")
-        key = {"ExcludedVolume": "exv", "DebyeHuckel": "dh", "LennardJones": "lj"}[t.kind]
+        key = {"ExcludedVolume": "exv", "DebyeHuckel": "dh"}.get(t.kind, "lj")
         if key in pairs:
-            raise InputError(f"forcefields.global[{i}]: a second {t.kind} term is not supported")
+            raise InputError(f"forcefields.global[{i}]: a second {'Lennard-Jones family' if key == 'lj' else t.kind} "
+                             "term is not supported")
         pairs[key] = t
     locs = {}
     for i, loc in enumerate(ff.get("local", [])):
@@ -591,9 +609,13 @@ def dumps(desc: SystemDesc, total_step: int = 1000, save_step: int = 100, prefix
         a("[[forcefields.global]]")
         a('interaction = "Pair"')
         a(f"potential = {_fmt(t.kind)}")
-        a(f"cutoff = {_fmt(float(t.cutoff))}")
+        if t.kind != "WCA":
+            a(f"cutoff = {_fmt(float(t.cutoff))}")
         if t.kind == "ExcludedVolume":
             a(f"epsilon = {_fmt(float(t.epsilon))}")
+        if t.kind == "UniformLennardJones":
+            a(f"sigma = {_fmt(float(t.param0[0]))}")
+            a(f"epsilon = {_fmt(float(t.param1[0]))}")
         a(f'spatial_partition = {{type = "CellList", margin = {_fmt(float(t.margin))}}}')
         mol = t.ignore_molecule if t.ignore_molecule is not None else desc.ignore_molecule
         within = t.ignore_within if t.ignore_within is not None else (
@@ -601,9 +623,12 @@ def dumps(desc: SystemDesc, total_step: int = 1000, save_step: int = 100, prefix
         a(f"ignore.molecule = {_fmt(mol)}")
         a("ignore.particles_within = {" + ", ".join(f"{k} = {int(v)}" for k, v in within.items()) + "}")
         a("parameters = [")
-        name = {"ExcludedVolume": "radius", "DebyeHuckel": "charge", "LennardJones": "sigma"}[t.kind]
+        name = {"ExcludedVolume": "radius", "DebyeHuckel": "charge"}.get(t.kind, "sigma")
         for q in range(len(t.idx)):
-            extra = f", epsilon = {_fmt(float(t.param1[q]))}" if t.kind == "LennardJones" else ""
+            if t.kind == "UniformLennardJones":
+                a(f"  {{index = {int(t.idx[q])}}},")
+                continue
+            extra = f", epsilon = {_fmt(float(t.param1[q]))}" if t.kind in LJ_FAMILY else ""
             a(f"  {{index = {int(t.idx[q])}, {name} = {_fmt(float(t.param0[q]))}{extra}}},")
         a("]")
     return "\n".join(L) + "\n"

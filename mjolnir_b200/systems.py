@@ -24,7 +24,9 @@ KB_KCAL = 1.38064852e-23 * (1.0 / 4.184 / 1000.0) * 6.022140857e23  # kB in kcal
 @dataclasses.dataclass
 class PairTerm:
     """One ``[[forcefields.global]]`` pair interaction."""
-    kind: str                          # "ExcludedVolume" | "DebyeHuckel" | "LennardJones"
+    kind: str                          # "ExcludedVolume" | "DebyeHuckel" | "LennardJones" | "WCA" |
+                                       # "LennardJonesAttractive" | "UniformLennardJones" (the last
+                                       # four share the third global term, SystemDesc.lj)
     idx: np.ndarray                    # participant particle indices (input order)
     param0: np.ndarray                 # radius | charge | sigma
     param1: Optional[np.ndarray] = None  # LJ epsilon

@@ -49,6 +49,7 @@ class OrcSpec(C.Structure):
         ("dh_n", C.c_int64), ("dh_idx", _i64p), ("dh_charge", _f64p),
         ("lj_on", C.c_int32), ("lj_cutoff", C.c_double), ("lj_margin", C.c_double),
         ("lj_n", C.c_int64), ("lj_idx", _i64p), ("lj_sigma", _f64p), ("lj_eps", _f64p),
+        ("lj_kind", C.c_int32),
         ("nbond", C.c_int64), ("bond_idx", _i64p), ("bond_k", _f64p), ("bond_v0", _f64p),
         ("nangle", C.c_int64), ("angle_idx", _i64p), ("angle_k", _f64p), ("angle_v0", _f64p),
         ("ndihd", C.c_int64), ("dihd_idx", _i64p), ("dihd_k", _f64p), ("dihd_n", _i32p),
@@ -59,6 +60,9 @@ class OrcSpec(C.Structure):
 
 def _ptr(a, ct):
     return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
+
+
+LJ_KINDS = {"LennardJones": 0, "WCA": 1, "LennardJonesAttractive": 2, "UniformLennardJones": 3}
 
 
 def _uniform_ignore(desc):
@@ -128,6 +132,7 @@ def make_spec(desc):
         s.lj_idx = _ptr(arr(t.idx, np.int64), C.c_int64)
         s.lj_sigma = _ptr(arr(t.param0, np.float64), C.c_double)
         s.lj_eps = _ptr(arr(t.param1, np.float64), C.c_double)
+        s.lj_kind = LJ_KINDS[t.kind]
     if desc.bonds is not None:
         idx, k, v0 = desc.bonds
         s.nbond = len(idx)

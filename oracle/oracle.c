@@ -72,6 +72,7 @@ typedef struct
     /* potential constants */
     double   eps, cutoff_ratio, coef_at_cutoff;
     double   dh[5];
+    int      kind;       /* third term: ORC_LJ / ORC_WCA / ORC_LJ_ATTRACTIVE / ORC_LJ_UNIFORM */
     /* current half list: partners of particle i are nbr[lb[i] .. le[i]) */
     int64_t* lb;
     int64_t* le;
@@ -316,9 +317,12 @@ static void setup_global(orc_state* st, int gi, int on, int64_t np, const int64_
         orc_dh_params(st->s.temperature, st->s.ionic_strength, cutoff_ratio, g->dh);
         g->cutoff = g->dh[0] * cutoff_ratio;
     }
-    else               /* LennardJonesPotential.hpp:36-41, :75-91 */
+    else               /* LennardJonesPotential.hpp:36-41, :75-91 and the family */
     {
-        g->coef_at_cutoff = pow(1.0 / cutoff_ratio, 12) - pow(1.0 / cutoff_ratio, 6);
+        g->kind = st->s.lj_kind;
+        /* WCAPotential.hpp: no shift; the others: LennardJones' shift */
+        g->coef_at_cutoff = g->kind == ORC_WCA ? 0.0 :
+                            pow(1.0 / cutoff_ratio, 12) - pow(1.0 / cutoff_ratio, 6);
         double ms = 0;
         for(int64_t k=0; k<np; ++k) {if(ms < p0[k]) {ms = p0[k];}}
         g->cutoff = np == 0 ? 1.0 : ms * cutoff_ratio;
@@ -670,11 +674,116 @@ static double dh_force(const orc_state* st, const orc_global* g, const double* p
     return energy;
 }
 
+/* The Lennard-Jones family through the generic pair loop
+ * (GlobalPairInteraction.hpp:148-213): WCAPotential (WCAPotential.hpp:37-58),
+ * LennardJonesAttractivePotential (LennardJonesAttractivePotential.hpp:36-70),
+ * UniformLennardJonesPotential (UniformLennardJonesPotential.hpp:41-61; one
+ * sigma and epsilon for every pair, kept here as equal per-particle values). */
+static const double ORC_SIXTH_ROOT_OF_TWO = 1.12246204831;
+
+static double ljfam_derivative(int kind, double r, double sigma, double epsilon, double cutoff_ratio)
+{
+    if(kind == ORC_WCA)
+    {
+        if(sigma * ORC_SIXTH_ROOT_OF_TWO < r) {return 0;}
+        const double rinv = 1 / r;
+        const double r1s1 = sigma * rinv;
+        const double r3s3 = r1s1 * r1s1 * r1s1;
+        const double r6s6 = r3s3 * r3s3;
+        return 24 * epsilon * (r6s6 * (1 - 2 * r6s6)) * rinv;
+    }
+    if(kind == ORC_LJ_ATTRACTIVE)
+    {
+        if(r < sigma * ORC_SIXTH_ROOT_OF_TWO || sigma * cutoff_ratio < r) {return 0;}
+        const double rinv = 1 / r;
+        const double sr1 = sigma * rinv;
+        const double sr3 = sr1 * sr1 * sr1;
+        const double sr6 = sr3 * sr3;
+        return 24 * epsilon * (sr6 - 2 * sr6 * sr6) * rinv;
+    }
+    /* ORC_LJ_UNIFORM */
+    if(sigma * cutoff_ratio < r) {return 0;}
+    const double rinv = 1 / r;
+    const double sr1  = sigma * rinv;
+    const double sr3  = sr1 * sr1 * sr1;
+    const double sr6  = sr3 * sr3;
+    return (epsilon * 24) * sr6 * (1 - 2 * sr6) * rinv;
+}
+
+static double ljfam_potential(int kind, double r, double sigma, double epsilon, double cutoff_ratio,
+                              double coef_at_cutoff)
+{
+    if(kind == ORC_WCA)
+    {
+        if(sigma * ORC_SIXTH_ROOT_OF_TWO < r) {return 0;}
+        const double r1s1 = sigma / r;
+        const double r3s3 = r1s1 * r1s1 * r1s1;
+        const double r6s6 = r3s3 * r3s3;
+        return 4 * epsilon * (r6s6 * (r6s6 - 1) + 0.25);
+    }
+    if(kind == ORC_LJ_ATTRACTIVE)
+    {
+        if(r < sigma * ORC_SIXTH_ROOT_OF_TWO) {return -epsilon;}
+        if(sigma * cutoff_ratio < r) {return 0;}
+        const double sr1 = sigma / r;
+        const double sr3 = sr1 * sr1 * sr1;
+        const double sr6 = sr3 * sr3;
+        return 4 * epsilon * (sr6 * (sr6 - 1) - coef_at_cutoff);
+    }
+    if(sigma * cutoff_ratio < r) {return 0;}
+    const double sr1 = sigma / r;
+    const double sr3 = sr1 * sr1 * sr1;
+    const double sr6 = sr3 * sr3;
+    return (epsilon * 4) * (sr6 * (sr6 - 1) - coef_at_cutoff);
+}
+
+static double ljfam_force(const orc_state* st, const orc_global* g, const double* pos,
+                          double* force, int need_force)
+{
+    double energy = 0;
+    for(int64_t q=0; q+1<g->np; ++q)
+    {
+        const int64_t i = g->idx[q];
+        for(int64_t m=g->lb[i]; m<g->le[i]; ++m)
+        {
+            const int64_t j = g->nbr[m];
+            const double sigma = (g->pp0[i] + g->pp0[j]) / 2;       /* LorentzBerthelotRule */
+            const double e1 = g->pp1[i], e2 = g->pp1[j];
+            const double epsilon = (e1 == e2) ? e1 : sqrt(e1 * e2);
+            double rij[3];
+            adjust_direction(st, pos + 3*i, pos + 3*j, rij);
+            const double l2 = length_sq(rij);
+            if(need_force)
+            {
+                const double rl = 1.0 / sqrt(l2);
+                const double l  = l2 * rl;
+                const double f_mag = ljfam_derivative(g->kind, l, sigma, epsilon, g->cutoff_ratio);
+                if(f_mag == 0.0) {continue;}
+                const double c = f_mag * rl;
+                for(int k=0; k<3; ++k)
+                {
+                    const double f = rij[k] * c;
+                    force[3*i+k] += f;
+                    force[3*j+k] -= f;
+                }
+                energy += ljfam_potential(g->kind, l, sigma, epsilon, g->cutoff_ratio, g->coef_at_cutoff);
+            }
+            else
+            {
+                energy += ljfam_potential(g->kind, sqrt(l2), sigma, epsilon, g->cutoff_ratio,
+                                          g->coef_at_cutoff);
+            }
+        }
+    }
+    return energy;
+}
+
 /* forcefield/global/GlobalPairLennardJonesInteraction.hpp:148-198 with the
  * Lorentz-Berthelot rule of ParameterList.hpp:240-251 */
 static double lj_force(const orc_state* st, const orc_global* g, const double* pos,
                        double* force, int need_force)
 {
+    if(g->kind != ORC_LJ) {return ljfam_force(st, g, pos, force, need_force);}
     const double coef_at_cutoff  = g->coef_at_cutoff;
     const double cutoff_ratio    = g->cutoff_ratio;
     const double cutoff_ratio_sq = cutoff_ratio * cutoff_ratio;

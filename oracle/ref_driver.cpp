@@ -35,6 +35,9 @@
 #include <mjolnir/forcefield/global/ExcludedVolumePotential.hpp>
 #include <mjolnir/forcefield/global/DebyeHuckelPotential.hpp>
 #include <mjolnir/forcefield/global/LennardJonesPotential.hpp>
+#include <mjolnir/forcefield/global/WCAPotential.hpp>
+#include <mjolnir/forcefield/global/LennardJonesAttractivePotential.hpp>
+#include <mjolnir/forcefield/global/UniformLennardJonesPotential.hpp>
 #include <mjolnir/forcefield/local/BondLengthInteraction.hpp>
 #include <mjolnir/forcefield/local/BondAngleInteraction.hpp>
 #include <mjolnir/forcefield/local/DihedralAngleInteraction.hpp>
@@ -112,6 +115,10 @@ struct RefSim final : public RefSimBase
     using exv_pot = ExcludedVolumePotential<double>;
     using dh_pot  = DebyeHuckelPotential<double>;
     using lj_pot  = LennardJonesPotential<double>;
+    using wca_pot = WCAPotential<double>;
+    using lja_pot = LennardJonesAttractivePotential<double>;
+    using ulj_pot = UniformLennardJonesPotential<double>;
+    int lj_kind = ORC_LJ;
 
     std::unique_ptr<system_type>  sys;
     std::unique_ptr<ff_base_type> ff;
@@ -273,7 +280,12 @@ struct RefSim final : public RefSimBase
             globals[1] = p.get();
             global.emplace(std::move(p));
         }
-        if(s.lj_on)
+        lj_kind = s.lj_kind;
+        if(s.lj_on && s.lj_kind != ORC_LJ)
+        {
+            add_lj_family(s, global, within, mol_rule, is_periodic{});
+        }
+        else if(s.lj_on)
         {
             using plist = LorentzBerthelotRule<traitsT, lj_pot>;
             std::vector<std::pair<std::size_t, typename plist::parameter_type>> ps;
@@ -393,6 +405,44 @@ struct RefSim final : public RefSimBase
     long long dump(global_base*, const std::vector<std::size_t>&, long long*,
                    long long, std::false_type) {return -1;}
 
+    // WCA / LennardJonesAttractive (Lorentz-Berthelot parameters) and
+    // UniformLennardJones (one sigma and epsilon) through the generic
+    // GlobalPairInteraction, as input/read_global_potential.hpp builds them
+    template<typename potT, typename withinT, typename molT, typename periodicT>
+    void add_lb(const orc_spec& s, potT pot, GlobalForceField<traitsT>& global, const withinT& within,
+                const molT& mol_rule, periodicT per)
+    {
+        using plist = LorentzBerthelotRule<traitsT, potT>;
+        std::vector<std::pair<std::size_t, typename plist::parameter_type>> ps;
+        for(long long k=0; k<s.lj_n; ++k)
+        {
+            ps.emplace_back(std::size_t(s.lj_idx[k]), typename plist::parameter_type{s.lj_sigma[k], s.lj_eps[k]});
+        }
+        auto p = make_unique<GlobalPairInteraction<traitsT, potT>>(std::move(pot),
+            ParameterList<traitsT, potT>(make_unique<plist>(ps, within, IgnoreMolecule<std::size_t>(mol_rule),
+                IgnoreGroup<std::string>(std::map<std::string, std::vector<std::string>>{}))),
+            make_partition<potT>(s.lj_margin, per));
+        globals[2] = p.get();
+        global.emplace(std::move(p));
+    }
+    template<typename withinT, typename molT, typename periodicT>
+    void add_lj_family(const orc_spec& s, GlobalForceField<traitsT>& global, const withinT& within,
+                       const molT& mol_rule, periodicT per)
+    {
+        if(s.lj_kind == ORC_WCA)                {add_lb(s, wca_pot(), global, within, mol_rule, per); return;}
+        if(s.lj_kind == ORC_LJ_ATTRACTIVE)      {add_lb(s, lja_pot(s.lj_cutoff), global, within, mol_rule, per); return;}
+        using plist = EmptyCombinationRule<traitsT, ulj_pot>;
+        std::vector<std::size_t> parts;
+        for(long long k=0; k<s.lj_n; ++k) {parts.push_back(std::size_t(s.lj_idx[k]));}
+        auto p = make_unique<GlobalPairInteraction<traitsT, ulj_pot>>(
+            ulj_pot(s.lj_cutoff, s.lj_n > 0 ? s.lj_sigma[0] : 1.0, s.lj_n > 0 ? s.lj_eps[0] : 1.0),
+            ParameterList<traitsT, ulj_pot>(make_unique<plist>(parts, within, IgnoreMolecule<std::size_t>(mol_rule),
+                IgnoreGroup<std::string>(std::map<std::string, std::vector<std::string>>{}))),
+            make_partition<ulj_pot>(s.lj_margin, per));
+        globals[2] = p.get();
+        global.emplace(std::move(p));
+    }
+
     long long neighbors(int term, long long* pairs, long long cap) override
     {
         const int g = term - ORC_TERM_EXV;
@@ -400,6 +450,9 @@ struct RefSim final : public RefSimBase
         std::integral_constant<bool, Sequential> seq;
         if(g == 0) {return dump<exv_pot>(globals[0], leading[0], pairs, cap, seq);}
         if(g == 1) {return dump<dh_pot >(globals[1], leading[1], pairs, cap, seq);}
+        if(lj_kind == ORC_WCA)           {return dump<wca_pot>(globals[2], leading[2], pairs, cap, seq);}
+        if(lj_kind == ORC_LJ_ATTRACTIVE) {return dump<lja_pot>(globals[2], leading[2], pairs, cap, seq);}
+        if(lj_kind == ORC_LJ_UNIFORM)    {return dump<ulj_pot>(globals[2], leading[2], pairs, cap, seq);}
         return dump<lj_pot>(globals[2], leading[2], pairs, cap, seq);
     }
 

@@ -21,6 +21,8 @@ extern "C" {
 enum { ORC_UNLIMITED = 0, ORC_PERIODIC = 1 };
 enum { ORC_BAOAB = 0, ORC_VV = 1 };
 enum { ORC_IGNORE_NOTHING = 0, ORC_IGNORE_SELF = 1, ORC_IGNORE_OTHERS = 2 };
+/* potential of the third global term (Lennard-Jones family) */
+enum { ORC_LJ = 0, ORC_WCA = 1, ORC_LJ_ATTRACTIVE = 2, ORC_LJ_UNIFORM = 3 };
 enum { ORC_TERM_BOND = 0, ORC_TERM_ANGLE = 1, ORC_TERM_DIHEDRAL = 2,
        ORC_TERM_EXV = 3, ORC_TERM_DH = 4, ORC_TERM_LJ = 5, ORC_NTERMS = 6 };
 
@@ -51,6 +53,7 @@ typedef struct orc_spec
     int32_t lj_on;   double lj_cutoff, lj_margin;
     int64_t lj_n;    const int64_t* lj_idx;  const double* lj_sigma;
     const double* lj_eps;
+    int32_t lj_kind;             /* ORC_LJ / ORC_WCA / ORC_LJ_ATTRACTIVE / ORC_LJ_UNIFORM */
 
     /* local terms (BondLength topology "bond"; angle/dihedral "none")     */
     int64_t nbond;   const int64_t* bond_idx;  const double* bond_k;

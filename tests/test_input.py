@@ -175,7 +175,7 @@ include = "ff.toml"
 
 
 @pytest.mark.parametrize("edit, msg", [
-    (lambda t: t.replace('potential   = "LennardJones"', 'potential   = "WCA"'), "WCA"),
+    (lambda t: t.replace('potential   = "LennardJones"', 'potential   = "InversePower"'), "InversePower"),
     (lambda t: t.replace('ignore.molecule = "Nothing"', 'ignore.molecule = "Nothing"\nignore.group.intra = ["A"]'),
      "ignore.group"),
     (lambda t: t.replace('length = "angstrom"', 'length = "nm"'), "angstrom"),
@@ -230,3 +230,31 @@ def test_linear_schedule_matches_reference_formula():
     from mjolnir_b200.anneal import current
     assert current(350.0, 280.0, 0.0) == 350.0 and current(350.0, 280.0, 1.0) == 280.0
     assert current(300.0, 100.0, 0.25) == 300.0 * 0.75 + 100.0 * 0.25
+
+
+@pytest.mark.parametrize("kind", ["WCA", "LennardJonesAttractive", "UniformLennardJones"])
+def test_lj_family_round_trip(kind, tmp_path):
+    from lj_family import fluid
+    d = fluid(kind, n=64)
+    path = str(tmp_path / "f.toml")
+    I.dump(d, path)
+    g = I.load(path).desc
+    assert g.lj.kind == kind and g.lj.cutoff == d.lj.cutoff
+    np.testing.assert_array_equal(g.lj.idx, d.lj.idx)
+    np.testing.assert_array_equal(g.lj.param0, d.lj.param0)
+    np.testing.assert_array_equal(g.lj.param1, d.lj.param1)
+
+
+def test_uniform_lj_without_parameters_takes_every_particle(tmp_path):
+    text = HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF
+    start = text.index("[[forcefields.global]]")
+    text = text[:start] + """[[forcefields.global]]
+interaction = "Pair"
+potential   = "UniformLennardJones"
+sigma = 1.5
+epsilon = 0.4
+spatial_partition = {type = "CellList", margin = 0.3}
+"""
+    d = I.load(_write(tmp_path, "u.toml", text)).desc
+    np.testing.assert_array_equal(d.lj.idx, np.arange(4))
+    assert set(d.lj.param0) == {1.5} and set(d.lj.param1) == {0.4} and d.lj.cutoff == 2.5
