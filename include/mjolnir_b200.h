@@ -130,6 +130,17 @@ MJG_API int mjg_dh_set(mjg_context* ctx, int sys, double cutoff_ratio, double ma
  * (forcefield/global/LennardJonesPotential.hpp:15-110, ParameterList.hpp:185-329). */
 MJG_API int mjg_lj_set(mjg_context* ctx, int sys, double cutoff_ratio, double margin,
                int64_t np, const int64_t* idx, const double* sigma, const double* epsilon);
+/* The first global term with another potential of the ExcludedVolume
+ * family, by the reference's input name: "InversePower"
+ * (forcefield/global/InversePowerPotential.hpp; per-particle radius in p0,
+ * sigma_ij = r_i + r_j, E = eps ((sigma/r)^n - rc^-n), exponent `power`) or
+ * "HardCoreExcludedVolume" (HardCoreExcludedVolumePotential.hpp; per-particle
+ * soft_shell_thickness in p0 and core_radius in p1, sigma_ij and R_ij the
+ * sums, E = eps ((sigma / (r - R))^12 - rc^-12)).  Both run through the
+ * generic pair loop (GlobalPairInteraction.hpp:148-213). */
+MJG_API int mjg_exv_family_set(mjg_context* ctx, int sys, const char* potential, double epsilon,
+                               double cutoff_ratio, int power, double margin, int64_t np,
+                               const int64_t* idx, const double* p0, const double* p1);
 /* The third global term with any potential of the Lennard-Jones family, by
  * the name the reference's input uses: "LennardJones" (as mjg_lj_set),
  * "WCA" (forcefield/global/WCAPotential.hpp; its cutoff is fixed at

@@ -41,6 +41,8 @@ SIGNATURES = {
     "mjg_system_freeze": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "mjg_exv_set": (C.c_int, [_ctx, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int64, _i64p, _f64p]),
     "mjg_dh_set": (C.c_int, [_ctx, C.c_int, C.c_double, C.c_double, C.c_int64, _i64p, _f64p]),
+    "mjg_exv_family_set": (C.c_int, [_ctx, C.c_int, C.c_char_p, C.c_double, C.c_double, C.c_int, C.c_double,
+                                     C.c_int64, _i64p, _f64p, _f64p]),
     "mjg_pair_set": (C.c_int, [_ctx, C.c_int, C.c_char_p, C.c_double, C.c_double, C.c_int64, _i64p, _f64p, _f64p]),
     "mjg_lj_set": (C.c_int, [_ctx, C.c_int, C.c_double, C.c_double, C.c_int64, _i64p, _f64p, _f64p]),
     "mjg_ignore_set": (C.c_int, [_ctx, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_char_p), _i32p]),

@@ -43,6 +43,10 @@ constexpr double FX_MAGIC     = 6755399441055744.0;     // 1.5 * 2^52
 // forcefield/global/GlobalPairLennardJonesInteraction.hpp) or a potential of
 // the family through the generic pair loop (GlobalPairInteraction.hpp:148-213)
 enum LjKind { LJ_PLAIN = 0, LJ_WCA = 1, LJ_ATTRACTIVE = 2, LJ_UNIFORM = 3 };
+// potential of the first global term: ExcludedVolume (its own interaction,
+// GlobalPairExcludedVolumeInteraction.hpp) or InversePower /
+// HardCoreExcludedVolume through the generic pair loop
+enum ExvKind { EXV_PLAIN = 0, EXV_INVERSE_POWER = 1, EXV_HARD_CORE = 2 };
 constexpr double SIXTH_ROOT_OF_TWO = 1.12246204831;   // WCAPotential.hpp default_cutoff
 
 struct GlobalParams {       // per system, per global term
@@ -68,7 +72,8 @@ struct GlobalParams {       // per system, per global term
     int    ignore_mol;      // IgnoreMol
     int    rebuild;         // set by the margin kernel, cleared after a rebuild
     int    rebuilds;        // rebuild counter
-    int    kind;            // third term's potential (LjKind)
+    int    kind;            // the term's potential (ExvKind for the first, LjKind for the third)
+    int    power;           // InversePower exponent n
     int    on;
 };
 

@@ -83,7 +83,8 @@ struct DevBuf {
 
 struct HostGlobal {
     bool on = false;
-    int kind = LJ_PLAIN;         // third term: potential of the Lennard-Jones family
+    int kind = 0;                // potential within the term's family (ExvKind / LjKind)
+    int power = 12;              // InversePower n
     double eps = 0.0, cutoff_ratio = 0.0, margin = 0.5;
     std::vector<int64_t> idx;
     std::vector<double> p0, p1;
@@ -682,12 +683,20 @@ void make_sysdev(const HostSystem& s, SysDev& d)
         G.ignore_mol = H.ignore_mol;
         G.eps = H.eps;
         const int64_t np = (int64_t)H.idx.size();
-        if(g == G_EXV)             // ExcludedVolumePotential.hpp:44-48,92-106
+        if(g == G_EXV)             // ExcludedVolumePotential.hpp:44-48,92-106 and the family
         {
-            G.coef_at_cutoff = std::pow(1.0 / H.cutoff_ratio, 12);
-            double mr = 0;
+            G.kind = H.kind;
+            G.power = H.power;
+            G.coef_at_cutoff = H.kind == EXV_INVERSE_POWER ? std::pow(1.0 / H.cutoff_ratio, H.power)
+                                                          : std::pow(1.0 / H.cutoff_ratio, 12);
+            double mr = 0, mc = 0;
             for(double r : H.p0) {mr = std::max(mr, r);}
             G.cutoff = np == 0 ? 1.0 : mr * 2 * H.cutoff_ratio;
+            if(H.kind == EXV_HARD_CORE && np > 0)   // HardCoreExcludedVolumePotential.hpp:109-126
+            {
+                for(double c : H.p1) {mc = std::max(mc, c);}
+                G.cutoff = mr * 2 * H.cutoff_ratio + mc * 2;
+            }
         }
         else if(g == G_DH)         // DebyeHuckelPotential.hpp:126-167,245-248
         {
@@ -1050,7 +1059,7 @@ void commit(mjg_context* c)
         CK(cudaMemsetAsync(T.nnb.p, 0, T.nnb.bytes, st));
         t.part_particle = T.part_particle.as<int>();
         t.part_p0 = T.part_p0.as<double>();
-        t.part_p1 = g == G_LJ ? T.part_p1.as<double>() : nullptr;
+        t.part_p1 = T.part_p1.as<double>();     // LJ-family epsilon, HardCore core radius
         t.part_lead = T.part_lead.as<unsigned char>();
         t.part_sys = T.part_sys.as<int>();
         t.part_cell = T.part_cell.as<int>();
@@ -1478,7 +1487,7 @@ int mjg_exv_set(mjg_context* c, int sys, double eps, double cutoff_ratio, double
     check_idx(s, np, idx);
     if(!(cutoff_ratio > 0) || !(margin >= 0) || (np > 0 && !radius)) {throw Error(MJG_EINVAL, "bad ExcludedVolume parameters");}
     HostGlobal& g = s.g[G_EXV];
-    g.on = true; g.eps = eps; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
+    g.on = true; g.kind = EXV_PLAIN; g.eps = eps; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
     g.idx.assign(idx, idx + np); g.p0.assign(radius, radius + np); g.p1.clear();
     ABI_END(c)
 }
@@ -1508,6 +1517,32 @@ int mjg_lj_set(mjg_context* c, int sys, double cutoff_ratio, double margin, int6
     HostGlobal& g = s.g[G_LJ];
     g.on = true; g.kind = LJ_PLAIN; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
     g.idx.assign(idx, idx + np); g.p0.assign(sigma, sigma + np); g.p1.assign(epsilon, epsilon + np);
+    ABI_END(c)
+}
+
+int mjg_exv_family_set(mjg_context* c, int sys, const char* potential, double eps, double cutoff_ratio,
+                       int power, double margin, int64_t np, const int64_t* idx, const double* p0,
+                       const double* p1)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(s.resident) {throw Error(MJG_ESTATE, "interactions are fixed once committed");}
+    if(!potential) {throw Error(MJG_EINVAL, "potential name is NULL");}
+    const std::string name(potential);
+    int kind;
+    if(name == "InversePower")                {kind = EXV_INVERSE_POWER;}
+    else if(name == "HardCoreExcludedVolume") {kind = EXV_HARD_CORE;}
+    else {throw Error(MJG_EINVAL, "unknown ExcludedVolume-family potential: " + name);}
+    check_idx(s, np, idx);
+    if(!(cutoff_ratio > 0) || !(margin >= 0) || (np > 0 && !p0) || (kind == EXV_HARD_CORE && np > 0 && !p1) ||
+       (kind == EXV_INVERSE_POWER && power <= 0))
+    {
+        throw Error(MJG_EINVAL, "bad " + name + " parameters");
+    }
+    HostGlobal& g = s.g[G_EXV];
+    g.on = true; g.kind = kind; g.power = power; g.eps = eps; g.cutoff_ratio = cutoff_ratio; g.margin = margin;
+    g.idx.assign(idx, idx + np); g.p0.assign(p0, p0 + np);
+    if(kind == EXV_HARD_CORE) {g.p1.assign(p1, p1 + np);} else {g.p1.clear();}
     ABI_END(c)
 }
 

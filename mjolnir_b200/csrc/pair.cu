@@ -100,7 +100,7 @@ struct PairEval {
     bool periodic;
     double crsq, coefc, eps, eps12, debye, inv_debye, abs_cut_sq, qi, inv4pi, epsi, cr;
     float eps12f, epsf, coefcf, debf, invdf;
-    int kind;
+    int kind, power;
     const double* slot_p1;
 
     __device__ __forceinline__ PairEval(const Arena& a, const TermArrays& t, long long slot, int sys)
@@ -113,6 +113,7 @@ struct PairEval {
         crsq  = P.cutoff_ratio_sq;
         cr    = P.cutoff_ratio;
         kind  = P.kind;
+        power = P.power;
         coefc = P.coef_at_cutoff;
         eps   = P.eps;
         eps12 = eps * 12;
@@ -120,7 +121,8 @@ struct PairEval {
         abs_cut_sq = P.abs_cutoff * P.abs_cutoff;
         qi = pi.w; inv4pi = P.inv4pi;
         slot_p1 = t.slot_p1;
-        epsi  = (G == G_LJ) ? t.slot_p1[slot] : 0.0;
+        // second per-slot parameter: LJ-family epsilon, HardCore core radius
+        epsi  = (G == G_LJ || (G == G_EXV && kind == EXV_HARD_CORE)) ? t.slot_p1[slot] : 0.0;
         eps12f = (float)eps12; epsf = (float)eps; coefcf = (float)coefc;
         debf = (float)debye; invdf = (float)inv_debye;
     }
@@ -207,6 +209,67 @@ struct PairEval {
         }
     }
 
+    // InversePower (InversePowerPotential.hpp:38-57; sigma_ij = r_i + r_j)
+    // and HardCoreExcludedVolume (HardCoreExcludedVolumePotential.hpp:44-80;
+    // sigma_ij = s_i + s_j, R_ij = c_i + c_j) through the generic pair loop
+    template<typename T>
+    __device__ __forceinline__ T exv_derivative(T r, T sigma, T radius) const
+    {
+        if(kind == EXV_INVERSE_POWER)
+        {
+            if(sigma * T(cr) < r) {return T(0);}
+            const T rinv = T(1) / r;
+            const T d_r = sigma * rinv;
+            const T drn = pow(d_r, T(power));
+            return T(-power) * T(eps) * drn * rinv;
+        }
+        if(sigma * T(cr) + radius < r) {return T(0);}
+        if(r < radius) {return T(INFINITY);}
+        const T gapinv = T(1) / (r - radius);
+        const T s1 = sigma * gapinv;
+        const T s3 = s1 * s1 * s1;
+        const T s6 = s3 * s3;
+        return T(-12) * T(eps) * s6 * s6 * gapinv;
+    }
+    template<typename T>
+    __device__ __forceinline__ T exv_potential(T r, T sigma, T radius) const
+    {
+        if(kind == EXV_INVERSE_POWER)
+        {
+            if(sigma * T(cr) < r) {return T(0);}
+            const T d_r = sigma / r;
+            const T drn = pow(d_r, T(power));
+            return T(eps) * (drn - T(coefc));
+        }
+        if(sigma * T(cr) + radius < r) {return T(0);}
+        if(r < radius) {return T(INFINITY);}
+        const T gap = r - radius;
+        const T s1 = sigma / gap;
+        const T s3 = s1 * s1 * s1;
+        const T s6 = s3 * s3;
+        return T(eps) * (s6 * s6 - T(coefc));
+    }
+    __device__ __forceinline__ void exv_family(double sigma, double radius, double l2, double dx, double dy,
+                                               double dz, bool count_e, Acc<PREC>& acc, double& energy,
+                                               bool& ovf) const
+    {
+        using T = typename std::conditional<PREC == P_FP64, double, float>::type;
+        if(NF)
+        {
+            const T rl = PREC == P_FP64 ? T(rsqrt(l2)) : T(rsqrtf((float)l2));
+            const T l  = T(l2) * rl;
+            const T f_mag = exv_derivative<T>(l, T(sigma), T(radius));
+            if(f_mag == T(0)) {return;}
+            acc.add((double)(f_mag * rl), dx, dy, dz, ovf);
+            if(count_e) {energy += (double)exv_potential<T>(l, T(sigma), T(radius));}
+        }
+        else if(count_e)
+        {
+            const T l = PREC == P_FP64 ? T(sqrt(l2)) : sqrtf((float)l2);
+            energy += (double)exv_potential<T>(l, T(sigma), T(radius));
+        }
+    }
+
     __device__ __forceinline__ void operator()(const double4& pj, const int q, Acc<PREC>& acc,
                                                double& energy, bool& ovf) const
     {
@@ -221,6 +284,12 @@ struct PairEval {
         const bool count_e = NE && (s < q);
         if(G == G_EXV)
         {
+            if(kind != EXV_PLAIN)
+            {
+                const double radius = kind == EXV_HARD_CORE ? epsi + slot_p1[q] : 0.0;
+                exv_family(pi.w + pj.w, radius, l2, dx, dy, dz, count_e, acc, energy, ovf);
+                return;
+            }
             const double sigma = pi.w + pj.w;
             const double sigma_sq = sigma * sigma;
             const bool in = !(sigma_sq * crsq < l2);
@@ -618,7 +687,12 @@ __global__ void k_count_cut(Arena a, TermArrays t, int sys_filter, unsigned long
             }
             const double l2 = fma(dz, dz, fma(dy, dy, dx * dx));
             bool in = false;
-            if(G == G_EXV)     {const double sg = pi.w + pj.w; in = !(sg * sg * P.cutoff_ratio_sq < l2);}
+            if(G == G_EXV && P.kind == EXV_HARD_CORE)
+            {
+                const double sg = pi.w + pj.w, core = t.slot_p1[s] + t.slot_p1[q];
+                in = !(sg * P.cutoff_ratio + core < sqrt(l2));
+            }
+            else if(G == G_EXV) {const double sg = pi.w + pj.w; in = !(sg * sg * P.cutoff_ratio_sq < l2);}
             else if(G == G_DH) {in = l2 < P.abs_cutoff * P.abs_cutoff;}
             else               {const double sg = (pi.w + pj.w) / 2; in = !(sg * sg * P.cutoff_ratio_sq < l2);}
             cnt += in ? 1 : 0;

@@ -87,9 +87,14 @@ class Engine:
                 within = [("bond", d.ignore_bond_within)] if d.ignore_bond_within > 0 else []
             idx = _arr(t.idx, np.int64)
             p0 = _arr(t.param0, np.float64)
-            if term == A.TERM_EXV:
+            if term == A.TERM_EXV and t.kind == "ExcludedVolume":
                 self._c(L.mjg_exv_set(self.ctx, s, float(t.epsilon), float(t.cutoff), float(t.margin),
                                       len(idx), A.i64(idx), A.f64(p0)))
+            elif term == A.TERM_EXV:                # InversePower, HardCoreExcludedVolume
+                p1 = _arr(t.param1, np.float64) if t.param1 is not None else None
+                self._c(L.mjg_exv_family_set(self.ctx, s, t.kind.encode(), float(t.epsilon), float(t.cutoff),
+                                             int(t.exponent), float(t.margin), len(idx), A.i64(idx),
+                                             A.f64(p0), A.f64(p1)))
             elif term == A.TERM_DH:
                 self._c(L.mjg_dh_set(self.ctx, s, float(t.cutoff), float(t.margin), len(idx),
                                      A.i64(idx), A.f64(p0)))

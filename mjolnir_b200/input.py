@@ -26,7 +26,9 @@ ready for :meth:`Engine.add_system`:
   BondAngle with Harmonic (``k``, ``v0``) and DihedralAngle with Cosine
   (``k``, ``n``, ``v0``), ``indices`` plus an optional ``offset``
   (input/read_local_potential.hpp:473-522); ``[[forcefields.global]]`` Pair
-  with ExcludedVolume (``epsilon``, ``radius``), DebyeHuckel (``charge``),
+  with ExcludedVolume (``epsilon``, ``radius``), InversePower (``epsilon``,
+  ``n``, ``radius``; cutoff default 2^(12/n)), HardCoreExcludedVolume
+  (``epsilon``, ``soft_shell_thickness``, ``core_radius``), DebyeHuckel (``charge``),
   LennardJones, WCA or LennardJonesAttractive (``sigma|σ``, ``epsilon|ε``) or
   UniformLennardJones (global ``sigma``, ``epsilon``; ``parameters`` optional),
   ``cutoff`` (defaults 2.0 / 5.5 / 2.5; WCA's is fixed at 2^(1/6)),
@@ -57,7 +59,8 @@ import numpy as np
 
 from .systems import KB_KCAL, PairTerm, SystemDesc
 
-DEFAULT_CUTOFF = {"ExcludedVolume": 2.0, "DebyeHuckel": 5.5, "LennardJones": 2.5,
+DEFAULT_CUTOFF = {"ExcludedVolume": 2.0, "HardCoreExcludedVolume": 2.0, "InversePower": None,
+                  "DebyeHuckel": 5.5, "LennardJones": 2.5,
                   "WCA": 1.12246204831, "LennardJonesAttractive": 2.5, "UniformLennardJones": 2.5}
 LJ_FAMILY = ("LennardJones", "WCA", "LennardJonesAttractive", "UniformLennardJones")
 LOCAL_FORMS = {("BondLength", "Harmonic"): 2, ("BondAngle", "Harmonic"): 3,
@@ -305,8 +308,10 @@ def _global(g, n, where):
         raise InputError(f'{where}: "{inter}" / "{pot}" is not run here (Pair with ExcludedVolume, '
                          "DebyeHuckel, LennardJones, WCA, LennardJonesAttractive or UniformLennardJones)")
     allowed = {"interaction", "potential", "ignore", "spatial_partition", "parameters", "env", "cutoff"}
-    if pot in ("ExcludedVolume", "UniformLennardJones"):
+    if pot in ("ExcludedVolume", "UniformLennardJones", "InversePower", "HardCoreExcludedVolume"):
         allowed |= {"epsilon"}
+    if pot == "InversePower":
+        allowed |= {"n"}
     if pot == "UniformLennardJones":
         allowed |= {"sigma"}
     if "table" in g:
@@ -325,12 +330,31 @@ def _global(g, n, where):
     _no_overlap(idx.tolist(), where)
     if idx.size and (idx.min() < 0 or idx.max() >= n):
         raise InputError(f"{where}: participant index out of range")
-    # WCA's cutoff is fixed (input/read_global_potential.hpp warns and ignores it)
-    cutoff = DEFAULT_CUTOFF[pot] if pot == "WCA" else float(g.get("cutoff", DEFAULT_CUTOFF[pot]))
+    # WCA's cutoff is fixed (input/read_global_potential.hpp warns and ignores it);
+    # InversePower's default is 2^(12 / n) with an integer quotient
+    # (InversePowerPotential.hpp:27-30)
+    if pot == "InversePower":
+        if "n" not in g or "epsilon" not in g:
+            raise InputError(f"{where}: InversePower needs epsilon and n")
+        power = int(g["n"])
+        if power <= 0:
+            raise InputError(f"{where}: InversePower n must be positive")
+        cutoff = float(g.get("cutoff", 2.0 ** (12 // power)))
+    else:
+        cutoff = DEFAULT_CUTOFF[pot] if pot == "WCA" else float(g.get("cutoff", DEFAULT_CUTOFF[pot]))
     mol, within = _ignore(g, where)
-    if pot == "ExcludedVolume":
+    if pot in ("ExcludedVolume", "InversePower"):
+        if "epsilon" not in g:
+            raise InputError(f"{where}: {pot} needs epsilon")
         p0 = np.array([float(_param(it, env, "radius", where=where)) for it in items])
-        term = PairTerm(pot, idx, p0, cutoff=cutoff, margin=margin, epsilon=float(g["epsilon"]))
+        term = PairTerm(pot, idx, p0, cutoff=cutoff, margin=margin, epsilon=float(g["epsilon"]),
+                        exponent=power if pot == "InversePower" else 12)
+    elif pot == "HardCoreExcludedVolume":
+        if "epsilon" not in g:
+            raise InputError(f"{where}: HardCoreExcludedVolume needs epsilon")
+        p0 = np.array([float(_param(it, env, "soft_shell_thickness", where=where)) for it in items])
+        p1 = np.array([float(_param(it, env, "core_radius", where=where)) for it in items])
+        term = PairTerm(pot, idx, p0, p1, cutoff=cutoff, margin=margin, epsilon=float(g["epsilon"]))
     elif pot == "DebyeHuckel":
         p0 = np.array([float(_param(it, env, "charge", where=where)) for it in items])
         term = PairTerm(pot, idx, p0, cutoff=cutoff, margin=margin)
@@ -396,10 +420,11 @@ def _forcefield(ff, n, input_path, base_dir):
     for i, g in enumerate(ff.get("global", [])):
         g = _from_file(g, "global", input_path, base_dir)
         t = _global(g, n, f"forcefields.global[{i}]")
-        key = {"ExcludedVolume": "exv", "DebyeHuckel": "dh"}.get(t.kind, "lj")
+        key = {"ExcludedVolume": "exv", "InversePower": "exv", "HardCoreExcludedVolume": "exv",
+               "DebyeHuckel": "dh"}.get(t.kind, "lj")
         if key in pairs:
-            raise InputError(f"forcefields.global[{i}]: a second {'Lennard-Jones family' if key == 'lj' else t.kind} "
-                             "term is not supported")
+            family = {"exv": "ExcludedVolume-family", "dh": "DebyeHuckel", "lj": "Lennard-Jones-family"}[key]
+            raise InputError(f"forcefields.global[{i}]: a second {family} term is not supported")
         pairs[key] = t
     locs = {}
     for i, loc in enumerate(ff.get("local", [])):
@@ -611,8 +636,10 @@ def dumps(desc: SystemDesc, total_step: int = 1000, save_step: int = 100, prefix
         a(f"potential = {_fmt(t.kind)}")
         if t.kind != "WCA":
             a(f"cutoff = {_fmt(float(t.cutoff))}")
-        if t.kind == "ExcludedVolume":
+        if t.kind in ("ExcludedVolume", "InversePower", "HardCoreExcludedVolume"):
             a(f"epsilon = {_fmt(float(t.epsilon))}")
+        if t.kind == "InversePower":
+            a(f"n = {int(t.exponent)}")
         if t.kind == "UniformLennardJones":
             a(f"sigma = {_fmt(float(t.param0[0]))}")
             a(f"epsilon = {_fmt(float(t.param1[0]))}")
@@ -623,10 +650,15 @@ def dumps(desc: SystemDesc, total_step: int = 1000, save_step: int = 100, prefix
         a(f"ignore.molecule = {_fmt(mol)}")
         a("ignore.particles_within = {" + ", ".join(f"{k} = {int(v)}" for k, v in within.items()) + "}")
         a("parameters = [")
-        name = {"ExcludedVolume": "radius", "DebyeHuckel": "charge"}.get(t.kind, "sigma")
+        name = {"ExcludedVolume": "radius", "InversePower": "radius", "DebyeHuckel": "charge",
+                "HardCoreExcludedVolume": "soft_shell_thickness"}.get(t.kind, "sigma")
         for q in range(len(t.idx)):
             if t.kind == "UniformLennardJones":
                 a(f"  {{index = {int(t.idx[q])}}},")
+                continue
+            if t.kind == "HardCoreExcludedVolume":
+                a(f"  {{index = {int(t.idx[q])}, soft_shell_thickness = {_fmt(float(t.param0[q]))}, "
+                  f"core_radius = {_fmt(float(t.param1[q]))}}},")
                 continue
             extra = f", epsilon = {_fmt(float(t.param1[q]))}" if t.kind in LJ_FAMILY else ""
             a(f"  {{index = {int(t.idx[q])}, {name} = {_fmt(float(t.param0[q]))}{extra}}},")

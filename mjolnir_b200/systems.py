@@ -24,15 +24,17 @@ KB_KCAL = 1.38064852e-23 * (1.0 / 4.184 / 1000.0) * 6.022140857e23  # kB in kcal
 @dataclasses.dataclass
 class PairTerm:
     """One ``[[forcefields.global]]`` pair interaction."""
-    kind: str                          # "ExcludedVolume" | "DebyeHuckel" | "LennardJones" | "WCA" |
-                                       # "LennardJonesAttractive" | "UniformLennardJones" (the last
-                                       # four share the third global term, SystemDesc.lj)
+    kind: str                          # "ExcludedVolume" | "InversePower" | "HardCoreExcludedVolume"
+                                       # (the first global term, SystemDesc.exv) | "DebyeHuckel" |
+                                       # "LennardJones" | "WCA" | "LennardJonesAttractive" |
+                                       # "UniformLennardJones" (the third, SystemDesc.lj)
     idx: np.ndarray                    # participant particle indices (input order)
-    param0: np.ndarray                 # radius | charge | sigma
-    param1: Optional[np.ndarray] = None  # LJ epsilon
+    param0: np.ndarray                 # radius | charge | sigma (HardCore: soft_shell_thickness)
+    param1: Optional[np.ndarray] = None  # LJ-family epsilon | HardCore core_radius
     cutoff: float = 2.0                # relative cutoff (potential default)
     margin: float = 0.5                # relative Verlet skin of the cell list
-    epsilon: float = 0.2               # ExcludedVolume epsilon
+    epsilon: float = 0.2               # ExcludedVolume / InversePower / HardCoreExcludedVolume epsilon
+    exponent: int = 12                 # InversePower n
     # this term's own ``ignore`` table; None falls back to the system-wide rule
     ignore_molecule: Optional[str] = None       # "Nothing" | "Self" | "Others"
     ignore_within: Optional[dict] = None        # {connection kind: topological distance}

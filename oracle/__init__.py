@@ -45,6 +45,7 @@ class OrcSpec(C.Structure):
         ("exv_on", C.c_int32), ("exv_eps", C.c_double), ("exv_cutoff", C.c_double),
         ("exv_margin", C.c_double), ("exv_n", C.c_int64), ("exv_idx", _i64p),
         ("exv_radius", _f64p),
+        ("exv_kind", C.c_int32), ("exv_power", C.c_int32), ("exv_core", _f64p),
         ("dh_on", C.c_int32), ("dh_cutoff", C.c_double), ("dh_margin", C.c_double),
         ("dh_n", C.c_int64), ("dh_idx", _i64p), ("dh_charge", _f64p),
         ("lj_on", C.c_int32), ("lj_cutoff", C.c_double), ("lj_margin", C.c_double),
@@ -63,6 +64,7 @@ def _ptr(a, ct):
 
 
 LJ_KINDS = {"LennardJones": 0, "WCA": 1, "LennardJonesAttractive": 2, "UniformLennardJones": 3}
+EXV_KINDS = {"ExcludedVolume": 0, "InversePower": 1, "HardCoreExcludedVolume": 2}
 
 
 def _uniform_ignore(desc):
@@ -119,6 +121,10 @@ def make_spec(desc):
         s.exv_n = len(t.idx)
         s.exv_idx = _ptr(arr(t.idx, np.int64), C.c_int64)
         s.exv_radius = _ptr(arr(t.param0, np.float64), C.c_double)
+        s.exv_kind = EXV_KINDS[t.kind]
+        s.exv_power = int(t.exponent)
+        if t.kind == "HardCoreExcludedVolume":
+            s.exv_core = _ptr(arr(t.param1, np.float64), C.c_double)
     if desc.dh is not None:
         t = desc.dh
         s.dh_on, s.dh_cutoff, s.dh_margin = 1, t.cutoff, t.margin

@@ -72,7 +72,8 @@ typedef struct
     /* potential constants */
     double   eps, cutoff_ratio, coef_at_cutoff;
     double   dh[5];
-    int      kind;       /* third term: ORC_LJ / ORC_WCA / ORC_LJ_ATTRACTIVE / ORC_LJ_UNIFORM */
+    int      kind;       /* first term: ORC_EXV ...; third term: ORC_LJ ...           */
+    int      power;      /* InversePower n                                            */
     /* current half list: partners of particle i are nbr[lb[i] .. le[i]) */
     int64_t* lb;
     int64_t* le;
@@ -305,12 +306,25 @@ static void setup_global(orc_state* st, int gi, int on, int64_t np, const int64_
     g->cutoff_ratio = cutoff_ratio;
     g->lb = calloc((size_t)n, sizeof(int64_t));
     g->le = calloc((size_t)n, sizeof(int64_t));
-    if(gi == 0)        /* ExcludedVolumePotential.hpp:44-48, :92-106 */
+    if(gi == 0)        /* ExcludedVolumePotential.hpp:44-48, :92-106 and the family */
     {
-        g->coef_at_cutoff = pow(1.0 / cutoff_ratio, 12);
-        double mr = 0;
+        g->kind = st->s.exv_kind;
+        g->power = st->s.exv_power;
+        /* InversePowerPotential.hpp:32-36: (1/rc)^n; the others (1/rc)^12 */
+        g->coef_at_cutoff = g->kind == ORC_INVERSE_POWER ? pow(1.0 / cutoff_ratio, g->power)
+                                                        : pow(1.0 / cutoff_ratio, 12);
+        double mr = 0, mc = 0;
         for(int64_t k=0; k<np; ++k) {if(mr < p0[k]) {mr = p0[k];}}
-        g->cutoff = np == 0 ? 1.0 : mr * 2 * cutoff_ratio;
+        if(g->kind == ORC_HARD_CORE_EXV)
+        {
+            for(int64_t k=0; k<np; ++k) {if(mc < p1[k]) {mc = p1[k];}}
+            /* HardCoreExcludedVolumePotential.hpp:109-126 */
+            g->cutoff = np == 0 ? 1.0 : mr * 2 * cutoff_ratio + mc * 2;
+        }
+        else
+        {
+            g->cutoff = np == 0 ? 1.0 : mr * 2 * cutoff_ratio;
+        }
     }
     else if(gi == 1)   /* DebyeHuckelPotential.hpp:126-167, :245-248 */
     {
@@ -373,7 +387,8 @@ orc_state* orc_create(const orc_spec* s)
     build_exclusions(st, &g);
     free(g.off); free(g.adj);
 
-    setup_global(st, 0, s->exv_on, s->exv_n, s->exv_idx, s->exv_radius, NULL, s->exv_cutoff, s->exv_margin);
+    setup_global(st, 0, s->exv_on, s->exv_n, s->exv_idx, s->exv_radius,
+                 s->exv_kind == ORC_HARD_CORE_EXV ? s->exv_core : NULL, s->exv_cutoff, s->exv_margin);
     setup_global(st, 1, s->dh_on,  s->dh_n,  s->dh_idx,  s->dh_charge,  NULL, s->dh_cutoff,  s->dh_margin);
     setup_global(st, 2, s->lj_on,  s->lj_n,  s->lj_idx,  s->lj_sigma,   s->lj_eps, s->lj_cutoff, s->lj_margin);
     if(s->exv_on) {st->g[0].eps = s->exv_eps;}
@@ -579,9 +594,13 @@ int64_t orc_neighbors(const orc_state* st, int term, const double* pos,
 /* ---------------------------------------------------------------- forces */
 
 /* forcefield/global/GlobalPairExcludedVolumeInteraction.hpp:148-195 */
+static double exvfam_force(const orc_state* st, const orc_global* g, const double* pos,
+                           double* force, int need_force);
+
 static double exv_force(const orc_state* st, const orc_global* g, const double* pos,
                         double* force, int need_force)
 {
+    if(g->kind != ORC_EXV) {return exvfam_force(st, g, pos, force, need_force);}
     const double coef_at_cutoff  = g->coef_at_cutoff;
     const double cutoff_ratio    = g->cutoff_ratio;
     const double cutoff_ratio_sq = cutoff_ratio * cutoff_ratio;
@@ -668,6 +687,87 @@ static double dh_force(const orc_state* st, const orc_global* g, const double* p
                 const double l = sqrt(l2);
                 energy += (abs_cutoff <= l) ? 0.0 :
                           qq * (exp(-l * inv_debye) / l - coef_at_cutoff);
+            }
+        }
+    }
+    return energy;
+}
+
+/* The ExcludedVolume family through the generic pair loop
+ * (GlobalPairInteraction.hpp:148-213): InversePowerPotential
+ * (InversePowerPotential.hpp:38-57, sigma_ij = r_i + r_j, :185-188) and
+ * HardCoreExcludedVolumePotential (HardCoreExcludedVolumePotential.hpp:44-80,
+ * sigma_ij = s_i + s_j and R_ij = c_i + c_j, :209-217). */
+static double exvfam_derivative(const orc_global* g, double r, double sigma, double radius)
+{
+    if(g->kind == ORC_INVERSE_POWER)
+    {
+        if(sigma * g->cutoff_ratio < r) {return 0.0;}
+        const double rinv = 1.0 / r;
+        const double d_r = sigma * rinv;
+        const double drn = pow(d_r, g->power);
+        return -g->power * g->eps * drn * rinv;
+    }
+    if(sigma * g->cutoff_ratio + radius < r) {return 0.0;}
+    if(r < radius) {return INFINITY;}
+    const double gapinv = 1 / (r - radius);
+    const double sigma1gap1 = sigma * gapinv;
+    const double sigma3gap3 = sigma1gap1 * sigma1gap1 * sigma1gap1;
+    const double sigma6gap6 = sigma3gap3 * sigma3gap3;
+    return -12.0 * g->eps * sigma6gap6 * sigma6gap6 * gapinv;
+}
+
+static double exvfam_potential(const orc_global* g, double r, double sigma, double radius)
+{
+    if(g->kind == ORC_INVERSE_POWER)
+    {
+        if(sigma * g->cutoff_ratio < r) {return 0.0;}
+        const double d_r = sigma / r;
+        const double drn = pow(d_r, g->power);
+        return g->eps * (drn - g->coef_at_cutoff);
+    }
+    if(sigma * g->cutoff_ratio + radius < r) {return 0;}
+    if(r < radius) {return INFINITY;}
+    const double gap = r - radius;
+    const double sigma1gap1 = sigma / gap;
+    const double sigma3gap3 = sigma1gap1 * sigma1gap1 * sigma1gap1;
+    const double sigma6gap6 = sigma3gap3 * sigma3gap3;
+    return g->eps * (sigma6gap6 * sigma6gap6 - g->coef_at_cutoff);
+}
+
+static double exvfam_force(const orc_state* st, const orc_global* g, const double* pos,
+                           double* force, int need_force)
+{
+    double energy = 0;
+    for(int64_t q=0; q+1<g->np; ++q)
+    {
+        const int64_t i = g->idx[q];
+        for(int64_t m=g->lb[i]; m<g->le[i]; ++m)
+        {
+            const int64_t j = g->nbr[m];
+            const double sigma  = g->pp0[i] + g->pp0[j];
+            const double radius = g->kind == ORC_HARD_CORE_EXV ? g->pp1[i] + g->pp1[j] : 0.0;
+            double rij[3];
+            adjust_direction(st, pos + 3*i, pos + 3*j, rij);
+            const double l2 = length_sq(rij);
+            if(need_force)
+            {
+                const double rl = 1.0 / sqrt(l2);
+                const double l  = l2 * rl;
+                const double f_mag = exvfam_derivative(g, l, sigma, radius);
+                if(f_mag == 0.0) {continue;}
+                const double c = f_mag * rl;
+                for(int k=0; k<3; ++k)
+                {
+                    const double f = rij[k] * c;
+                    force[3*i+k] += f;
+                    force[3*j+k] -= f;
+                }
+                energy += exvfam_potential(g, l, sigma, radius);
+            }
+            else
+            {
+                energy += exvfam_potential(g, sqrt(l2), sigma, radius);
             }
         }
     }

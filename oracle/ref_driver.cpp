@@ -36,6 +36,8 @@
 #include <mjolnir/forcefield/global/DebyeHuckelPotential.hpp>
 #include <mjolnir/forcefield/global/LennardJonesPotential.hpp>
 #include <mjolnir/forcefield/global/WCAPotential.hpp>
+#include <mjolnir/forcefield/global/InversePowerPotential.hpp>
+#include <mjolnir/forcefield/global/HardCoreExcludedVolumePotential.hpp>
 #include <mjolnir/forcefield/global/LennardJonesAttractivePotential.hpp>
 #include <mjolnir/forcefield/global/UniformLennardJonesPotential.hpp>
 #include <mjolnir/forcefield/local/BondLengthInteraction.hpp>
@@ -118,7 +120,10 @@ struct RefSim final : public RefSimBase
     using wca_pot = WCAPotential<double>;
     using lja_pot = LennardJonesAttractivePotential<double>;
     using ulj_pot = UniformLennardJonesPotential<double>;
+    using ipw_pot = InversePowerPotential<double>;
+    using hcx_pot = HardCoreExcludedVolumePotential<double>;
     int lj_kind = ORC_LJ;
+    int exv_kind = ORC_EXV;
 
     std::unique_ptr<system_type>  sys;
     std::unique_ptr<ff_base_type> ff;
@@ -244,7 +249,41 @@ struct RefSim final : public RefSimBase
                                s.ignore_molecule == ORC_IGNORE_OTHERS ? "Others" :
                                                                         "Nothing";
         GlobalForceField<traitsT> global;
-        if(s.exv_on)
+        exv_kind = s.exv_kind;
+        if(s.exv_on && s.exv_kind == ORC_INVERSE_POWER)
+        {
+            using plist = InversePowerParameterList<traitsT>;
+            std::vector<std::pair<std::size_t, typename plist::parameter_type>> ps;
+            for(long long k=0; k<s.exv_n; ++k)
+            {
+                ps.emplace_back(std::size_t(s.exv_idx[k]), typename plist::parameter_type{s.exv_radius[k]});
+            }
+            auto p = make_unique<GlobalPairInteraction<traitsT, ipw_pot>>(
+                ipw_pot(s.exv_cutoff, s.exv_power, s.exv_eps),
+                ParameterList<traitsT, ipw_pot>(make_unique<plist>(ps, within, IgnoreMolecule<std::size_t>(mol_rule),
+                    IgnoreGroup<std::string>(std::map<std::string, std::vector<std::string>>{}))),
+                make_partition<ipw_pot>(s.exv_margin, is_periodic{}));
+            globals[0] = p.get();
+            global.emplace(std::move(p));
+        }
+        else if(s.exv_on && s.exv_kind == ORC_HARD_CORE_EXV)
+        {
+            using plist = HardCoreExcludedVolumeParameterList<traitsT>;
+            std::vector<std::pair<std::size_t, typename plist::parameter_type>> ps;
+            for(long long k=0; k<s.exv_n; ++k)
+            {
+                ps.emplace_back(std::size_t(s.exv_idx[k]),
+                                typename plist::parameter_type{s.exv_radius[k], s.exv_core[k]});
+            }
+            auto p = make_unique<GlobalPairInteraction<traitsT, hcx_pot>>(
+                hcx_pot(s.exv_cutoff, s.exv_eps),
+                ParameterList<traitsT, hcx_pot>(make_unique<plist>(ps, within, IgnoreMolecule<std::size_t>(mol_rule),
+                    IgnoreGroup<std::string>(std::map<std::string, std::vector<std::string>>{}))),
+                make_partition<hcx_pot>(s.exv_margin, is_periodic{}));
+            globals[0] = p.get();
+            global.emplace(std::move(p));
+        }
+        else if(s.exv_on)
         {
             using plist = ExcludedVolumeParameterList<traitsT>;
             std::vector<std::pair<std::size_t, typename plist::parameter_type>> ps;
@@ -448,7 +487,12 @@ struct RefSim final : public RefSimBase
         const int g = term - ORC_TERM_EXV;
         if(g < 0 || g > 2 || !globals[g]) {return -1;}
         std::integral_constant<bool, Sequential> seq;
-        if(g == 0) {return dump<exv_pot>(globals[0], leading[0], pairs, cap, seq);}
+        if(g == 0)
+        {
+            if(exv_kind == ORC_INVERSE_POWER) {return dump<ipw_pot>(globals[0], leading[0], pairs, cap, seq);}
+            if(exv_kind == ORC_HARD_CORE_EXV) {return dump<hcx_pot>(globals[0], leading[0], pairs, cap, seq);}
+            return dump<exv_pot>(globals[0], leading[0], pairs, cap, seq);
+        }
         if(g == 1) {return dump<dh_pot >(globals[1], leading[1], pairs, cap, seq);}
         if(lj_kind == ORC_WCA)           {return dump<wca_pot>(globals[2], leading[2], pairs, cap, seq);}
         if(lj_kind == ORC_LJ_ATTRACTIVE) {return dump<lja_pot>(globals[2], leading[2], pairs, cap, seq);}

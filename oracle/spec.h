@@ -21,6 +21,8 @@ extern "C" {
 enum { ORC_UNLIMITED = 0, ORC_PERIODIC = 1 };
 enum { ORC_BAOAB = 0, ORC_VV = 1 };
 enum { ORC_IGNORE_NOTHING = 0, ORC_IGNORE_SELF = 1, ORC_IGNORE_OTHERS = 2 };
+/* potential of the first global term (ExcludedVolume family) */
+enum { ORC_EXV = 0, ORC_INVERSE_POWER = 1, ORC_HARD_CORE_EXV = 2 };
 /* potential of the third global term (Lennard-Jones family) */
 enum { ORC_LJ = 0, ORC_WCA = 1, ORC_LJ_ATTRACTIVE = 2, ORC_LJ_UNIFORM = 3 };
 enum { ORC_TERM_BOND = 0, ORC_TERM_ANGLE = 1, ORC_TERM_DIHEDRAL = 2,
@@ -46,6 +48,9 @@ typedef struct orc_spec
 
     int32_t exv_on;  double exv_eps, exv_cutoff, exv_margin;
     int64_t exv_n;   const int64_t* exv_idx; const double* exv_radius;
+    int32_t exv_kind;            /* ORC_EXV / ORC_INVERSE_POWER / ORC_HARD_CORE_EXV */
+    int32_t exv_power;           /* InversePower n                          */
+    const double* exv_core;      /* HardCoreExcludedVolume core_radius (exv_radius: soft_shell_thickness) */
 
     int32_t dh_on;   double dh_cutoff, dh_margin;
     int64_t dh_n;    const int64_t* dh_idx;  const double* dh_charge;

@@ -258,3 +258,32 @@ spatial_partition = {type = "CellList", margin = 0.3}
     d = I.load(_write(tmp_path, "u.toml", text)).desc
     np.testing.assert_array_equal(d.lj.idx, np.arange(4))
     assert set(d.lj.param0) == {1.5} and set(d.lj.param1) == {0.4} and d.lj.cutoff == 2.5
+
+
+@pytest.mark.parametrize("case", ["InversePower12", "InversePower6", "HardCoreExcludedVolume"])
+def test_exv_family_round_trip(case, tmp_path):
+    from exv_family import system
+    d = system(case)
+    path = str(tmp_path / "f.toml")
+    I.dump(d, path)
+    g = I.load(path).desc
+    assert g.exv.kind == d.exv.kind and g.exv.cutoff == d.exv.cutoff and g.exv.epsilon == d.exv.epsilon
+    assert g.exv.exponent == d.exv.exponent
+    np.testing.assert_array_equal(g.exv.param0, d.exv.param0)
+    if d.exv.param1 is not None:
+        np.testing.assert_array_equal(g.exv.param1, d.exv.param1)
+
+
+def test_inverse_power_default_cutoff_uses_integer_quotient(tmp_path):
+    text = HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF
+    start = text.index("[[forcefields.global]]")
+    text = text[:start] + """[[forcefields.global]]
+interaction = "Pair"
+potential   = "InversePower"
+epsilon = 0.5
+n = 5
+spatial_partition = {type = "CellList", margin = 0.3}
+parameters = [{index = 0, radius = 1.0}, {index = 1, radius = 1.0}]
+"""
+    d = I.load(_write(tmp_path, "ip.toml", text)).desc
+    assert d.exv.kind == "InversePower" and d.exv.exponent == 5 and d.exv.cutoff == 4.0   # 2^(12 // 5)
