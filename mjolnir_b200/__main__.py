@@ -4,9 +4,12 @@
 
 Reads the file with :func:`mjolnir_b200.input.load`, advances the system
 ``total_step`` steps and, every ``save_step`` steps (and at step 0), appends
-the per-term energies and the kinetic energy to ``<path>/<prefix>.ene`` and a
-frame of positions to ``<path>/<prefix>.xyz`` (the quantities the reference's
-EnergyObserver and XYZObserver write; core/EnergyObserver.hpp:89-153).
+the per-term energies, the kinetic energy and the attributes to
+``<path>/<prefix>.ene``, and frames of positions and velocities to
+``<path>/<prefix>_position.xyz`` and ``_velocity.xyz``, in the layout of the reference's
+EnergyObserver and XYZObserver (core/EnergyObserver.hpp:63-153,
+core/XYZObserver.hpp:46-76; interactions in the order bonds, angles,
+dihedrals, then the global terms).
 ``precision = "double"`` in the input selects the FP64 form unless
 ``--precision`` says otherwise.  A ``SimulatedAnnealing`` input follows its
 linear temperature schedule (:mod:`mjolnir_b200.anneal`).
@@ -24,23 +27,36 @@ from .anneal import current
 from .engine import Engine
 from .input import load
 
-TERM_LABEL = {"bond": "BondLength:Harmonic", "angle": "BondAngle:Harmonic",
-              "dihedral": "DihedralAngle:Cosine", "exv": "ExcludedVolume",
-              "dh": "DebyeHuckel", "lj": "LennardJones"}
+# interaction names as the reference's name() returns them (the energy file's
+# column titles): forcefield/local/*Interaction.hpp, GlobalPair*Interaction.hpp
+PAIR_NAME = {"ExcludedVolume": "GlobalPairExcludedVolume", "LennardJones": "GlobalPairLennardJones",
+             "DebyeHuckel": "Pair:DebyeHuckel", "WCA": "Pair:WCA",
+             "LennardJonesAttractive": "Pair:LennardJonesAttractive",
+             "UniformLennardJones": "Pair:LennardJones", "InversePower": "Pair:InversePower",
+             "HardCoreExcludedVolume": "Pair:HardCoreExcludedVolume"}
 
 
 def _present(desc):
+    """(term key, column title) of every interaction, local then global."""
     out = []
     if desc.bonds is not None:
-        out.append("bond")
+        out.append(("bond", "BondLength:Harmonic"))
     if desc.angles is not None:
-        out.append("angle")
+        out.append(("angle", "BondAngle:Harmonic"))
     if desc.dihedrals is not None:
-        out.append("dihedral")
+        out.append(("dihedral", "DihedralAngle:Cosine"))
     for key in ("exv", "dh", "lj"):
-        if getattr(desc, key) is not None:
-            out.append(key)
+        t = getattr(desc, key)
+        if t is not None:
+            out.append((key, PAIR_NAME[t.kind]))
     return out
+
+
+def _frame(f, names, arr, step):
+    """One frame of core/XYZObserver.hpp:46-76: count, "step = N", then
+    "name x y z" with eight decimals."""
+    f.write(f"{arr.shape[0]}\nstep = {step}\n")
+    f.write("".join(f"{nm} {x:.8f} {y:.8f} {z:.8f}\n" for nm, (x, y, z) in zip(names, arr)))
 
 
 def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) -> dict:
@@ -51,25 +67,35 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
     save = max(1, inp.save_step)
     os.makedirs(inp.output_path, exist_ok=True)
     ene_path = os.path.join(inp.output_path, inp.output_prefix + ".ene")
-    xyz_path = os.path.join(inp.output_path, inp.output_prefix + ".xyz")
+    xyz_path = os.path.join(inp.output_path, inp.output_prefix + "_position.xyz")
+    vel_path = os.path.join(inp.output_path, inp.output_prefix + "_velocity.xyz")
     terms = _present(d)
+    widths = [max(len(title), 10) for _, title in terms]       # LocalForceField.hpp:57
+    names = ["X"] * d.n
     eng = Engine(prec, device=device)
     sid = eng.add_system(d)
     eng.commit()
     t0 = time.perf_counter()
     anneal = inp.schedule                    # SimulatedAnnealing: (first, last, each_step)
     r_total = 1.0 / total if total else 0.0
-    with open(ene_path, "w") as ene, open(xyz_path, "w") as xyz:
-        ene.write("# timestep " + " ".join(TERM_LABEL[t] for t in terms) + " kinetic_energy\n")
+    temperature = d.temperature
+    with open(ene_path, "w") as ene, open(xyz_path, "w") as xyz, open(vel_path, "w") as vel:
+        # core/EnergyObserver.hpp:63-87 (header), :89-153 (rows)
+        attrs = sorted({"temperature": 0.0, "ionic_strength": 0.0})
+        ene.write("# timestep  " + "".join(title + " " for _, title in terms) + " kinetic_energy" +
+                  "".join(f" attribute:{a}" for a in attrs) + "\n")
         done = 0
         while True:
             if done % save == 0 or done >= total:
                 e = eng.energies(sid)
                 p, v, _ = eng.state(sid)
-                kin = 0.5 * float(np.sum(d.mass[:, None] * v * v))
-                ene.write(f"{done} " + " ".join(f"{e[t]:.10e}" for t in terms) + f" {kin:.10e}\n")
-                xyz.write(f"{d.n}\nstep = {done}\n")
-                xyz.write("".join(f"X {x:.6f} {y:.6f} {z:.6f}\n" for x, y, z in p))
+                kin = 0.5 * float(np.sum(np.sum(v * v, axis=1) * d.mass))
+                values = {"temperature": temperature, "ionic_strength": d.ionic_strength}
+                ene.write(f"{str(done):<11} " +
+                          "".join(f"{e[key]:>{w}.6f} " for (key, _), w in zip(terms, widths)) +
+                          f"{kin:>14.6f}" + "".join(f" {values[a]:>{10 + len(a)}.6f}" for a in attrs) + "\n")
+                _frame(xyz, names, p, done)
+                _frame(vel, names, v, done)
             if done >= total:
                 break
             k = min(save - done % save, total - done)
@@ -78,11 +104,12 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
             eng.step(k)
             done += k
             if anneal and done % anneal[2] == 0:    # core/SimulatedAnnealingSimulator.hpp:144-154
-                eng.set_temperature(sid, current(anneal[0], anneal[1], done * r_total))
+                temperature = current(anneal[0], anneal[1], done * r_total)
+                eng.set_temperature(sid, temperature)
     wall = time.perf_counter() - t0
     eng.close()
     res = {"steps": total, "particles": d.n, "precision": prec, "wall_s": wall,
-           "energy_file": ene_path, "trajectory": xyz_path}
+           "energy_file": ene_path, "trajectory": xyz_path, "velocities": vel_path}
     print(res, file=out)
     return res
 

@@ -18,9 +18,14 @@ def test_toml_run_matches_direct(tmp_path):
     text = open(path).read().replace('output.path = "./"', f'output.path = "{tmp_path}/"')
     open(path, "w").write(text)
     res = run(path, precision="mixed")
+    head = open(res["energy_file"]).readline()
+    assert head.split() == ["#", "timestep", "BondLength:Harmonic", "BondAngle:Harmonic",
+                            "DihedralAngle:Cosine", "GlobalPairExcludedVolume", "Pair:DebyeHuckel",
+                            "kinetic_energy", "attribute:ionic_strength", "attribute:temperature"]
     ene = np.loadtxt(res["energy_file"])
-    assert ene.shape == (3, 7)                       # steps 0, 20, 40; 5 terms + kinetic
+    assert ene.shape == (3, 9)                       # steps 0, 20, 40; 5 terms, kinetic, 2 attributes
     assert list(ene[:, 0]) == [0, 20, 40]
+    assert ene[0, 8] == d.temperature and ene[0, 7] > 0
     e = Engine("mixed")
     sid = e.add_system(d)
     e.commit()
@@ -28,10 +33,12 @@ def test_toml_run_matches_direct(tmp_path):
     en = e.energies(sid)
     row = ene[-1]
     for k, t in enumerate(("bond", "angle", "dihedral", "exv", "dh")):
-        assert row[1 + k] == pytest.approx(en[t], rel=1e-9, abs=1e-9)
+        assert row[1 + k] == pytest.approx(en[t], rel=1e-6, abs=1e-6)    # six decimals
     p, v, _ = e.state(sid)
     kin = 0.5 * float(np.sum(d.mass[:, None] * v * v))
-    assert row[6] == pytest.approx(kin, rel=1e-9)
+    assert row[6] == pytest.approx(kin, rel=1e-6, abs=1e-6)
+    xyz = open(res["trajectory"]).read().split("\n")
+    assert xyz[0] == str(d.n) and xyz[1] == "step = 0" and xyz[2].startswith("X ")
     e.close()
 
 
