@@ -9,7 +9,9 @@ the per-term energies, the kinetic energy and the attributes to
 ``<path>/<prefix>_position.xyz`` and ``_velocity.xyz``, in the layout of the reference's
 EnergyObserver and XYZObserver (core/EnergyObserver.hpp:63-153,
 core/XYZObserver.hpp:46-76; interactions in the order bonds, angles,
-dihedrals, then the global terms).
+dihedrals, then the global terms).  Every ``checkpoint_step`` steps and at the
+end it writes ``<prefix>_system.msg`` and ``<prefix>_rng.msg``
+(:mod:`mjolnir_b200.checkpoint`).
 ``precision = "double"`` in the input selects the FP64 form unless
 ``--precision`` says otherwise.  A ``SimulatedAnnealing`` input follows its
 linear temperature schedule (:mod:`mjolnir_b200.anneal`).
@@ -23,6 +25,7 @@ import time
 
 import numpy as np
 
+from . import checkpoint
 from .anneal import current
 from .engine import Engine
 from .input import load
@@ -71,6 +74,8 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
     vel_path = os.path.join(inp.output_path, inp.output_prefix + "_velocity.xyz")
     terms = _present(d)
     widths = [max(len(title), 10) for _, title in terms]       # LocalForceField.hpp:57
+    ckpt = max(1, inp.checkpoint_step or save)
+    ck_prefix = os.path.join(inp.output_path, inp.output_prefix)
     names = ["X"] * d.n
     eng = Engine(prec, device=device)
     sid = eng.add_system(d)
@@ -86,6 +91,8 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
                   "".join(f" attribute:{a}" for a in attrs) + "\n")
         done = 0
         while True:
+            if done > 0 and (done % ckpt == 0 or done >= total):   # MsgPackSaver at checkpoint_step and at the end
+                checkpoint.save(eng, sid, d, ck_prefix)
             if done % save == 0 or done >= total:
                 e = eng.energies(sid)
                 p, v, _ = eng.state(sid)
@@ -98,7 +105,7 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
                 _frame(vel, names, v, done)
             if done >= total:
                 break
-            k = min(save - done % save, total - done)
+            k = min(save - done % save, ckpt - done % ckpt, total - done)
             if anneal:
                 k = min(k, anneal[2] - done % anneal[2])
             eng.step(k)

@@ -85,6 +85,7 @@ class Input:
     output_format: str
     input_path: str
     schedule: Optional[tuple] = None   # SimulatedAnnealing: (first, last, each_step)
+    checkpoint_step: int = 0           # checkpoint interval (default: save_step)
 
 
 # ------------------------------------------------------------------ helpers
@@ -533,6 +534,7 @@ def load(path: str) -> Input:
         desc.dihedrals, desc.dihedral_topology = (idx, k, nn, v0), topo
     return Input(desc=desc, simulator=sim["type"], schedule=schedule, precision=prec, parallelism=par,
                  total_step=int(sim["total_step"]), save_step=int(sim["save_step"]), seed=seed,
+                 checkpoint_step=int(sim.get("checkpoint_step", sim["save_step"])),
                  output_prefix=str(out.get("prefix", "mjolnir")), output_path=str(out.get("path", "./")),
                  output_format=str(out.get("format", "xyz")), input_path=input_path)
 

@@ -39,6 +39,9 @@ def test_toml_run_matches_direct(tmp_path):
     assert row[6] == pytest.approx(kin, rel=1e-6, abs=1e-6)
     xyz = open(res["trajectory"]).read().split("\n")
     assert xyz[0] == str(d.n) and xyz[1] == "step = 0" and xyz[2].startswith("X ")
+    from mjolnir_b200 import checkpoint as K
+    ck = K.read_system(str(tmp_path / "melt_system.msg"))           # the last checkpoint: step 40
+    assert np.array_equal(ck["pos"], p) and K.read_rng(str(tmp_path / "melt_rng.msg"))[1] == 40
     e.close()
 
 
