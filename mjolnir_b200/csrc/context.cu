@@ -106,8 +106,9 @@ struct HostSystem {
     int64_t n = 0;
     int boundary = B_UNLIMITED;
     double lower[3] = {0, 0, 0}, upper[3] = {0, 0, 0};
-    std::vector<double> pos, vel, mass, force;
+    std::vector<double> pos, vel, mass, force, accel;
     bool force_valid = false;
+    bool accel_valid = false;    // UnderdampedLangevin acceleration carried over a commit
     double T = 300.0, I = 0.1;
     std::vector<std::pair<std::string, std::pair<int64_t, int64_t>>> connections;
     HostGlobal g[NGLOBAL];
@@ -166,7 +167,8 @@ struct mjg_context {
     std::vector<int> arena_ids;            // arena slot -> system id
     long long n_tot = 0;
     mjg::DevBuf d_sys, d_pos, d_vel, d_force, d_coef, d_psys, d_staging, d_mol;
-    mjg::DevBuf b_sys, b_pos, b_vel, b_force;   // rollback copies
+    mjg::DevBuf d_accel;                        // UnderdampedLangevin accelerations
+    mjg::DevBuf b_sys, b_pos, b_vel, b_force, b_accel;   // rollback copies
     mjg::DevBuf d_force_scratch;
     double* h_pinned = nullptr;             // page-locked host staging (state, forces)
     size_t h_pinned_bytes = 0;
@@ -197,6 +199,7 @@ int64_t device_bytes(const mjg_context* c)
     int64_t b = 0;
     const DevBuf* bufs[] = {&c->d_sys, &c->d_pos, &c->d_vel, &c->d_force, &c->d_coef, &c->d_psys,
                             &c->d_staging, &c->d_mol, &c->b_sys, &c->b_pos, &c->b_vel, &c->b_force,
+                            &c->d_accel, &c->b_accel,
                             &c->d_force_scratch, &c->l_bond_idx, &c->l_bond_k, &c->l_bond_v0,
                             &c->l_bond_sys, &c->l_angle_idx, &c->l_angle_k, &c->l_angle_v0,
                             &c->l_angle_sys, &c->l_dihd_idx, &c->l_dihd_k, &c->l_dihd_n,
@@ -471,7 +474,8 @@ void save_resident_state(mjg_context* c)
     const size_t per = 3 * (size_t)c->n_tot;
     double* h = pinned(c, sizeof(double) * per);
     double* st = c->d_staging.as<double>();
-    for(int field = 0; field < 3; ++field)
+    const int nfield = c->arena.accel ? 4 : 3;
+    for(int field = 0; field < nfield; ++field)
     {
         launch_pack_state(c->arena, st, field, 0, c->n_tot, c->stream);
         CK(cudaMemcpyAsync(h, st, sizeof(double) * per, cudaMemcpyDeviceToHost, c->stream));
@@ -479,9 +483,11 @@ void save_resident_state(mjg_context* c)
         parallel_for((int64_t)c->arena_ids.size(), [&](int64_t k) {
             HostSystem& s = c->sys[c->arena_ids[k]];
             if(!s.alive) {return;}
-            std::vector<double>& dst = field == 0 ? s.pos : field == 1 ? s.vel : s.force;
+            if(field == 3 && s.integrator != I_UNDERDAMPED) {return;}
+            std::vector<double>& dst = field == 0 ? s.pos : field == 1 ? s.vel : field == 2 ? s.force : s.accel;
             dst.assign(h + 3 * s.off, h + 3 * (s.off + s.n));
             if(field == 2) {s.force_valid = true;}
+            if(field == 3) {s.accel_valid = true;}
         });
     }
 }
@@ -742,7 +748,7 @@ void commit(mjg_context* c)
     {
         HostSystem& s = c->sys[i];
         if(!s.alive) {continue;}
-        if(s.integrator == I_BAOAB && (int64_t)s.gamma.size() != s.n)
+        if(s.integrator != I_VV && (int64_t)s.gamma.size() != s.n)
         {
             throw Error(MJG_ESTATE, "system " + std::to_string(i) + " has no integrator set");
         }
@@ -859,7 +865,12 @@ void commit(mjg_context* c)
             pos[gi] = make_double4(p[0], p[1], p[2], 0.0);
             vel[gi] = make_double4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], 0.0);
             const double rmass = 1.0 / s.mass[i];
-            if(s.integrator == I_BAOAB)        // reset_parameters (:73-99)
+            if(s.integrator == I_UNDERDAMPED)  // UnderdampedLangevinIntegrator::update (:55-70)
+            {
+                const double noise_coef = std::sqrt(2 * u.kB * s.T / s.dt);
+                coef[gi] = make_double4(rmass, s.gamma[i], noise_coef * std::sqrt(s.gamma[i] * rmass), s.dt);
+            }
+            else if(s.integrator == I_BAOAB)   // reset_parameters (:73-99)
             {
                 const double gamma_dt = -1 * s.gamma[i] * s.dt;
                 coef[gi] = make_double4(halfdt * rmass, std::exp(gamma_dt),
@@ -967,6 +978,10 @@ void commit(mjg_context* c)
     put(c->d_mol, c_mol);
     c->d_force.ensure(32 * (size_t)std::max<long long>(n_tot, 1));
     c->d_force_scratch.ensure(32 * (size_t)std::max<long long>(n_tot, 1));
+    bool any_underdamped = false;
+    for(int id : ids) {any_underdamped = any_underdamped || c->sys[id].integrator == I_UNDERDAMPED;}
+    if(any_underdamped) {c->d_accel.ensure(32 * (size_t)std::max<long long>(n_tot, 1));}
+    else                {c->d_accel.release();}
     c->d_staging.ensure(sizeof(double) * 3 * (size_t)std::max<long long>(n_tot, 1));
     if(c->rollback)
     {
@@ -974,10 +989,12 @@ void commit(mjg_context* c)
         c->b_pos.ensure(c->d_pos.bytes);
         c->b_vel.ensure(c->d_vel.bytes);
         c->b_force.ensure(c->d_force.bytes);
+        if(any_underdamped) {c->b_accel.ensure(c->d_accel.bytes);} else {c->b_accel.release();}
     }
     else
     {
         c->b_sys.release(); c->b_pos.release(); c->b_vel.release(); c->b_force.release();
+        c->b_accel.release();
     }
 
     Arena& a = c->arena;
@@ -993,6 +1010,7 @@ void commit(mjg_context* c)
     a.psys = c->d_psys.as<int>();
     a.staging = c->d_staging.as<double>();
     a.mol = c->d_mol.as<int>();
+    a.accel = any_underdamped ? c->d_accel.as<double4>() : nullptr;
 
     for(int g = 0; g < NGLOBAL; ++g)
     {
@@ -1175,6 +1193,27 @@ void commit(mjg_context* c)
             }
         }
     }
+    // UnderdampedLangevin: resident systems keep their accelerations, the
+    // others start from Integrator::initialize
+    if(any_underdamped)
+    {
+        double* stg = c->d_staging.as<double>();
+        for(int k = 0; k < nsys; ++k)
+        {
+            HostSystem& s = c->sys[ids[k]];
+            if(s.integrator != I_UNDERDAMPED) {continue;}
+            if(s.accel_valid && (int64_t)s.accel.size() == 3 * s.n)
+            {
+                CK(cudaMemcpyAsync(stg + 3 * s.off, s.accel.data(), sizeof(double) * 3 * s.n,
+                                   cudaMemcpyHostToDevice, st));
+                launch_set_accel(c->arena, stg + 3 * s.off, s.off, s.n, st);
+            }
+            else
+            {
+                launch_init_accel(c->arena, s.off, s.n, st);
+            }
+        }
+    }
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
     tm.mark("forces");
@@ -1217,6 +1256,10 @@ void run_steps(mjg_context* c, int64_t nsteps)
             CK(cudaMemcpyAsync(c->b_pos.p, c->d_pos.p, c->d_pos.bytes, cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(c->b_vel.p, c->d_vel.p, c->d_vel.bytes, cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(c->b_force.p, c->d_force.p, c->d_force.bytes, cudaMemcpyDeviceToDevice, st));
+            if(c->d_accel.bytes)
+            {
+                CK(cudaMemcpyAsync(c->b_accel.p, c->d_accel.p, c->d_accel.bytes, cudaMemcpyDeviceToDevice, st));
+            }
         }
         // step 1 of the chunk, then steps 2..n with the previous closing
         // half-kick fused into their first pass, then the last closing kick
@@ -1244,6 +1287,10 @@ void run_steps(mjg_context* c, int64_t nsteps)
         CK(cudaMemcpyAsync(c->d_pos.p, c->b_pos.p, c->d_pos.bytes, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(c->d_vel.p, c->b_vel.p, c->d_vel.bytes, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(c->d_force.p, c->b_force.p, c->d_force.bytes, cudaMemcpyDeviceToDevice, st));
+        if(c->d_accel.bytes)
+        {
+            CK(cudaMemcpyAsync(c->d_accel.p, c->b_accel.p, c->d_accel.bytes, cudaMemcpyDeviceToDevice, st));
+        }
         for(int g = 0; g < NGLOBAL; ++g)
         {
             TermDev& T = c->term[g];
@@ -1382,14 +1429,21 @@ int mjg_system_set_temperature(mjg_context* c, int sys, double T)
     HostSystem& s = get_sys(c, sys);
     if(!(T > 0)) {throw Error(MJG_EINVAL, "temperature must be positive");}
     s.T = T;
-    if(!c->committed || !s.resident || s.integrator != I_BAOAB) {return MJG_OK;}
-    // BAOABLangevinIntegrator::update -> reset_parameters (:47-58, :73-99): the
-    // noise coefficients of the system's particles, computed as at commit
+    if(!c->committed || !s.resident || s.integrator == I_VV) {return MJG_OK;}
+    // BAOABLangevinIntegrator::update -> reset_parameters (:47-58, :73-99) or
+    // UnderdampedLangevinIntegrator::update (:55-70): the noise coefficients of
+    // the system's particles, computed as at commit
     const Units u;
     const double kBT = u.kB * s.T;
     std::vector<double> z((size_t)s.n);
     for(int64_t i = 0; i < s.n; ++i)
     {
+        if(s.integrator == I_UNDERDAMPED)
+        {
+            const double rmass = 1.0 / s.mass[i];
+            z[i] = std::sqrt(2 * u.kB * s.T / s.dt) * std::sqrt(s.gamma[i] * rmass);
+            continue;
+        }
         const double gamma_dt = -1 * s.gamma[i] * s.dt;
         z[i] = std::sqrt(kBT * (1 - std::exp(2 * gamma_dt)) * (1.0 / s.mass[i]));
     }
@@ -1654,10 +1708,13 @@ int mjg_integrator_set(mjg_context* c, int sys, int kind, double dt, const doubl
     ABI_BEGIN(c)
     HostSystem& s = get_sys(c, sys);
     if(s.resident) {throw Error(MJG_ESTATE, "the integrator is fixed once committed");}
-    if(kind != MJG_BAOAB && kind != MJG_VELOCITY_VERLET) {throw Error(MJG_EINVAL, "unknown integrator");}
+    if(kind != MJG_BAOAB && kind != MJG_VELOCITY_VERLET && kind != MJG_UNDERDAMPED_LANGEVIN)
+    {
+        throw Error(MJG_EINVAL, "unknown integrator");
+    }
     if(!(dt > 0)) {throw Error(MJG_EINVAL, "dt must be positive");}
-    if(kind == MJG_BAOAB && !gamma) {throw Error(MJG_EINVAL, "BAOAB needs gammas");}
-    s.integrator = kind == MJG_BAOAB ? I_BAOAB : I_VV;
+    if(kind != MJG_VELOCITY_VERLET && !gamma) {throw Error(MJG_EINVAL, "Langevin integrators need gammas");}
+    s.integrator = kind == MJG_BAOAB ? I_BAOAB : kind == MJG_VELOCITY_VERLET ? I_VV : I_UNDERDAMPED;
     s.dt = dt;
     s.gamma = gamma ? std::vector<double>(gamma, gamma + s.n) : std::vector<double>(s.n, 0.0);
     s.seed = seed;
@@ -1753,6 +1810,7 @@ int mjg_set_state(mjg_context* c, int sys, const double* pos, const double* vel)
         rebuild_all(c);
         // forces at the new positions (the integrator's next B step uses them)
         compute_initial_forces(c);
+        launch_init_accel(c->arena, s.off, s.n, c->stream);   // Integrator::initialize for this system
         CK(cudaStreamSynchronize(c->stream));
     }
     ABI_END(c)
@@ -1795,6 +1853,7 @@ int mjg_set_state_all(mjg_context* c, const double* pos, const double* vel)
         launch_unpack_state(c->arena, stg, nullptr, 0, c->n_tot, c->stream);
         rebuild_all(c);
         compute_initial_forces(c);
+        launch_init_accel(c->arena, 0, c->n_tot, c->stream);   // new positions: Integrator::initialize
     }
     CK(cudaStreamSynchronize(c->stream));
     ABI_END(c)

@@ -36,10 +36,30 @@ __device__ __forceinline__ void zero_force(void* force, long long i)
     else               {static_cast<longlong4*>(force)[i] = make_longlong4(0, 0, 0, 0);}
 }
 
-// B-A-O-A of BAOAB (or the first half-kick and drift of velocity Verlet),
-// force reset and the per-system largest squared displacement.  With KICK the
-// previous step's closing half-kick v += (halfdt/m) f is applied first, as a
-// separate rounding step, so that consecutive steps of a chunk share one pass.
+// The closing half of an UnderdampedLangevin step
+// (core/UnderdampedLangevinIntegrator.hpp:252-264): a = f/m + sigma R with the
+// noise of counter `ctr`, v += halfdt (1 - gamma halfdt) a.
+__device__ __forceinline__ void underdamped_close(const SysDev& S, long long i, double4& v, double4& acc,
+                                                  const double4& c, double fx, double fy, double fz,
+                                                  unsigned long long ctr)
+{
+    double r0, r1, r2;
+    gaussian3(S.seed, (unsigned long long)(i - S.off), ctr, r0, r1, r2);
+    acc.x = __dadd_rn(__dmul_rn(fx, c.x), __dmul_rn(r0, c.z));
+    acc.y = __dadd_rn(__dmul_rn(fy, c.x), __dmul_rn(r1, c.z));
+    acc.z = __dadd_rn(__dmul_rn(fz, c.x), __dmul_rn(r2, c.z));
+    const double halfdt = c.w / 2;
+    const double k = __dmul_rn(halfdt, __dsub_rn(1.0, __dmul_rn(c.y, halfdt)));
+    v.x = __dadd_rn(v.x, __dmul_rn(k, acc.x));
+    v.y = __dadd_rn(v.y, __dmul_rn(k, acc.y));
+    v.z = __dadd_rn(v.z, __dmul_rn(k, acc.z));
+}
+
+// B-A-O-A of BAOAB (or the first half-kick and drift of velocity Verlet, or
+// the first half of an UnderdampedLangevin step), force reset and the
+// per-system largest squared displacement.  With KICK the previous step's
+// closing half is applied first, as separate rounding steps, so that
+// consecutive steps of a chunk share one pass.
 template<int PREC, bool KICK>
 __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
 {
@@ -55,14 +75,35 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
         const double4 c = a.coef[i];     // {halfdt*rmass, exp(-gamma dt), noise, halfdt | dt}
         double fx, fy, fz;
         load_force<PREC>(a.force, i, fx, fy, fz);
-        if(KICK)
+        const bool uld = S.integrator == I_UNDERDAMPED;
+        if(KICK && !uld)
         {
             v.x = __dadd_rn(v.x, __dmul_rn(c.x, fx));
             v.y = __dadd_rn(v.y, __dmul_rn(c.x, fy));
             v.z = __dadd_rn(v.z, __dmul_rn(c.x, fz));
         }
         double dx, dy, dz;
-        if(S.integrator == I_BAOAB)
+        if(uld)             // core/UnderdampedLangevinIntegrator.hpp:198-221
+        {
+            double4 acc = a.accel[i];
+            if(KICK) {underdamped_close(S, i, v, acc, c, fx, fy, fz, S.step); a.accel[i] = acc;}
+            const double dt = c.w, halfdt = dt / 2, halfdt2 = dt * dt / 2;
+            const double gdo2 = __dmul_rn(c.y, halfdt);                 // gamma dt / 2
+            const double omg  = __dsub_rn(1.0, gdo2);
+            const double cv   = __dmul_rn(dt, omg);
+            dx = __dadd_rn(__dmul_rn(cv, v.x), __dmul_rn(halfdt2, acc.x));
+            dy = __dadd_rn(__dmul_rn(cv, v.y), __dmul_rn(halfdt2, acc.y));
+            dz = __dadd_rn(__dmul_rn(cv, v.z), __dmul_rn(halfdt2, acc.z));
+            const double sv = __dmul_rn(omg, __dadd_rn(__dmul_rn(omg, omg), gdo2));
+            v.x = __dmul_rn(v.x, sv);
+            v.y = __dmul_rn(v.y, sv);
+            v.z = __dmul_rn(v.z, sv);
+            const double sa = __dmul_rn(halfdt, omg);
+            v.x = __dadd_rn(v.x, __dmul_rn(sa, acc.x));
+            v.y = __dadd_rn(v.y, __dmul_rn(sa, acc.y));
+            v.z = __dadd_rn(v.z, __dmul_rn(sa, acc.z));
+        }
+        else if(S.integrator == I_BAOAB)
         {
             double r0, r1, r2;
             gaussian3(S.seed, (unsigned long long)(i - S.off), S.step, r0, r1, r2);
@@ -165,20 +206,52 @@ __global__ void k_margin(Arena a, int* any0, int* any1, int* any2)
     }
 }
 
-// final half-kick v += (halfdt/m) f of both integrators
+// closing half of the last step of a chunk: v += (halfdt/m) f (BAOAB,
+// velocity Verlet) or the UnderdampedLangevin closing
 template<int PREC>
 __global__ void __launch_bounds__(TPB) k_integrate_last(Arena a)
 {
     const long long i = (long long)blockIdx.x * TPB + threadIdx.x;
-    if(i >= a.n || a.sys[a.psys[i]].frozen) {return;}
-    const double c = a.coef[i].x;
+    if(i >= a.n) {return;}
+    const SysDev& S = a.sys[a.psys[i]];
+    if(S.frozen) {return;}
     double fx, fy, fz;
     load_force<PREC>(a.force, i, fx, fy, fz);
     double4 v = a.vel[i];
+    if(S.integrator == I_UNDERDAMPED)
+    {
+        double4 acc = a.accel[i];
+        underdamped_close(S, i, v, acc, a.coef[i], fx, fy, fz, S.step);
+        a.accel[i] = acc;
+        a.vel[i] = v;
+        return;
+    }
+    const double c = a.coef[i].x;
     v.x = __dadd_rn(v.x, __dmul_rn(c, fx));
     v.y = __dadd_rn(v.y, __dmul_rn(c, fy));
     v.z = __dadd_rn(v.z, __dmul_rn(c, fz));
     a.vel[i] = v;
+}
+
+// UnderdampedLangevinIntegrator::initialize (:160-181): a = f/m + sigma R,
+// with the noise counter at the system's current step (a resumed system gets
+// the acceleration the uninterrupted run had)
+template<int PREC>
+__global__ void k_init_accel(Arena a, long long first, long long count)
+{
+    const long long k = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(k >= count) {return;}
+    const long long i = first + k;
+    const SysDev& S = a.sys[a.psys[i]];
+    if(S.integrator != I_UNDERDAMPED) {return;}
+    double fx, fy, fz;
+    load_force<PREC>(a.force, i, fx, fy, fz);
+    const double4 c = a.coef[i];
+    double r0, r1, r2;
+    gaussian3(S.seed, (unsigned long long)(i - S.off), S.step, r0, r1, r2);
+    a.accel[i] = make_double4(__dadd_rn(__dmul_rn(fx, c.x), __dmul_rn(r0, c.z)),
+                              __dadd_rn(__dmul_rn(fy, c.x), __dmul_rn(r1, c.z)),
+                              __dadd_rn(__dmul_rn(fz, c.x), __dmul_rn(r2, c.z)), 0.0);
 }
 
 template<int PREC>
@@ -206,6 +279,7 @@ __global__ void k_pack(Arena a, double* dst, int what, long long first, long lon
     double x, y, z;
     if(what == 0)      {const double4 p = a.pos[i]; x = p.x; y = p.y; z = p.z;}
     else if(what == 1) {const double4 v = a.vel[i]; x = v.x; y = v.y; z = v.z;}
+    else if(what == 3) {const double4 q = a.accel ? a.accel[i] : make_double4(0, 0, 0, 0); x = q.x; y = q.y; z = q.z;}
     else               {load_force<PREC>(a.force, i, x, y, z);}
     dst[3*k] = x; dst[3*k+1] = y; dst[3*k+2] = z;
 }
@@ -266,6 +340,27 @@ void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s)
     k_margin<<<(a.nsys + 127) / 128, 128, 0, s>>>(a,
         t[0].on ? t[0].any_rebuild : nullptr, t[1].on ? t[1].any_rebuild : nullptr,
         t[2].on ? t[2].any_rebuild : nullptr);
+    note_launches(1);
+}
+
+__global__ void k_set_accel(Arena a, const double* src, long long first, long long count)
+{
+    const long long k = (long long)blockIdx.x * TPB + threadIdx.x;
+    if(k < count) {a.accel[first + k] = make_double4(src[3 * k], src[3 * k + 1], src[3 * k + 2], 0.0);}
+}
+
+void launch_set_accel(const Arena& a, const double* src, long long first, long long count, cudaStream_t s)
+{
+    if(count == 0 || !a.accel) {return;}
+    k_set_accel<<<blocks(count), TPB, 0, s>>>(a, src, first, count);
+    note_launches(1);
+}
+
+void launch_init_accel(const Arena& a, long long first, long long count, cudaStream_t s)
+{
+    if(count == 0 || !a.accel) {return;}
+    if(a.precision == P_FP64) {k_init_accel<P_FP64><<<blocks(count), TPB, 0, s>>>(a, first, count);}
+    else                      {k_init_accel<P_MIXED><<<blocks(count), TPB, 0, s>>>(a, first, count);}
     note_launches(1);
 }
 

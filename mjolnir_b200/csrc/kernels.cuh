@@ -14,7 +14,9 @@ struct Arena {
     double4*  pos;
     double4*  vel;
     void*     force;            // double4 (P_FP64) or longlong4 (P_MIXED)
-    double4*  coef;
+    double4*  coef;             // BAOAB {halfdt/m, e^-g dt, noise, halfdt}; VV {halfdt/m, 1, 0, dt};
+                                // UnderdampedLangevin {1/m, gamma, noise sigma, dt}
+    double4*  accel;            // UnderdampedLangevin: acceleration with noise (nullptr: none)
     int*      psys;
     double*   staging;          // [3 n] host-layout staging for copies
     // exclusions (per global term): excluded partners of every particle,
@@ -75,6 +77,11 @@ void launch_pack_state(const Arena& a, double* dst, int what, long long first, l
 
 // kick: apply the previous step's closing half-kick in the same pass
 void launch_integrate_first(const Arena& a, cudaStream_t s, bool kick = false);
+// UnderdampedLangevin: acceleration from the current forces and noise for the
+// particles [first, first + count) (Integrator::initialize)
+void launch_init_accel(const Arena& a, long long first, long long count, cudaStream_t s);
+// accel[first + k] = src[3k .. 3k + 2] (host-layout staging)
+void launch_set_accel(const Arena& a, const double* src, long long first, long long count, cudaStream_t s);
 void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s);
 void launch_integrate_last(const Arena& a, cudaStream_t s);
 void launch_zero_force(const Arena& a, cudaStream_t s);

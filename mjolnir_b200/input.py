@@ -16,8 +16,9 @@ ready for :meth:`Engine.add_system`:
   (``schedule = {type = "linear", begin, end}``, ``each_step``), ``boundary_type``,
   ``precision``, ``parallelism``, ``seed`` (or the deprecated
   ``integrator.seed``), ``delta_t``, ``total_step``, ``save_step``,
-  ``integrator.type`` = ``"BAOABLangevin"`` (``gammas`` or the deprecated
-  ``parameters``, input/read_integrator.hpp:120-187) or ``"VelocityVerlet"``;
+  ``integrator.type`` = ``"BAOABLangevin"`` or ``"UnderdampedLangevin"``
+  (``gammas`` or the deprecated ``parameters``, input/read_integrator.hpp:55-187)
+  or ``"VelocityVerlet"``;
 * ``[[systems]]`` (the first): ``attributes``, ``boundary_shape``,
   ``particles`` with ``mass|m``, ``position|pos``, ``velocity|vel``, ``name``,
   ``group`` (input/read_system.hpp:93-290), or ``file_name = "x.msg"``, a
@@ -233,8 +234,9 @@ def _integrator(integ, n):
     if kind == "VelocityVerlet":
         _check_keys(integ, {"type", "seed", "remove"}, "[simulator.integrator]")
         return "VelocityVerlet", np.zeros(n)
-    if kind != "BAOABLangevin":
-        raise InputError(f'integrator type "{kind}": only "BAOABLangevin" and "VelocityVerlet" are supported')
+    if kind not in ("BAOABLangevin", "UnderdampedLangevin"):
+        raise InputError(f'integrator type "{kind}": only "BAOABLangevin", "UnderdampedLangevin" and '
+                         '"VelocityVerlet" are supported')
     _check_keys(integ, {"type", "seed", "remove", "env", "parameters", "gammas"}, "[simulator.integrator]")
     if "parameters" in integ and "gammas" in integ:
         raise InputError('duplicated keys: both "parameters" and "gammas" are provided')
@@ -249,7 +251,7 @@ def _integrator(integ, n):
         gamma[i] = float(_param(it, env, "gamma", "γ", where="integrator.gammas"))
     if gamma.shape[0] != n:
         raise InputError(f"integrator.gammas index {gamma.shape[0] - 1} is out of range")
-    return "BAOAB", gamma
+    return ("BAOAB" if kind == "BAOABLangevin" else "UnderdampedLangevin"), gamma
 
 
 def _system(sysd, boundary):
@@ -500,7 +502,7 @@ def load(path: str) -> Input:
         _check_keys(sch, {"type", "begin", "end", "each_step"}, "[simulator.schedule]")
         if sch.get("type") != "linear":
             raise InputError('schedule.type: only "linear" is supported')
-        if integrator != "BAOAB":
+        if integrator == "VelocityVerlet":
             raise InputError("SimulatedAnnealing needs a Langevin integrator")
         schedule = (float(sch["begin"]), float(sch["end"]), int(sim["each_step"]))
         temperature = schedule[0]                   # current(0), set before initialisation
@@ -582,7 +584,8 @@ def dumps(desc: SystemDesc, total_step: int = 1000, save_step: int = 100, prefix
     if desc.integrator == "VelocityVerlet":
         a('integrator.type = "VelocityVerlet"')
     else:
-        a('integrator.type = "BAOABLangevin"')
+        a('integrator.type = "UnderdampedLangevin"' if desc.integrator == "UnderdampedLangevin"
+          else 'integrator.type = "BAOABLangevin"')
         g = desc.gamma if desc.gamma is not None else np.zeros(desc.n)
         a("integrator.gammas = [")
         for i, x in enumerate(g):

@@ -62,7 +62,7 @@ class SystemDesc:
     bond_topology: str = "bond"        # connection kind each local term writes
     angle_topology: str = "none"
     dihedral_topology: str = "none"
-    integrator: str = "BAOAB"          # "BAOAB" | "VelocityVerlet"
+    integrator: str = "BAOAB"          # "BAOAB" | "VelocityVerlet" | "UnderdampedLangevin"
     dt: float = 0.01
     gamma: Optional[np.ndarray] = None
     seed: int = 12345

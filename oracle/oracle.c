@@ -94,6 +94,7 @@ struct orc_state
     /* integrator */
     double   dt, halfdt, kB, T;
     double  *exp_gamma_dt, *noise_coeff;
+    double  *accel;      /* UnderdampedLangevin: [3n] acceleration with noise */
     uint64_t step;
     /* local terms */
     int64_t  nbond, nangle, ndihd;
@@ -400,6 +401,7 @@ orc_state* orc_create(const orc_spec* s)
     st->halfdt = s->dt / 2;
     st->exp_gamma_dt = calloc((size_t)n, sizeof(double));
     st->noise_coeff  = calloc((size_t)n, sizeof(double));
+    st->accel        = calloc((size_t)(3 * n), sizeof(double));
     return st;
 }
 
@@ -407,7 +409,7 @@ void orc_destroy(orc_state* st)
 {
     if(!st) {return;}
     void* ptrs[] = {st->pos, st->vel, st->force, st->mass, st->rmass, st->gamma, st->mol,
-                    st->ex_ranges, st->ex_idx, st->exp_gamma_dt, st->noise_coeff,
+                    st->ex_ranges, st->ex_idx, st->exp_gamma_dt, st->noise_coeff, st->accel,
                     st->bond_idx, st->bond_k, st->bond_v0, st->angle_idx, st->angle_k,
                     st->angle_v0, st->dihd_idx, st->dihd_k, st->dihd_n, st->dihd_v0};
     for(size_t k=0; k<sizeof(ptrs)/sizeof(ptrs[0]); ++k) {free(ptrs[k]);}
@@ -1226,20 +1228,55 @@ void orc_gaussian3(uint64_t seed, uint64_t particle, uint64_t step, double out[3
 
 /* ------------------------------------------------------------ integrator */
 
-/* BAOABLangevinIntegrator::reset_parameters (:73-99) and initialize (:135-168);
- * VelocityVerletIntegrator::initialize has the same force evaluation. */
-int orc_init_dynamics(orc_state* st)
+/* Noise coefficients of the Langevin integrators.
+ * BAOAB: BAOABLangevinIntegrator::reset_parameters (:73-99),
+ *   exp(-gamma dt) and sqrt(kB T (1 - exp(-2 gamma dt)) / m).
+ * UnderdampedLangevin: UnderdampedLangevinIntegrator::update (:281-300), the
+ *   acceleration noise sigma = sqrt(2 kB T / dt) sqrt(gamma / m), kept in
+ *   noise_coeff (exp_gamma_dt unused). */
+static void noise_parameters(orc_state* st)
 {
     const double kBT = st->kB * st->T;
+    const double ul_coef = sqrt(2 * st->kB * st->T / st->dt);
     for(int64_t i=0; i<st->n; ++i)
     {
+        if(st->s.integrator == ORC_UNDERDAMPED)
+        {
+            st->exp_gamma_dt[i] = 1.0;
+            st->noise_coeff[i]  = ul_coef * sqrt(st->gamma[i] * st->rmass[i]);
+            continue;
+        }
         const double gamma_dt = -1 * st->gamma[i] * st->dt;
         st->exp_gamma_dt[i] = exp(gamma_dt);
         st->noise_coeff[i]  = sqrt(kBT * (1 - exp(2 * gamma_dt)) * st->rmass[i]);
     }
+}
+
+/* a = f/m + sigma R (UnderdampedLangevinIntegrator::initialize, :160-181, and
+ * the closing of step, :252-264), with the Philox noise of counter `ctr` */
+static void underdamped_accel(orc_state* st, int64_t i, uint64_t ctr)
+{
+    double R[3];
+    orc_gaussian3(st->s.seed, (uint64_t)i, ctr, R);
+    for(int d=0; d<3; ++d)
+    {
+        st->accel[3*i+d] = st->force[3*i+d] * st->rmass[i] + R[d] * st->noise_coeff[i];
+    }
+}
+
+/* BAOABLangevinIntegrator::initialize (:135-168); VelocityVerletIntegrator and
+ * UnderdampedLangevinIntegrator::initialize (:160-181) have the same force
+ * evaluation, the latter followed by the first acceleration (noise counter 0). */
+int orc_init_dynamics(orc_state* st)
+{
+    noise_parameters(st);
     memset(st->force, 0, sizeof(double) * 3 * st->n);
     calc_force(st);
     st->step = 0;
+    if(st->s.integrator == ORC_UNDERDAMPED)
+    {
+        for(int64_t i=0; i<st->n; ++i) {underdamped_accel(st, i, st->step);}
+    }
     return 0;
 }
 
@@ -1251,13 +1288,7 @@ int orc_init_dynamics(orc_state* st)
 void orc_set_temperature(orc_state* st, double T)
 {
     st->T = T;
-    const double kBT = st->kB * st->T;
-    for(int64_t i=0; i<st->n; ++i)
-    {
-        const double gamma_dt = -1 * st->gamma[i] * st->dt;
-        st->exp_gamma_dt[i] = exp(gamma_dt);
-        st->noise_coeff[i]  = sqrt(kBT * (1 - exp(2 * gamma_dt)) * st->rmass[i]);
-    }
+    noise_parameters(st);
 }
 
 /* GlobalPairInteraction::reduce_margin -> ...GridCellList::reduce_margin */
@@ -1297,6 +1328,28 @@ int orc_run(orc_state* st, int64_t nsteps)
                 largest_disp2 = largest_disp2 < d2 ? d2 : largest_disp2;
             }
         }
+        else if(st->s.integrator == ORC_UNDERDAMPED)   /* UnderdampedLangevinIntegrator.hpp:198-221 */
+        {
+            const double dt = st->dt, halfdt2 = dt * dt / 2;
+            for(int64_t i=0; i<n; ++i)
+            {
+                const double gdo2 = st->gamma[i] * halfdt;
+                const double omg  = 1 - gdo2;
+                const double* a = st->accel + 3*i;
+                double disp[3];
+                for(int d=0; d<3; ++d)
+                {
+                    disp[d] = (dt * omg) * st->vel[3*i+d] + halfdt2 * a[d];
+                    st->pos[3*i+d] = st->pos[3*i+d] + disp[d];
+                    st->vel[3*i+d] *= omg * (omg * omg + gdo2);
+                    st->vel[3*i+d] += (halfdt * omg) * a[d];
+                    st->force[3*i+d] = 0;
+                }
+                adjust_position(st, st->pos + 3*i);
+                const double d2 = length_sq(disp);
+                largest_disp2 = largest_disp2 < d2 ? d2 : largest_disp2;
+            }
+        }
         else                              /* BAOABLangevinIntegrator.hpp:170-240 */
         {
             for(int64_t i=0; i<n; ++i)
@@ -1326,10 +1379,22 @@ int orc_run(orc_state* st, int64_t nsteps)
         }
         reduce_margin(st, 2 * sqrt(largest_disp2));
         calc_force(st);
-        for(int64_t i=0; i<n; ++i)
+        if(st->s.integrator == ORC_UNDERDAMPED)   /* UnderdampedLangevinIntegrator.hpp:252-264 */
         {
-            const double c = halfdt * st->rmass[i];
-            for(int d=0; d<3; ++d) {st->vel[3*i+d] += c * st->force[3*i+d];}
+            for(int64_t i=0; i<n; ++i)
+            {
+                underdamped_accel(st, i, st->step + 1);
+                const double k = halfdt * (1 - st->gamma[i] * halfdt);
+                for(int d=0; d<3; ++d) {st->vel[3*i+d] += k * st->accel[3*i+d];}
+            }
+        }
+        else
+        {
+            for(int64_t i=0; i<n; ++i)
+            {
+                const double c = halfdt * st->rmass[i];
+                for(int d=0; d<3; ++d) {st->vel[3*i+d] += c * st->force[3*i+d];}
+            }
         }
         st->step++;
     }

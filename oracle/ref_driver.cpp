@@ -9,7 +9,8 @@
 //   - its half neighbour lists       (SpatialPartition::neighbors(), the CSR of
 //                                     core/NeighborList.hpp:151-266),
 //   - trajectories                   (BAOABLangevinIntegrator::step,
-//                                     VelocityVerletIntegrator::step),
+//                                     VelocityVerletIntegrator::step,
+//                                     UnderdampedLangevinIntegrator::step),
 //   - timings of its sequential and OpenMP paths.
 // The objects are put together the way the input readers do it
 // (input/read_global_interaction.hpp:25-98, input/read_local_interaction.hpp,
@@ -27,6 +28,7 @@
 #include <mjolnir/core/MsgPackLoader.hpp>
 #include <mjolnir/core/BAOABLangevinIntegrator.hpp>
 #include <mjolnir/core/VelocityVerletIntegrator.hpp>
+#include <mjolnir/core/UnderdampedLangevinIntegrator.hpp>
 #include <mjolnir/core/PeriodicGridCellList.hpp>
 #include <mjolnir/core/UnlimitedGridCellList.hpp>
 #include <mjolnir/forcefield/global/GlobalPairInteraction.hpp>
@@ -130,6 +132,7 @@ struct RefSim final : public RefSimBase
     rng_type rng;
     std::unique_ptr<BAOABLangevinIntegrator<traitsT>> baoab;
     std::unique_ptr<VelocityVerletIntegrator<traitsT>> vv;
+    std::unique_ptr<UnderdampedLangevinIntegrator<traitsT>> ul;
     local_base*  locals [3] = {nullptr, nullptr, nullptr};
     global_base* globals[3] = {nullptr, nullptr, nullptr};
     double time = 0.0;
@@ -352,6 +355,11 @@ struct RefSim final : public RefSimBase
         {
             make_vv(s.dt, std::integral_constant<bool, Sequential>{});
         }
+        else if(s.integrator == ORC_UNDERDAMPED)
+        {
+            ul = make_unique<UnderdampedLangevinIntegrator<traitsT>>(s.dt,
+                        std::move(gam), remover_type(false, false, false));
+        }
         else
         {
             baoab = make_unique<BAOABLangevinIntegrator<traitsT>>(s.dt,
@@ -502,14 +510,16 @@ struct RefSim final : public RefSimBase
 
     void initialize() override
     {
-        if(baoab) {baoab->initialize(*sys, ff, rng);}
-        else      {vv->initialize(*sys, ff, rng);}
+        if(baoab)   {baoab->initialize(*sys, ff, rng);}
+        else if(ul) {ul->initialize(*sys, ff, rng);}
+        else        {vv->initialize(*sys, ff, rng);}
     }
     void run(long long nsteps) override
     {
         for(long long s=0; s<nsteps; ++s)
         {
             time = baoab ? baoab->step(time, *sys, ff, rng)
+                 : ul    ? ul->step(time, *sys, ff, rng)
                          : vv->step(time, *sys, ff, rng);
         }
     }

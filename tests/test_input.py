@@ -182,7 +182,7 @@ include = "ff.toml"
     (lambda t: t.replace('{index = 3, sigma', '{index = 2, sigma'), "twice"),
     (lambda t: t.replace('{mass = 1.0, position = [1.0, 1.0, 1.0]}',
                          '{mass = 1.0, position = [1.0, 1.0, 1.0], velocity = [0.0, 0.0, 0.0]}'), "velocity"),
-    (lambda t: t.replace('integrator.type = "BAOABLangevin"', 'integrator.type = "UnderdampedLangevin"'),
+    (lambda t: t.replace('integrator.type = "BAOABLangevin"', 'integrator.type = "gBAOABLangevin"'),
      "BAOABLangevin"),
     (lambda t: t.replace('k = "k"', 'k = "kk"'), "kk"),
     (lambda t: t.replace('type = "CellList"', 'type = "Naive"'), "CellList"),
