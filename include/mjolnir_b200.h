@@ -48,7 +48,7 @@ enum { MJG_UNLIMITED = 0, MJG_PERIODIC_CUBOID = 1 };
 enum { MJG_TERM_BOND = 0, MJG_TERM_ANGLE = 1, MJG_TERM_DIHEDRAL = 2,
        MJG_TERM_EXV = 3, MJG_TERM_DH = 4, MJG_TERM_LJ = 5 };
 enum { MJG_IGNORE_NOTHING = 0, MJG_IGNORE_SELF = 1, MJG_IGNORE_OTHERS = 2 };
-enum { MJG_BAOAB = 0, MJG_VELOCITY_VERLET = 1, MJG_UNDERDAMPED_LANGEVIN = 2 };
+enum { MJG_BAOAB = 0, MJG_VELOCITY_VERLET = 1, MJG_UNDERDAMPED_LANGEVIN = 2, MJG_GJF_LANGEVIN = 3 };
 
 /* ---------------------------------------------------------------- context */
 
@@ -184,8 +184,10 @@ MJG_API int mjg_dihedrals_set(mjg_context* ctx, int sys, const char* topology, i
  * (core/VelocityVerletIntegrator.hpp) or UnderdampedLangevinIntegrator(dt,
  * gammas) (core/UnderdampedLangevinIntegrator.hpp; its acceleration with noise
  * is carried from step to step, across commits and rollbacks; replacing a
- * system's positions starts it again as Integrator::initialize does).
- * gamma[n] (ignored for Verlet).  The Langevin noise is Philox4x32-10 keyed
+ * system's positions starts it again as Integrator::initialize does) or
+ * GJFNVTLangevinIntegrator(dt, alphas) (core/GJFNVTLangevinIntegrator.hpp,
+ * "G-JFLangevin"; input/read_integrator.hpp:242-300).
+ * gamma[n]: the friction gammas, or the G-JF alphas (ignored for Verlet).  The Langevin noise is Philox4x32-10 keyed
  * by `seed` and counted by (particle, step), in place of the reference's
  * mt19937 stream (core/RandomNumberGenerator.hpp:13-86); the underdamped
  * closing of step t draws counter t + 1, its initialisation the current

@@ -870,6 +870,13 @@ void commit(mjg_context* c)
                 const double noise_coef = std::sqrt(2 * u.kB * s.T / s.dt);
                 coef[gi] = make_double4(rmass, s.gamma[i], noise_coef * std::sqrt(s.gamma[i] * rmass), s.dt);
             }
+            else if(s.integrator == I_GJF)     // GJFNVTLangevinIntegrator::reset_parameters (:111-136)
+            {
+                const double alpha = s.gamma[i], m = s.mass[i];
+                const double b = 1.0 / (1.0 + alpha * s.dt * 0.5 / m);
+                coef[gi] = make_double4(halfdt * rmass, 1.0 - alpha * b * s.dt / m,
+                                        std::sqrt(2 * alpha * kBT * s.dt), s.dt);
+            }
             else if(s.integrator == I_BAOAB)   // reset_parameters (:73-99)
             {
                 const double gamma_dt = -1 * s.gamma[i] * s.dt;
@@ -978,10 +985,17 @@ void commit(mjg_context* c)
     put(c->d_mol, c_mol);
     c->d_force.ensure(32 * (size_t)std::max<long long>(n_tot, 1));
     c->d_force_scratch.ensure(32 * (size_t)std::max<long long>(n_tot, 1));
-    bool any_underdamped = false;
-    for(int id : ids) {any_underdamped = any_underdamped || c->sys[id].integrator == I_UNDERDAMPED;}
-    if(any_underdamped) {c->d_accel.ensure(32 * (size_t)std::max<long long>(n_tot, 1));}
-    else                {c->d_accel.release();}
+    // the per-particle auxiliary array: UnderdampedLangevin accelerations,
+    // G-JF coefficients
+    bool any_underdamped = false, any_gjf = false;
+    for(int id : ids)
+    {
+        any_underdamped = any_underdamped || c->sys[id].integrator == I_UNDERDAMPED;
+        any_gjf = any_gjf || c->sys[id].integrator == I_GJF;
+    }
+    const bool any_aux = any_underdamped || any_gjf;
+    if(any_aux) {c->d_accel.ensure(32 * (size_t)std::max<long long>(n_tot, 1));}
+    else        {c->d_accel.release();}
     c->d_staging.ensure(sizeof(double) * 3 * (size_t)std::max<long long>(n_tot, 1));
     if(c->rollback)
     {
@@ -989,7 +1003,7 @@ void commit(mjg_context* c)
         c->b_pos.ensure(c->d_pos.bytes);
         c->b_vel.ensure(c->d_vel.bytes);
         c->b_force.ensure(c->d_force.bytes);
-        if(any_underdamped) {c->b_accel.ensure(c->d_accel.bytes);} else {c->b_accel.release();}
+        if(any_aux) {c->b_accel.ensure(c->d_accel.bytes);} else {c->b_accel.release();}
     }
     else
     {
@@ -1010,7 +1024,7 @@ void commit(mjg_context* c)
     a.psys = c->d_psys.as<int>();
     a.staging = c->d_staging.as<double>();
     a.mol = c->d_mol.as<int>();
-    a.accel = any_underdamped ? c->d_accel.as<double4>() : nullptr;
+    a.accel = any_aux ? c->d_accel.as<double4>() : nullptr;
 
     for(int g = 0; g < NGLOBAL; ++g)
     {
@@ -1194,13 +1208,33 @@ void commit(mjg_context* c)
         }
     }
     // UnderdampedLangevin: resident systems keep their accelerations, the
-    // others start from Integrator::initialize
-    if(any_underdamped)
+    // others start from Integrator::initialize.  G-JF: the coefficients
+    // {1/2m, b/m, b dt} of GJFNVTLangevinIntegrator::reset_parameters
+    // (:111-136) and step (:183-204).
+    if(c->arena.accel)
     {
         double* stg = c->d_staging.as<double>();
+        std::vector<double> gjf;
         for(int k = 0; k < nsys; ++k)
         {
             HostSystem& s = c->sys[ids[k]];
+            if(s.integrator == I_GJF)
+            {
+                gjf.resize(3 * (size_t)s.n);
+                for(int64_t i = 0; i < s.n; ++i)
+                {
+                    const double alpha = s.gamma[i], m = s.mass[i], rm = 1.0 / m;
+                    const double b = 1.0 / (1.0 + alpha * s.dt * 0.5 / m);
+                    gjf[3 * i] = 0.5 * rm;
+                    gjf[3 * i + 1] = b * rm;
+                    gjf[3 * i + 2] = b * s.dt;
+                }
+                CK(cudaMemcpyAsync(stg + 3 * s.off, gjf.data(), sizeof(double) * 3 * s.n,
+                                   cudaMemcpyHostToDevice, st));
+                launch_set_accel(c->arena, stg + 3 * s.off, s.off, s.n, st);
+                CK(cudaStreamSynchronize(st));    // gjf is reused for the next system
+                continue;
+            }
             if(s.integrator != I_UNDERDAMPED) {continue;}
             if(s.accel_valid && (int64_t)s.accel.size() == 3 * s.n)
             {
@@ -1430,8 +1464,9 @@ int mjg_system_set_temperature(mjg_context* c, int sys, double T)
     if(!(T > 0)) {throw Error(MJG_EINVAL, "temperature must be positive");}
     s.T = T;
     if(!c->committed || !s.resident || s.integrator == I_VV) {return MJG_OK;}
-    // BAOABLangevinIntegrator::update -> reset_parameters (:47-58, :73-99) or
-    // UnderdampedLangevinIntegrator::update (:55-70): the noise coefficients of
+    // BAOABLangevinIntegrator::update -> reset_parameters (:47-58, :73-99),
+    // UnderdampedLangevinIntegrator::update (:55-70) or
+    // GJFNVTLangevinIntegrator::update (:87-97): the noise coefficients of
     // the system's particles, computed as at commit
     const Units u;
     const double kBT = u.kB * s.T;
@@ -1444,6 +1479,7 @@ int mjg_system_set_temperature(mjg_context* c, int sys, double T)
             z[i] = std::sqrt(2 * u.kB * s.T / s.dt) * std::sqrt(s.gamma[i] * rmass);
             continue;
         }
+        if(s.integrator == I_GJF) {z[i] = std::sqrt(2 * s.gamma[i] * kBT * s.dt); continue;}
         const double gamma_dt = -1 * s.gamma[i] * s.dt;
         z[i] = std::sqrt(kBT * (1 - std::exp(2 * gamma_dt)) * (1.0 / s.mass[i]));
     }
@@ -1708,13 +1744,15 @@ int mjg_integrator_set(mjg_context* c, int sys, int kind, double dt, const doubl
     ABI_BEGIN(c)
     HostSystem& s = get_sys(c, sys);
     if(s.resident) {throw Error(MJG_ESTATE, "the integrator is fixed once committed");}
-    if(kind != MJG_BAOAB && kind != MJG_VELOCITY_VERLET && kind != MJG_UNDERDAMPED_LANGEVIN)
+    if(kind != MJG_BAOAB && kind != MJG_VELOCITY_VERLET && kind != MJG_UNDERDAMPED_LANGEVIN &&
+       kind != MJG_GJF_LANGEVIN)
     {
         throw Error(MJG_EINVAL, "unknown integrator");
     }
     if(!(dt > 0)) {throw Error(MJG_EINVAL, "dt must be positive");}
     if(kind != MJG_VELOCITY_VERLET && !gamma) {throw Error(MJG_EINVAL, "Langevin integrators need gammas");}
-    s.integrator = kind == MJG_BAOAB ? I_BAOAB : kind == MJG_VELOCITY_VERLET ? I_VV : I_UNDERDAMPED;
+    s.integrator = kind == MJG_BAOAB ? I_BAOAB : kind == MJG_VELOCITY_VERLET ? I_VV :
+                   kind == MJG_UNDERDAMPED_LANGEVIN ? I_UNDERDAMPED : I_GJF;
     s.dt = dt;
     s.gamma = gamma ? std::vector<double>(gamma, gamma + s.n) : std::vector<double>(s.n, 0.0);
     s.seed = seed;

@@ -56,7 +56,7 @@ __device__ __forceinline__ void underdamped_close(const SysDev& S, long long i, 
 }
 
 // B-A-O-A of BAOAB (or the first half-kick and drift of velocity Verlet, or
-// the first half of an UnderdampedLangevin step), force reset and the
+// the first half of an UnderdampedLangevin or G-JF step), force reset and the
 // per-system largest squared displacement.  With KICK the previous step's
 // closing half is applied first, as separate rounding steps, so that
 // consecutive steps of a chunk share one pass.
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
         const SysDev& S = a.sys[s];
         double4 p = a.pos[i];
         double4 v = a.vel[i];
-        const double4 c = a.coef[i];     // {halfdt*rmass, exp(-gamma dt), noise, halfdt | dt}
+        const double4 c = a.coef[i];     // per integrator: see Arena::coef
         double fx, fy, fz;
         load_force<PREC>(a.force, i, fx, fy, fz);
         const bool uld = S.integrator == I_UNDERDAMPED;
@@ -102,6 +102,21 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
             v.x = __dadd_rn(v.x, __dmul_rn(sa, acc.x));
             v.y = __dadd_rn(v.y, __dmul_rn(sa, acc.y));
             v.z = __dadd_rn(v.z, __dmul_rn(sa, acc.z));
+        }
+        else if(S.integrator == I_GJF)   // core/GJFNVTLangevinIntegrator.hpp:183-204
+        {
+            double r0, r1, r2;
+            gaussian3(S.seed, (unsigned long long)(i - S.off), S.step, r0, r1, r2);
+            const double4 x = a.accel[i];                       // {1/2m, b/m, b dt}
+            const double b0 = __dmul_rn(r0, c.z), b1 = __dmul_rn(r1, c.z), b2 = __dmul_rn(r2, c.z);
+            // dp = (b dt) (v + 1/2m (dt f + beta))
+            dx = __dmul_rn(x.z, __dadd_rn(v.x, __dmul_rn(x.x, __dadd_rn(__dmul_rn(c.w, fx), b0))));
+            dy = __dmul_rn(x.z, __dadd_rn(v.y, __dmul_rn(x.x, __dadd_rn(__dmul_rn(c.w, fy), b1))));
+            dz = __dmul_rn(x.z, __dadd_rn(v.z, __dmul_rn(x.x, __dadd_rn(__dmul_rn(c.w, fz), b2))));
+            // v = a (v + (dt/2m) f) + (b/m) beta
+            v.x = __dadd_rn(__dmul_rn(c.y, __dadd_rn(v.x, __dmul_rn(c.x, fx))), __dmul_rn(x.y, b0));
+            v.y = __dadd_rn(__dmul_rn(c.y, __dadd_rn(v.y, __dmul_rn(c.x, fy))), __dmul_rn(x.y, b1));
+            v.z = __dadd_rn(__dmul_rn(c.y, __dadd_rn(v.z, __dmul_rn(c.x, fz))), __dmul_rn(x.y, b2));
         }
         else if(S.integrator == I_BAOAB)
         {
@@ -207,7 +222,7 @@ __global__ void k_margin(Arena a, int* any0, int* any1, int* any2)
 }
 
 // closing half of the last step of a chunk: v += (halfdt/m) f (BAOAB,
-// velocity Verlet) or the UnderdampedLangevin closing
+// velocity Verlet, G-JF) or the UnderdampedLangevin closing
 template<int PREC>
 __global__ void __launch_bounds__(TPB) k_integrate_last(Arena a)
 {

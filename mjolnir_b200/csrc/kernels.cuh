@@ -15,8 +15,10 @@ struct Arena {
     double4*  vel;
     void*     force;            // double4 (P_FP64) or longlong4 (P_MIXED)
     double4*  coef;             // BAOAB {halfdt/m, e^-g dt, noise, halfdt}; VV {halfdt/m, 1, 0, dt};
-                                // UnderdampedLangevin {1/m, gamma, noise sigma, dt}
-    double4*  accel;            // UnderdampedLangevin: acceleration with noise (nullptr: none)
+                                // UnderdampedLangevin {1/m, gamma, noise sigma, dt};
+                                // G-JF {halfdt/m, a, beta, dt}
+    double4*  accel;            // UnderdampedLangevin: acceleration with noise; G-JF: {1/2m, b/m, b dt}
+                                // (nullptr: no system of either kind)
     int*      psys;
     double*   staging;          // [3 n] host-layout staging for copies
     // exclusions (per global term): excluded partners of every particle,

@@ -17,8 +17,9 @@ ready for :meth:`Engine.add_system`:
   ``precision``, ``parallelism``, ``seed`` (or the deprecated
   ``integrator.seed``), ``delta_t``, ``total_step``, ``save_step``,
   ``integrator.type`` = ``"BAOABLangevin"`` or ``"UnderdampedLangevin"``
-  (``gammas`` or the deprecated ``parameters``, input/read_integrator.hpp:55-187)
-  or ``"VelocityVerlet"``;
+  (``gammas`` or the deprecated ``parameters``, input/read_integrator.hpp:55-187),
+  ``"G-JFLangevin"`` (``alphas`` or ``parameters``, :242-300) or
+  ``"VelocityVerlet"``;
 * ``[[systems]]`` (the first): ``attributes``, ``boundary_shape``,
   ``particles`` with ``mass|m``, ``position|pos``, ``velocity|vel``, ``name``,
   ``group`` (input/read_system.hpp:93-290), or ``file_name = "x.msg"``, a
@@ -234,24 +235,32 @@ def _integrator(integ, n):
     if kind == "VelocityVerlet":
         _check_keys(integ, {"type", "seed", "remove"}, "[simulator.integrator]")
         return "VelocityVerlet", np.zeros(n)
-    if kind not in ("BAOABLangevin", "UnderdampedLangevin"):
-        raise InputError(f'integrator type "{kind}": only "BAOABLangevin", "UnderdampedLangevin" and '
-                         '"VelocityVerlet" are supported')
-    _check_keys(integ, {"type", "seed", "remove", "env", "parameters", "gammas"}, "[simulator.integrator]")
-    if "parameters" in integ and "gammas" in integ:
-        raise InputError('duplicated keys: both "parameters" and "gammas" are provided')
-    items = integ.get("gammas", integ.get("parameters"))
+    if kind not in _LANGEVIN:
+        raise InputError(f'integrator type "{kind}": only "BAOABLangevin", "UnderdampedLangevin", '
+                         '"G-JFLangevin" and "VelocityVerlet" are supported')
+    name, plural, single, alt = _LANGEVIN[kind]
+    _check_keys(integ, {"type", "seed", "remove", "env", "parameters", plural}, "[simulator.integrator]")
+    if "parameters" in integ and plural in integ:
+        raise InputError(f'duplicated keys: both "parameters" and "{plural}" are provided')
+    items = integ.get(plural, integ.get("parameters"))
     if items is None:
-        raise InputError("BAOABLangevin needs gammas")
+        raise InputError(f"{kind} needs {plural}")
     env = integ.get("env")
-    idx = [_index(it, env, "integrator.gammas") for it in items]
-    _no_overlap(idx, "integrator.gammas")
+    idx = [_index(it, env, f"integrator.{plural}") for it in items]
+    _no_overlap(idx, f"integrator.{plural}")
     gamma = np.zeros(max(n, max(idx, default=-1) + 1))
     for i, it in zip(idx, items):
-        gamma[i] = float(_param(it, env, "gamma", "γ", where="integrator.gammas"))
+        gamma[i] = float(_param(it, env, *[k for k in (single, alt) if k], where=f"integrator.{plural}"))
     if gamma.shape[0] != n:
-        raise InputError(f"integrator.gammas index {gamma.shape[0] - 1} is out of range")
-    return ("BAOAB" if kind == "BAOABLangevin" else "UnderdampedLangevin"), gamma
+        raise InputError(f"integrator.{plural} index {gamma.shape[0] - 1} is out of range")
+    return name, gamma
+
+
+# integrator type -> (SystemDesc.integrator, list key, parameter key, its
+# alternative spelling); input/read_integrator.hpp:55-187, 242-300
+_LANGEVIN = {"BAOABLangevin": ("BAOAB", "gammas", "gamma", "γ"),
+             "UnderdampedLangevin": ("UnderdampedLangevin", "gammas", "gamma", "γ"),
+             "G-JFLangevin": ("G-JFLangevin", "alphas", "alpha", None)}
 
 
 def _system(sysd, boundary):
@@ -584,12 +593,13 @@ def dumps(desc: SystemDesc, total_step: int = 1000, save_step: int = 100, prefix
     if desc.integrator == "VelocityVerlet":
         a('integrator.type = "VelocityVerlet"')
     else:
-        a('integrator.type = "UnderdampedLangevin"' if desc.integrator == "UnderdampedLangevin"
-          else 'integrator.type = "BAOABLangevin"')
+        kind = {v[0]: k for k, v in _LANGEVIN.items()}[desc.integrator]
+        _, plural, single, _ = _LANGEVIN[kind]
+        a(f'integrator.type = "{kind}"')
         g = desc.gamma if desc.gamma is not None else np.zeros(desc.n)
-        a("integrator.gammas = [")
+        a(f"integrator.{plural} = [")
         for i, x in enumerate(g):
-            a(f"  {{index = {i}, gamma = {_fmt(float(x))}}},")
+            a(f"  {{index = {i}, {single} = {_fmt(float(x))}}},")
         a("]")
     a("")
     a("[[systems]]")

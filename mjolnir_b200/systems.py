@@ -62,9 +62,9 @@ class SystemDesc:
     bond_topology: str = "bond"        # connection kind each local term writes
     angle_topology: str = "none"
     dihedral_topology: str = "none"
-    integrator: str = "BAOAB"          # "BAOAB" | "VelocityVerlet" | "UnderdampedLangevin"
+    integrator: str = "BAOAB"          # "BAOAB" | "VelocityVerlet" | "UnderdampedLangevin" | "G-JFLangevin"
     dt: float = 0.01
-    gamma: Optional[np.ndarray] = None
+    gamma: Optional[np.ndarray] = None # friction per particle (G-JFLangevin: its alpha)
     seed: int = 12345
     start_step: int = 0                # noise step counter to resume from (checkpoints)
 

@@ -95,6 +95,7 @@ struct orc_state
     double   dt, halfdt, kB, T;
     double  *exp_gamma_dt, *noise_coeff;
     double  *accel;      /* UnderdampedLangevin: [3n] acceleration with noise */
+    double  *gjf_b;      /* G-JF: [n] b = 1 / (1 + alpha dt / 2m)              */
     uint64_t step;
     /* local terms */
     int64_t  nbond, nangle, ndihd;
@@ -402,6 +403,7 @@ orc_state* orc_create(const orc_spec* s)
     st->exp_gamma_dt = calloc((size_t)n, sizeof(double));
     st->noise_coeff  = calloc((size_t)n, sizeof(double));
     st->accel        = calloc((size_t)(3 * n), sizeof(double));
+    st->gjf_b        = calloc((size_t)n, sizeof(double));
     return st;
 }
 
@@ -409,7 +411,7 @@ void orc_destroy(orc_state* st)
 {
     if(!st) {return;}
     void* ptrs[] = {st->pos, st->vel, st->force, st->mass, st->rmass, st->gamma, st->mol,
-                    st->ex_ranges, st->ex_idx, st->exp_gamma_dt, st->noise_coeff, st->accel,
+                    st->ex_ranges, st->ex_idx, st->exp_gamma_dt, st->noise_coeff, st->accel, st->gjf_b,
                     st->bond_idx, st->bond_k, st->bond_v0, st->angle_idx, st->angle_k,
                     st->angle_v0, st->dihd_idx, st->dihd_k, st->dihd_n, st->dihd_v0};
     for(size_t k=0; k<sizeof(ptrs)/sizeof(ptrs[0]); ++k) {free(ptrs[k]);}
@@ -1233,7 +1235,10 @@ void orc_gaussian3(uint64_t seed, uint64_t particle, uint64_t step, double out[3
  *   exp(-gamma dt) and sqrt(kB T (1 - exp(-2 gamma dt)) / m).
  * UnderdampedLangevin: UnderdampedLangevinIntegrator::update (:281-300), the
  *   acceleration noise sigma = sqrt(2 kB T / dt) sqrt(gamma / m), kept in
- *   noise_coeff (exp_gamma_dt unused). */
+ *   noise_coeff (exp_gamma_dt unused).
+ * G-JF: GJFNVTLangevinIntegrator::reset_parameters (:111-136), with alpha in
+ *   gamma: b = 1 / (1 + alpha dt / 2m) in gjf_b, beta = sqrt(2 alpha kB T dt)
+ *   in noise_coeff, a = 1 - alpha b dt / m in exp_gamma_dt. */
 static void noise_parameters(orc_state* st)
 {
     const double kBT = st->kB * st->T;
@@ -1244,6 +1249,14 @@ static void noise_parameters(orc_state* st)
         {
             st->exp_gamma_dt[i] = 1.0;
             st->noise_coeff[i]  = ul_coef * sqrt(st->gamma[i] * st->rmass[i]);
+            continue;
+        }
+        if(st->s.integrator == ORC_GJF)
+        {
+            const double alpha = st->gamma[i], m = st->mass[i];
+            st->gjf_b[i]        = 1.0 / (1.0 + alpha * st->dt * 0.5 / m);
+            st->noise_coeff[i]  = sqrt(2 * alpha * kBT * st->dt);
+            st->exp_gamma_dt[i] = 1.0 - alpha * st->gjf_b[i] * st->dt / m;
             continue;
         }
         const double gamma_dt = -1 * st->gamma[i] * st->dt;
@@ -1350,6 +1363,30 @@ int orc_run(orc_state* st, int64_t nsteps)
                 largest_disp2 = largest_disp2 < d2 ? d2 : largest_disp2;
             }
         }
+        else if(st->s.integrator == ORC_GJF)   /* GJFNVTLangevinIntegrator.hpp:175-204 */
+        {
+            const double dt = st->dt;
+            for(int64_t i=0; i<n; ++i)
+            {
+                const double rm = st->rmass[i], r2m = 0.5 * rm;
+                const double b = st->gjf_b[i], a = st->exp_gamma_dt[i];
+                double R[3], beta[3], dp[3];
+                orc_gaussian3(st->s.seed, (uint64_t)i, st->step, R);
+                for(int d=0; d<3; ++d) {beta[d] = R[d] * st->noise_coeff[i];}
+                for(int d=0; d<3; ++d)
+                {
+                    double* v = st->vel + 3*i+d;
+                    const double f = st->force[3*i+d];
+                    dp[d] = (b * dt) * (*v + r2m * (dt * f + beta[d]));
+                    st->pos[3*i+d] = st->pos[3*i+d] + dp[d];
+                    *v = a * (*v + (dt * r2m) * f) + b * rm * beta[d];
+                    st->force[3*i+d] = 0;
+                }
+                adjust_position(st, st->pos + 3*i);
+                const double d2 = length_sq(dp);
+                largest_disp2 = largest_disp2 < d2 ? d2 : largest_disp2;
+            }
+        }
         else                              /* BAOABLangevinIntegrator.hpp:170-240 */
         {
             for(int64_t i=0; i<n; ++i)
@@ -1388,7 +1425,7 @@ int orc_run(orc_state* st, int64_t nsteps)
                 for(int d=0; d<3; ++d) {st->vel[3*i+d] += k * st->accel[3*i+d];}
             }
         }
-        else
+        else    /* BAOAB, velocity Verlet; G-JF's (dt 0.5 / m) f (:211-218) is the same product */
         {
             for(int64_t i=0; i<n; ++i)
             {

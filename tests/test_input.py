@@ -287,3 +287,30 @@ parameters = [{index = 0, radius = 1.0}, {index = 1, radius = 1.0}]
 """
     d = I.load(_write(tmp_path, "ip.toml", text)).desc
     assert d.exv.kind == "InversePower" and d.exv.exponent == 5 and d.exv.cutoff == 4.0   # 2^(12 // 5)
+
+
+@pytest.mark.parametrize("integrator", ["UnderdampedLangevin", "G-JFLangevin", "VelocityVerlet"])
+def test_integrator_round_trip(integrator, tmp_path):
+    """Every supported integrator type is written and read back with its
+    per-particle parameters (gammas, or the G-JF alphas)."""
+    d = S.polymer_melt(nchains=2, nbeads=10, radius=30.0, seed=6)
+    d.integrator = integrator
+    d.gamma = np.random.default_rng(1).uniform(0.1, 2.0, d.n) if integrator != "VelocityVerlet" else np.zeros(d.n)
+    path = str(tmp_path / "i.toml")
+    I.dump(d, path)
+    text = open(path).read()
+    assert ("alphas" in text) == (integrator == "G-JFLangevin")
+    g = I.load(path).desc
+    assert g.integrator == integrator
+    np.testing.assert_array_equal(g.gamma, d.gamma)
+
+
+def test_gjf_rejects_gammas(tmp_path):
+    d = S.polymer_melt(nchains=2, nbeads=10, radius=30.0, seed=6)
+    d.integrator = "G-JFLangevin"
+    path = str(tmp_path / "i.toml")
+    I.dump(d, path)
+    text = open(path).read().replace("integrator.alphas", "integrator.gammas")
+    open(path, "w").write(text)
+    with pytest.raises(I.InputError, match="gammas"):
+        I.load(path)
