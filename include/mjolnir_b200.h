@@ -287,6 +287,10 @@ MJG_API int mjg_set_list_capacity(mjg_context* ctx, int term, int cap);
 MJG_API int mjg_rebuild_count(mjg_context* ctx, int sys, int term, int64_t* count);
 /* Number of integrator steps taken by a system since it was created. */
 MJG_API int mjg_step_count(mjg_context* ctx, int sys, int64_t* steps);
+/* Number of molecules of a system: the groups of particles joined by "bond"
+ * connections (Topology::construct_molecules, core/Topology.hpp:280-316;
+ * Topology::number_of_molecules, :118), as the DCD header records them. */
+MJG_API int mjg_molecule_count(mjg_context* ctx, int sys, int64_t* count);
 
 /* Number of particles of all committed systems, and of one system. */
 MJG_API int mjg_particle_count(mjg_context* ctx, int sys, int64_t* n);

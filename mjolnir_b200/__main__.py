@@ -3,18 +3,19 @@
     python -m mjolnir_b200 input.toml [--precision fp64|mixed] [--device 0]
 
 Reads the file with :func:`mjolnir_b200.input.load`, advances the system
-``total_step`` steps and, every ``save_step`` steps (and at step 0), appends
-the per-term energies, the kinetic energy and the attributes to
-``<path>/<prefix>.ene``, and frames of positions and velocities to
-``<path>/<prefix>_position.xyz`` and ``_velocity.xyz``, in the layout of the reference's
-EnergyObserver and XYZObserver (core/EnergyObserver.hpp:63-153,
-core/XYZObserver.hpp:46-76; interactions in the order bonds, angles,
-dihedrals, then the global terms).  Every ``checkpoint_step`` steps and at the
-end it writes ``<prefix>_system.msg`` and ``<prefix>_rng.msg``
-(:mod:`mjolnir_b200.checkpoint`).
+``total_step`` steps and writes what the reference's simulator writes for the
+same input, in the same layouts (:mod:`mjolnir_b200.observers`): at step 0,
+every ``save_step`` steps and at the end, ``<path><prefix>.ene`` (energies of
+the interactions in the order bonds, angles, dihedrals, then the global
+terms; kinetic energy; the system's attributes) and the trajectory formats of
+``files.output.format`` (xyz, dcd, trr); at step 0, every ``checkpoint_step``
+steps and at the end, ``<prefix>_system.msg`` and ``<prefix>_rng.msg``
+(:mod:`mjolnir_b200.checkpoint`).  The order of those calls is the one of
+core/MolecularDynamicsSimulator.hpp:72-125 and
+core/SimulatedAnnealingSimulator.hpp:121-150: observers and checkpoint before
+the step, the temperature update of an annealing run after it.
 ``precision = "double"`` in the input selects the FP64 form unless
-``--precision`` says otherwise.  A ``SimulatedAnnealing`` input follows its
-linear temperature schedule (:mod:`mjolnir_b200.anneal`).
+``--precision`` says otherwise (and sets the real type of the .trr file).
 """
 from __future__ import annotations
 
@@ -26,6 +27,7 @@ import time
 import numpy as np
 
 from . import checkpoint
+from . import observers as O
 from .anneal import current
 from .engine import Engine
 from .input import load
@@ -39,7 +41,7 @@ PAIR_NAME = {"ExcludedVolume": "GlobalPairExcludedVolume", "LennardJones": "Glob
              "HardCoreExcludedVolume": "Pair:HardCoreExcludedVolume"}
 
 
-def _present(desc):
+def present_terms(desc):
     """(term key, column title) of every interaction, local then global."""
     out = []
     if desc.bonds is not None:
@@ -55,68 +57,76 @@ def _present(desc):
     return out
 
 
-def _frame(f, names, arr, step):
-    """One frame of core/XYZObserver.hpp:46-76: count, "step = N", then
-    "name x y z" with eight decimals."""
-    f.write(f"{arr.shape[0]}\nstep = {step}\n")
-    f.write("".join(f"{nm} {x:.8f} {y:.8f} {z:.8f}\n" for nm, (x, y, z) in zip(names, arr)))
-
-
 def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) -> dict:
     inp = load(path)
     d = inp.desc
     prec = precision or ("fp64" if inp.precision == "double" else "mixed")
     total = inp.total_step if steps is None else int(steps)
     save = max(1, inp.save_step)
-    os.makedirs(inp.output_path, exist_ok=True)
-    ene_path = os.path.join(inp.output_path, inp.output_prefix + ".ene")
-    xyz_path = os.path.join(inp.output_path, inp.output_prefix + "_position.xyz")
-    vel_path = os.path.join(inp.output_path, inp.output_prefix + "_velocity.xyz")
-    terms = _present(d)
-    widths = [max(len(title), 10) for _, title in terms]       # LocalForceField.hpp:57
     ckpt = max(1, inp.checkpoint_step or save)
-    ck_prefix = os.path.join(inp.output_path, inp.output_prefix)
-    names = ["X"] * d.n
+    prefix = inp.file_prefix
+    if inp.output_path:
+        os.makedirs(inp.output_path, exist_ok=True)
+    terms = present_terms(d)
+    attrs = dict(inp.attributes or {})
+    if inp.schedule:                         # the schedule's first temperature, set at initialisation
+        attrs["temperature"] = d.temperature
     eng = Engine(prec, device=device)
     sid = eng.add_system(d)
     eng.commit()
+    width = tuple(float(u - lo) for u, lo in zip(d.upper, d.lower))
+    molecules = eng.molecule_count(sid)
+
+    def frame():
+        p, v, f = eng.state(sid)
+        e = eng.energies(sid)
+        return O.Frame(pos=p, vel=v, force=f, mass=d.mass, energies=[(title, e[key]) for key, title in terms],
+                       attributes=attrs, names=inp.names, periodic=d.periodic, width=width,
+                       molecules=molecules)
+
+    def save_checkpoint():
+        checkpoint.save(eng, sid, d, prefix, attributes=attrs, names=inp.names, groups=inp.groups)
+
+    obs = O.make(inp.output_formats, prefix, real="f8" if inp.precision == "double" else "f4")
     t0 = time.perf_counter()
     anneal = inp.schedule                    # SimulatedAnnealing: (first, last, each_step)
     r_total = 1.0 / total if total else 0.0
-    temperature = d.temperature
-    with open(ene_path, "w") as ene, open(xyz_path, "w") as xyz, open(vel_path, "w") as vel:
-        # core/EnergyObserver.hpp:63-87 (header), :89-153 (rows)
-        attrs = sorted({"temperature": 0.0, "ionic_strength": 0.0})
-        ene.write("# timestep  " + "".join(title + " " for _, title in terms) + " kinetic_energy" +
-                  "".join(f" attribute:{a}" for a in attrs) + "\n")
-        done = 0
-        while True:
-            if done > 0 and (done % ckpt == 0 or done >= total):   # MsgPackSaver at checkpoint_step and at the end
-                checkpoint.save(eng, sid, d, ck_prefix)
-            if done % save == 0 or done >= total:
-                e = eng.energies(sid)
-                p, v, _ = eng.state(sid)
-                kin = 0.5 * float(np.sum(np.sum(v * v, axis=1) * d.mass))
-                values = {"temperature": temperature, "ionic_strength": d.ionic_strength}
-                ene.write(f"{str(done):<11} " +
-                          "".join(f"{e[key]:>{w}.6f} " for (key, _), w in zip(terms, widths)) +
-                          f"{kin:>14.6f}" + "".join(f" {values[a]:>{10 + len(a)}.6f}" for a in attrs) + "\n")
-                _frame(xyz, names, p, done)
-                _frame(vel, names, v, done)
-            if done >= total:
-                break
-            k = min(save - done % save, ckpt - done % ckpt, total - done)
-            if anneal:
-                k = min(k, anneal[2] - done % anneal[2])
-            eng.step(k)
-            done += k
-            if anneal and done % anneal[2] == 0:    # core/SimulatedAnnealingSimulator.hpp:144-154
-                temperature = current(anneal[0], anneal[1], done * r_total)
-                eng.set_temperature(sid, temperature)
+    fr = frame()
+    for o in obs:
+        o.initialize(total, save, d.dt, fr)
+    done = 0
+    while done < total:
+        if done % save == 0:
+            fr = frame()
+            for o in obs:
+                o.output(done, d.dt, fr)
+        if done % ckpt == 0:
+            save_checkpoint()
+        k = min(save - done % save, ckpt - done % ckpt, total - done)
+        if anneal:
+            k = min(k, anneal[2] - done % anneal[2])
+        eng.step(k)
+        done += k
+        if anneal and done % anneal[2] == 0:    # core/SimulatedAnnealingSimulator.hpp:144-154
+            attrs["temperature"] = current(anneal[0], anneal[1], done * r_total)
+            eng.set_temperature(sid, attrs["temperature"])
+    fr = frame()                             # finalize: the last frame, then the checkpoint
+    for o in obs:
+        o.output(total, d.dt, fr)
+    for o in obs:
+        o.finalize(total, d.dt, fr)
+    save_checkpoint()
     wall = time.perf_counter() - t0
     eng.close()
     res = {"steps": total, "particles": d.n, "precision": prec, "wall_s": wall,
-           "energy_file": ene_path, "trajectory": xyz_path, "velocities": vel_path}
+           "energy_file": prefix + ".ene", "formats": list(inp.output_formats)}
+    if "xyz" in inp.output_formats:
+        res["trajectory"] = prefix + "_position.xyz"
+        res["velocities"] = prefix + "_velocity.xyz"
+    if "dcd" in inp.output_formats:
+        res["dcd"] = prefix + "_position.dcd"
+    if "trr" in inp.output_formats:
+        res["trr"] = prefix + ".trr"
     print(res, file=out)
     return res
 

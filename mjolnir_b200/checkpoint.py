@@ -105,13 +105,16 @@ def read_rng(path: str):
     return int(parts[1]), int(parts[2])
 
 
-def save(engine, sid: int, desc: SystemDesc, prefix: str):
+def save(engine, sid: int, desc: SystemDesc, prefix: str, attributes=None, names=None, groups=None):
     """Writes ``<prefix>_system.msg`` and ``<prefix>_rng.msg`` for system
-    `sid` of `engine` (its current state; `desc` gives masses, box and
-    attributes)."""
+    `sid` of `engine` (its current state; `desc` gives masses and box;
+    `attributes` default to the temperature and ionic strength of `desc`;
+    names "X" and groups "NONE" unless given)."""
     pos, vel, force = engine.state(sid)
+    if attributes is None:
+        attributes = {"temperature": desc.temperature, "ionic_strength": desc.ionic_strength}
     write_system(prefix + "_system.msg", pos, vel, force, desc.mass, desc.periodic, desc.lower,
-                 desc.upper, {"temperature": desc.temperature, "ionic_strength": desc.ionic_strength})
+                 desc.upper, attributes, names, groups)
     write_rng(prefix + "_rng.msg", desc.seed, engine.step_count(sid))
 
 

@@ -492,15 +492,10 @@ void save_resident_state(mjg_context* c)
     }
 }
 
-// the per-system data that depends on topology only (molecules, exclusion
-// lists), computed once in the edge order the reference's local force field
-// writes the topology, after which the local terms are put in order of their
-// smallest particle (the order the bonded kernel walks them in)
-void derive(HostSystem& s)
+// the topology graph of a system: every local term's connections, then the
+// explicit ones (LocalForceField::write_topology order)
+TopologyGraph topology_of(const HostSystem& s, std::map<std::string, int>& kinds)
 {
-    if(s.derived) {return;}
-    std::map<std::string, int> kinds;
-    const int bond_kind = kind_id(kinds, "bond");
     TopologyGraph topo(s.n);
     auto add_edges = [&](const HostLocal& L, int arity) {
         if(L.kind.empty() || L.kind == "none") {return;}
@@ -516,6 +511,19 @@ void derive(HostSystem& s)
     add_edges(s.angle, 3);
     add_edges(s.dihd, 4);
     for(const auto& e : s.connections) {topo.add(e.second.first, e.second.second, kind_id(kinds, e.first));}
+    return topo;
+}
+
+// the per-system data that depends on topology only (molecules, exclusion
+// lists), computed once in the edge order the reference's local force field
+// writes the topology, after which the local terms are put in order of their
+// smallest particle (the order the bonded kernel walks them in)
+void derive(HostSystem& s)
+{
+    if(s.derived) {return;}
+    std::map<std::string, int> kinds;
+    const int bond_kind = kind_id(kinds, "bond");
+    const TopologyGraph topo = topology_of(s, kinds);
     const std::vector<int64_t> m = topo.molecules(bond_kind);
     s.mol_local.assign(m.begin(), m.end());
     for(int g = 0; g < NGLOBAL; ++g)
@@ -1991,6 +1999,19 @@ int mjg_step_count(mjg_context* c, int sys, int64_t* steps)
     if(!steps) {throw Error(MJG_EINVAL, "steps is NULL");}
     download_sys(c);
     *steps = (int64_t)c->h_sys[s.arena_slot].step;
+    ABI_END(c)
+}
+
+int mjg_molecule_count(mjg_context* c, int sys, int64_t* count)
+{
+    ABI_BEGIN(c)
+    HostSystem& s = get_sys(c, sys);
+    if(!count) {throw Error(MJG_EINVAL, "count is NULL");}
+    std::map<std::string, int> kinds;
+    const int bond_kind = kind_id(kinds, "bond");
+    int64_t nmol = 0;
+    for(const int64_t m : topology_of(s, kinds).molecules(bond_kind)) {nmol = std::max<int64_t>(nmol, m + 1);}
+    *count = nmol;
     ABI_END(c)
 }
 

@@ -212,6 +212,12 @@ class Engine:
         self._c(self.lib.mjg_step_count(self.ctx, sid, C.byref(c)))
         return c.value
 
+    def molecule_count(self, sid: int) -> int:
+        """Molecules of a system (groups joined by "bond" connections)."""
+        c = C.c_int64()
+        self._c(self.lib.mjg_molecule_count(self.ctx, sid, C.byref(c)))
+        return c.value
+
     def device_bytes(self) -> int:
         c = C.c_int64()
         self._c(self.lib.mjg_device_bytes(self.ctx, C.byref(c)))

@@ -6,7 +6,9 @@ does, for the subset of the schema that this library runs, and returns an
 ready for :meth:`Engine.add_system`:
 
 * ``[files]``: ``input.path`` (where included files are looked up;
-  input/read_path.hpp:25-52), ``output.prefix/path/format``;
+  input/read_path.hpp:25-52), ``output.prefix``, ``output.path`` and
+  ``output.format`` (``"xyz"``, ``"dcd"``, ``"trr"`` or an array of them;
+  :mod:`mjolnir_b200.observers`);
 * ``include = "f.toml"`` / ``["a.toml", ...]`` in any table, merged into it
   (input/utility.hpp:244-318), and ``file_name`` tables
   (input/read_table_from_file.hpp:38-91);
@@ -83,11 +85,20 @@ class Input:
     save_step: int
     seed: int
     output_prefix: str
-    output_path: str
-    output_format: str
+    output_path: str                # ends with "/" (input/read_path.hpp:56-75)
+    output_formats: list            # "xyz" | "dcd" | "trr", in input order
     input_path: str
     schedule: Optional[tuple] = None   # SimulatedAnnealing: (first, last, each_step)
     checkpoint_step: int = 0           # checkpoint interval (default: save_step)
+    names: Optional[list] = None       # particle names (default "X")
+    groups: Optional[list] = None      # particle groups (default "NONE")
+    attributes: Optional[dict] = None  # [[systems]] attributes as given (temperature, ionic_strength, ...)
+
+    @property
+    def file_prefix(self) -> str:
+        """output path + prefix, the stem of every output file
+        (input/read_observer.hpp:68-74)."""
+        return self.output_path + self.output_prefix
 
 
 # ------------------------------------------------------------------ helpers
@@ -275,7 +286,7 @@ def _system(sysd, boundary):
     mass = np.empty(n)
     has_vel = "velocity" in parts[0] or "vel" in parts[0]
     vel = np.zeros((n, 3))
-    groups = set()
+    names, groups = [], []
     for i, p in enumerate(parts):
         _check_keys(p, {"mass", "m", "position", "pos", "velocity", "vel", "name", "group"}, f"particle {i}")
         mass[i] = float(p["m"] if "m" in p else p["mass"])
@@ -285,7 +296,8 @@ def _system(sysd, boundary):
             raise InputError("read_system: give velocity for all particles or for none")
         if pv:
             vel[i] = p["vel"] if "vel" in p else p["velocity"]
-        groups.add(p.get("group", "NONE"))
+        names.append(str(p.get("name", "X")))          # read_system.hpp:276-277
+        groups.append(str(p.get("group", "NONE")))
     attrs = sysd.get("attributes", {})
     shape = sysd.get("boundary_shape", {})
     lower = upper = (0.0, 0.0, 0.0)
@@ -297,7 +309,7 @@ def _system(sysd, boundary):
             raise InputError("boundary_shape: upper must exceed lower on every axis")
     elif shape:
         raise InputError("boundary_shape must be empty for an Unlimited boundary")
-    return pos, vel, mass, has_vel, attrs, lower, upper
+    return pos, vel, mass, has_vel, attrs, lower, upper, names, groups
 
 
 def _ignore(g, where):
@@ -466,6 +478,14 @@ def load(path: str) -> Input:
     if not input_path.endswith("/"):
         input_path += "/"
     out = files.get("output", {})
+    out_path = str(out.get("path", "./"))
+    if not out_path.endswith("/"):
+        out_path += "/"
+    fmt = out.get("format", "xyz")                 # read_observer.hpp:17-96: a string or an array
+    formats = [fmt] if isinstance(fmt, str) else list(fmt)
+    for f in formats:
+        if f not in ("xyz", "dcd", "trr"):
+            raise InputError(f'files.output.format "{f}": one of "xyz", "dcd" and "trr" is expected')
     _expand_include(root, input_path, base_dir)
     _units(root)
     sim = _from_file(root.get("simulator", {}), "simulator", input_path, base_dir)
@@ -487,9 +507,10 @@ def load(path: str) -> Input:
             raise InputError("the checkpoint's boundary does not match [simulator] boundary_type")
         pos, vel, mass, has_vel = ck["pos"], ck["vel"], ck["mass"], True
         attrs, lower, upper = ck["attributes"], ck["lower"], ck["upper"]
+        names, groups = ck["names"], ck["groups"]
     else:
         sysd = _from_file(first, "systems", input_path, base_dir)
-        pos, vel, mass, has_vel, attrs, lower, upper = _system(sysd, boundary)
+        pos, vel, mass, has_vel, attrs, lower, upper, names, groups = _system(sysd, boundary)
     n = pos.shape[0]
     temperature = float(attrs.get("temperature", 300.0))
     ionic = float(attrs.get("ionic_strength", 0.1))
@@ -546,8 +567,9 @@ def load(path: str) -> Input:
     return Input(desc=desc, simulator=sim["type"], schedule=schedule, precision=prec, parallelism=par,
                  total_step=int(sim["total_step"]), save_step=int(sim["save_step"]), seed=seed,
                  checkpoint_step=int(sim.get("checkpoint_step", sim["save_step"])),
-                 output_prefix=str(out.get("prefix", "mjolnir")), output_path=str(out.get("path", "./")),
-                 output_format=str(out.get("format", "xyz")), input_path=input_path)
+                 output_prefix=str(out.get("prefix", "mjolnir")), output_path=out_path,
+                 output_formats=formats, input_path=input_path, names=names, groups=groups,
+                 attributes={str(k): float(v) for k, v in attrs.items()})
 
 
 # ------------------------------------------------------------------ writer

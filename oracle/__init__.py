@@ -361,6 +361,9 @@ def _ref_lib():
         lib.ref_max_threads.restype = C.c_int
         lib.ref_save_msgpack.restype = C.c_int
         lib.ref_save_msgpack.argtypes = [C.c_void_p, C.c_char_p]
+        lib.ref_observe.restype = C.c_int
+        lib.ref_observe.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_longlong, C.c_longlong,
+                                    C.c_double]
         lib.ref_load_msgpack.restype = C.c_longlong
         lib.ref_load_msgpack.argtypes = [C.c_char_p, C.c_int, C.c_longlong, _f64p, _f64p, _f64p, _f64p,
                                          _f64p, _f64p, _f64p, _f64p]
@@ -432,6 +435,14 @@ class Reference(_Common):
         prefix + "_system.msg"."""
         if self.lib.ref_save_msgpack(self._h, prefix.encode()):
             raise RuntimeError("ref_save_msgpack: " + self.lib.ref_last_error().decode())
+
+    def observe(self, prefix: str, formats, total_step: int, save_step: int, dt: float):
+        """Runs total_step steps as MolecularDynamicsSimulator does, with the
+        reference's own observers of `formats` ("xyz", "dcd", "trr") and the
+        energy observer writing under `prefix` (call initialize() first)."""
+        mask = sum({"xyz": 1, "dcd": 2, "trr": 4}[f] for f in formats)
+        if self.lib.ref_observe(self._h, prefix.encode(), mask, total_step, save_step, dt):
+            raise RuntimeError("ref_observe: " + self.lib.ref_last_error().decode())
 
     @staticmethod
     def load_msgpack(path: str, periodic: bool, n_max: int = 1 << 22) -> dict:

@@ -27,6 +27,10 @@
 #include <mjolnir/core/Unit.hpp>
 #include <mjolnir/core/MsgPackSaver.hpp>
 #include <mjolnir/core/MsgPackLoader.hpp>
+#include <mjolnir/core/XYZObserver.hpp>
+#include <mjolnir/core/DCDObserver.hpp>
+#include <mjolnir/core/TRRObserver.hpp>
+#include <mjolnir/core/EnergyObserver.hpp>
 #include <mjolnir/core/BAOABLangevinIntegrator.hpp>
 #include <mjolnir/core/VelocityVerletIntegrator.hpp>
 #include <mjolnir/core/UnderdampedLangevinIntegrator.hpp>
@@ -86,6 +90,8 @@ void set_units_once()
     phys_type::set_length_to_m(unit_type::angstrom_to_m());
     phys_type::set_L_to_volume(1e-3 * std::pow(unit_type::m_to_angstrom(), 3));
     phys_type::set_volume_to_L(1e+3 * std::pow(unit_type::angstrom_to_m(), 3));
+    phys_type::set_energy_unit("kcal/mol");
+    phys_type::set_length_unit("angstrom");
 }
 
 struct RefSimBase
@@ -100,6 +106,8 @@ struct RefSimBase
     virtual void total_force(double* force) = 0;
     virtual double total_energy() = 0;
     virtual void save_msgpack(const std::string& prefix) = 0;
+    virtual void observe(const std::string& prefix, int formats, long long total_step,
+                         long long save_step, double dt) = 0;
 };
 
 template<typename coordT>
@@ -533,6 +541,28 @@ struct RefSim final : public RefSimBase
                          : vv->step(time, *sys, ff, rng);
         }
     }
+    // MolecularDynamicsSimulator::initialize / step / finalize
+    // (core/MolecularDynamicsSimulator.hpp:72-125) with the observers that
+    // read_observer builds (input/read_observer.hpp:17-96): formats bit 0 xyz,
+    // bit 1 dcd, bit 2 trr; the energy file always.  The integrator must have
+    // been initialised.
+    void observe(const std::string& prefix, int formats, long long total_step,
+                 long long save_step, double dt) override
+    {
+        std::vector<std::unique_ptr<ObserverBase<traitsT>>> obs;
+        if(formats & 1) {obs.push_back(make_unique<XYZObserver<traitsT>>(prefix));}
+        if(formats & 2) {obs.push_back(make_unique<DCDObserver<traitsT>>(prefix));}
+        if(formats & 4) {obs.push_back(make_unique<TRRObserver<traitsT>>(prefix));}
+        obs.push_back(make_unique<EnergyObserver<traitsT>>(prefix));
+        for(auto& o : obs) {o->initialize(total_step, save_step, dt, *sys, ff);}
+        for(long long st = 0; st < total_step; ++st)
+        {
+            if(st % save_step == 0) {for(auto& o : obs) {o->output(st, dt, *sys, ff);}}
+            run(1);
+        }
+        for(auto& o : obs) {o->output(total_step, dt, *sys, ff);}
+        for(auto& o : obs) {o->finalize(total_step, dt, *sys, ff);}
+    }
     // MsgPackSaver::save(System) writes prefix + "_system.msg"
     void save_msgpack(const std::string& prefix) override
     {
@@ -655,6 +685,21 @@ void ref_total_force(void* h, double* force) {static_cast<RefSimBase*>(h)->total
 double ref_total_energy(void* h) {return static_cast<RefSimBase*>(h)->total_energy();}
 
 // The reference's checkpoint writer on the current system state.
+int ref_observe(void* h, const char* prefix, int formats, long long total_step,
+                long long save_step, double dt)
+{
+    try
+    {
+        static_cast<RefSimBase*>(h)->observe(prefix, formats, total_step, save_step, dt);
+        return 0;
+    }
+    catch(const std::exception& e)
+    {
+        g_error = e.what();
+        return -1;
+    }
+}
+
 int ref_save_msgpack(void* h, const char* prefix)
 {
     try

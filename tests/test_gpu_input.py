@@ -18,7 +18,8 @@ def test_toml_run_matches_direct(tmp_path):
     text = open(path).read().replace('output.path = "./"', f'output.path = "{tmp_path}/"')
     open(path, "w").write(text)
     res = run(path, precision="mixed")
-    head = open(res["energy_file"]).readline()
+    unit_line, head = open(res["energy_file"]).readlines()[:2]
+    assert unit_line == "# unit of length : angstrom, unit of energy : kcal/mol\n"
     assert head.split() == ["#", "timestep", "BondLength:Harmonic", "BondAngle:Harmonic",
                             "DihedralAngle:Cosine", "GlobalPairExcludedVolume", "Pair:DebyeHuckel",
                             "kinetic_energy", "attribute:ionic_strength", "attribute:temperature"]
@@ -69,3 +70,41 @@ def test_checkpoint_restart_is_bit_exact(desc, tmp_path):
     e2.close()
     for a, b in zip(got, ref):
         assert np.array_equal(a, b)
+
+
+def test_runner_writes_dcd_and_trr(tmp_path):
+    """format = ["xyz", "dcd", "trr"]: every file is written, the DCD frames
+    are the engine's states in single precision and the last TRR frame is
+    the engine's final state (mixed form: the chunking of the run does not
+    change a bit)."""
+    import struct
+    d = S.bead_fluid(n=1500, density=0.003, seed=25, dt=0.2)
+    path = str(tmp_path / "f.toml")
+    I.dump(d, path, total_step=30, save_step=10, prefix="f")
+    text = open(path).read().replace('output.path = "./"', f'output.path = "{tmp_path}/"')
+    text = text.replace('output.format = "xyz"', 'output.format = ["xyz", "dcd", "trr"]')
+    open(path, "w").write(text)
+    res = run(path, precision="mixed")
+    assert res["formats"] == ["xyz", "dcd", "trr"]
+    e = Engine("mixed")
+    sid = e.add_system(d)
+    e.commit()
+    e.step(30)
+    p, v, f = e.state(sid)
+    nmol = e.molecule_count(sid)
+    e.close()
+    raw = open(res["trr"], "rb").read()
+    title = str(tmp_path / "f").encode()
+    frame = 12 + len(title) + 52 + 16 + 72 + 3 * 24 * d.n
+    assert len(raw) == 4 * frame                       # steps 0, 10, 20, 30
+    last = raw[3 * frame:]
+    assert struct.unpack("<i", last[12 + len(title) + 44:12 + len(title) + 48])[0] == 30
+    data = np.frombuffer(last[12 + len(title) + 52 + 16 + 72:], dtype="<f8").reshape(3, d.n, 3)
+    assert np.array_equal(data[0], p) and np.array_equal(data[1], v) and np.array_equal(data[2], f)
+    dcd = open(res["dcd"], "rb").read()
+    assert nmol == 1                                 # the fluid's single-molecule trick
+    assert struct.unpack("<5i", dcd[8:28]) == (4, 0, 10, 30, d.n)   # the input file has no bonds
+    tail = dcd[-3 * (4 * d.n + 8):]
+    for k in range(3):
+        xs = np.frombuffer(tail[k * (4 * d.n + 8) + 4:(k + 1) * (4 * d.n + 8) - 4], dtype="<f4")
+        assert np.array_equal(xs, p[:, k].astype(np.float32))
