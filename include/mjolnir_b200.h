@@ -246,8 +246,10 @@ MJG_API int mjg_context_get_stream(mjg_context* ctx, void** stream);
 /* Average duration in milliseconds of one launch of a term's force kernel
  * (pair kernel for MJG_TERM_EXV/DH/LJ, bonded kernel otherwise) on the
  * current lists over `reps` launches, each timed with CUDA events on the
- * context's stream after a 256 MiB write has evicted L2; the integrator's
- * forces are not touched.  Allocates and frees the 256 MiB buffer. */
+ * context's stream after a 256 MiB write has evicted L2 and a 256 MiB read
+ * of another buffer has replaced the written lines with clean ones; the
+ * integrator's forces are not touched.  Allocates and frees the two
+ * buffers. */
 MJG_API int mjg_time_kernel(mjg_context* ctx, int term, int reps, double* ms_per_launch);
 /* Performance knobs of a global term (they change no result in the mixed
  * form, whose force sums are exact and order independent):

@@ -356,11 +356,16 @@ int default_tpp(int max_count)
     return 1;
 }
 
+// words per slot the neighbour buffer holds for capacity cap: at least 16
+// (the widest block of the blocked layout), because the force launches read
+// a slot's first block before they know its length
+size_t list_words(int cap) {return (size_t)std::max(cap, 16);}
+
 // (re)allocates the neighbour arrays of term g for capacity cap
 void alloc_lists(mjg_context* c, int g, int cap)
 {
     TermDev& T = c->term[g];
-    T.nbr.alloc(sizeof(int) * (size_t)cap * (size_t)(T.t.np > 0 ? T.t.np : 1));
+    T.nbr.alloc(sizeof(int) * list_words(cap) * (size_t)(T.t.np > 0 ? T.t.np : 1));
     T.t.nbr = T.nbr.as<int>();
     T.t.cap = cap;
     T.cap_alloc = cap;
@@ -1033,6 +1038,7 @@ void commit(mjg_context* c)
     a.staging = c->d_staging.as<double>();
     a.mol = c->d_mol.as<int>();
     a.accel = any_aux ? c->d_accel.as<double4>() : nullptr;
+    for(int id : ids) {a.any_frozen |= c->sys[id].frozen ? 1 : 0;}
 
     for(int g = 0; g < NGLOBAL; ++g)
     {
@@ -1135,9 +1141,9 @@ void commit(mjg_context* c)
         // keep the list capacity of the previous arena when the buffer still
         // holds it; rebuild_all grows it where needed
         const int keep = T.cap_alloc;
-        if(keep > 0 && T.nbr.cap >= sizeof(int) * (size_t)keep * (size_t)np)
+        if(keep > 0 && T.nbr.cap >= sizeof(int) * list_words(keep) * (size_t)np)
         {
-            T.nbr.bytes = sizeof(int) * (size_t)keep * (size_t)np;
+            T.nbr.bytes = sizeof(int) * list_words(keep) * (size_t)np;
             t.nbr = T.nbr.as<int>();
             t.cap = keep;
             if(!T.tpp_fixed) {t.tpp = prev_tpp;}
@@ -1545,6 +1551,13 @@ int mjg_system_freeze(mjg_context* c, int sys, int frozen)
         c->h_sys[s.arena_slot].frozen = s.frozen ? 1 : 0;
         upload_sys(c);
         CK(cudaStreamSynchronize(c->stream));
+        int any = 0;
+        for(const auto& h : c->h_sys) {any |= h.frozen;}
+        if(any != c->arena.any_frozen)     // the captured launches carry the flag
+        {
+            c->arena.any_frozen = any;
+            release_graph(c);
+        }
     }
     ABI_END(c)
 }
@@ -2048,11 +2061,16 @@ int mjg_time_kernel(mjg_context* c, int term, int reps, double* ms)
     Arena a = c->arena;
     a.force = c->d_force_scratch.p;
     // each launch is timed on its own, after a write larger than L2 has
-    // evicted its inputs, as in a step where the other kernels run between
-    // two launches of this one
+    // evicted its inputs (as in a step where the other kernels run between
+    // two launches of this one) and a read of another buffer larger than L2
+    // has replaced the written lines, so that the launch starts with a clean
+    // L2 and does not pay for writing back the flush
     const size_t flush_bytes = (size_t)256 << 20;
-    DevBuf flush;
+    DevBuf flush, sweep, sink;
     flush.alloc(flush_bytes);
+    sweep.alloc(flush_bytes);
+    sink.alloc(sizeof(int));
+    CK(cudaMemsetAsync(sweep.p, 0, flush_bytes, c->stream));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -2065,6 +2083,7 @@ int mjg_time_kernel(mjg_context* c, int term, int reps, double* ms)
     for(int r = 0; r < reps; ++r)
     {
         CK(cudaMemsetAsync(flush.p, r & 0xff, flush_bytes, c->stream));
+        launch_read_sweep(sweep.p, flush_bytes, sink.as<int>(), c->stream);
         CK(cudaEventRecord(e0, c->stream));
         once(false);
         CK(cudaEventRecord(e1, c->stream));

@@ -59,8 +59,10 @@ __device__ __forceinline__ void underdamped_close(const SysDev& S, long long i, 
 // the first half of an UnderdampedLangevin or G-JF step), force reset and the
 // per-system largest squared displacement.  With KICK the previous step's
 // closing half is applied first, as separate rounding steps, so that
-// consecutive steps of a chunk share one pass.
-template<int PREC, bool KICK>
+// consecutive steps of a chunk share one pass.  AUX: the arena holds
+// UnderdampedLangevin or G-JF systems (their branches cost registers, and
+// occupancy, in the BAOAB / velocity-Verlet arenas that have none).
+template<int PREC, bool KICK, bool AUX>
 __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
 {
     const long long i = (long long)blockIdx.x * TPB + threadIdx.x;
@@ -75,7 +77,7 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
         const double4 c = a.coef[i];     // per integrator: see Arena::coef
         double fx, fy, fz;
         load_force<PREC>(a.force, i, fx, fy, fz);
-        const bool uld = S.integrator == I_UNDERDAMPED;
+        const bool uld = AUX && S.integrator == I_UNDERDAMPED;
         if(KICK && !uld)
         {
             v.x = __dadd_rn(v.x, __dmul_rn(c.x, fx));
@@ -103,7 +105,7 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
             v.y = __dadd_rn(v.y, __dmul_rn(sa, acc.y));
             v.z = __dadd_rn(v.z, __dmul_rn(sa, acc.z));
         }
-        else if(S.integrator == I_GJF)   // core/GJFNVTLangevinIntegrator.hpp:183-204
+        else if(AUX && S.integrator == I_GJF)   // core/GJFNVTLangevinIntegrator.hpp:183-204
         {
             double r0, r1, r2;
             gaussian3(S.seed, (unsigned long long)(i - S.off), S.step, r0, r1, r2);
@@ -336,15 +338,21 @@ inline unsigned blocks(long long n) {return (unsigned)((n + TPB - 1) / TPB);}
 void launch_integrate_first(const Arena& a, cudaStream_t s, bool kick)
 {
     if(a.n == 0) {return;}
+    const bool aux = a.accel != nullptr;
+    const int nb = (int)blocks(a.n);
     if(a.precision == P_FP64)
     {
-        if(kick) {k_integrate_first<P_FP64, true ><<<blocks(a.n), TPB, 0, s>>>(a);}
-        else     {k_integrate_first<P_FP64, false><<<blocks(a.n), TPB, 0, s>>>(a);}
+        if(aux) {if(kick) {k_integrate_first<P_FP64, true,  true ><<<nb, TPB, 0, s>>>(a);}
+                 else     {k_integrate_first<P_FP64, false, true ><<<nb, TPB, 0, s>>>(a);}}
+        else    {if(kick) {k_integrate_first<P_FP64, true,  false><<<nb, TPB, 0, s>>>(a);}
+                 else     {k_integrate_first<P_FP64, false, false><<<nb, TPB, 0, s>>>(a);}}
     }
     else
     {
-        if(kick) {k_integrate_first<P_MIXED, true ><<<blocks(a.n), TPB, 0, s>>>(a);}
-        else     {k_integrate_first<P_MIXED, false><<<blocks(a.n), TPB, 0, s>>>(a);}
+        if(aux) {if(kick) {k_integrate_first<P_MIXED, true,  true ><<<nb, TPB, 0, s>>>(a);}
+                 else     {k_integrate_first<P_MIXED, false, true ><<<nb, TPB, 0, s>>>(a);}}
+        else    {if(kick) {k_integrate_first<P_MIXED, true,  false><<<nb, TPB, 0, s>>>(a);}
+                 else     {k_integrate_first<P_MIXED, false, false><<<nb, TPB, 0, s>>>(a);}}
     }
     note_launches(1);
 }
@@ -416,6 +424,28 @@ void launch_clear_energy(const Arena& a, cudaStream_t s)
 {
     if(a.nsys == 0) {return;}
     k_clear_energy<<<(a.nsys + 127) / 128, 128, 0, s>>>(a);
+    note_launches(1);
+}
+
+// reads `n` int4 words and keeps one word of the result (only when it takes
+// an impossible value), so that every line read stays clean in L2
+__global__ void k_read_sweep(const int4* __restrict__ p, long long n, int* sink)
+{
+    int acc = 0;
+    for(long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+        k += (long long)gridDim.x * blockDim.x)
+    {
+        const int4 w = __ldcg(p + k);
+        acc ^= w.x ^ w.y ^ w.z ^ w.w;
+    }
+    if(acc == 0x7fffffff && sink) {*sink = acc;}
+}
+
+void launch_read_sweep(const void* p, size_t bytes, int* sink, cudaStream_t s)
+{
+    const long long n = (long long)(bytes / sizeof(int4));
+    if(n == 0) {return;}
+    k_read_sweep<<<148 * 8, 256, 0, s>>>(static_cast<const int4*>(p), n, sink);
     note_launches(1);
 }
 

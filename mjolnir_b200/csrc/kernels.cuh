@@ -10,6 +10,7 @@ struct Arena {
     int       precision;        // Precision
     long long n;                // particles
     int       nsys;
+    int       any_frozen;       // some system is frozen (kernels read the per-system flag only then)
     SysDev*   sys;              // [nsys]
     double4*  pos;
     double4*  vel;
@@ -121,6 +122,9 @@ void launch_local(const Arena& a, const LocalArrays& l, int which_mask, bool nee
 void launch_clear_energy(const Arena& a, cudaStream_t s);
 void launch_count_cut(const Arena& a, int g, TermArrays& t, int sys, unsigned long long* out,
                       cudaStream_t s);
+// reads `bytes` (a multiple of 16) at p, leaving clean lines in L2 (timing
+// aid: evicts dirty lines after a flush write)
+void launch_read_sweep(const void* p, size_t bytes, int* sink, cudaStream_t s);
 // coef[first + k].z = noise[k] (the Langevin noise coefficient) for k < count
 void launch_set_noise(const Arena& a, const double* noise, long long first, long long count,
                       cudaStream_t s);

@@ -415,8 +415,8 @@ __global__ void __launch_bounds__(TPB) k_local(Arena a, LocalArrays l, int mask)
         for(long long base = b0; base < b1; base += TPB)
         {
             const long long b = base + threadIdx.x;
-            if(PREC == P_FP64) {do_bond<PREC, NF, NE>(a, l, b, b < b1 && !a.sys[l.bond_sys[b]].frozen, W);}
-            else               {do_bond_f32<PREC, NF, NE>(a, l, b, b < b1 && !a.sys[l.bond_sys[b]].frozen, W);}
+            if(PREC == P_FP64) {do_bond<PREC, NF, NE>(a, l, b, b < b1 && !(a.any_frozen && a.sys[l.bond_sys[b]].frozen), W);}
+            else               {do_bond_f32<PREC, NF, NE>(a, l, b, b < b1 && !(a.any_frozen && a.sys[l.bond_sys[b]].frozen), W);}
         }
     }
     if(mask & 2)
@@ -425,8 +425,8 @@ __global__ void __launch_bounds__(TPB) k_local(Arena a, LocalArrays l, int mask)
         for(long long base = b0; base < b1; base += TPB)
         {
             const long long b = base + threadIdx.x;
-            if(PREC == P_FP64) {do_angle<PREC, NF, NE>(a, l, b, b < b1 && !a.sys[l.angle_sys[b]].frozen, W);}
-            else               {do_angle_f32<PREC, NF, NE>(a, l, b, b < b1 && !a.sys[l.angle_sys[b]].frozen, W);}
+            if(PREC == P_FP64) {do_angle<PREC, NF, NE>(a, l, b, b < b1 && !(a.any_frozen && a.sys[l.angle_sys[b]].frozen), W);}
+            else               {do_angle_f32<PREC, NF, NE>(a, l, b, b < b1 && !(a.any_frozen && a.sys[l.angle_sys[b]].frozen), W);}
         }
     }
     if(mask & 4)
@@ -435,8 +435,8 @@ __global__ void __launch_bounds__(TPB) k_local(Arena a, LocalArrays l, int mask)
         for(long long base = b0; base < b1; base += TPB)
         {
             const long long b = base + threadIdx.x;
-            if(PREC == P_FP64) {do_dihedral<PREC, NF, NE>(a, l, b, b < b1 && !a.sys[l.dihd_sys[b]].frozen, W);}
-            else               {do_dihedral_f32<PREC, NF, NE>(a, l, b, b < b1 && !a.sys[l.dihd_sys[b]].frozen, W);}
+            if(PREC == P_FP64) {do_dihedral<PREC, NF, NE>(a, l, b, b < b1 && !(a.any_frozen && a.sys[l.dihd_sys[b]].frozen), W);}
+            else               {do_dihedral_f32<PREC, NF, NE>(a, l, b, b < b1 && !(a.any_frozen && a.sys[l.dihd_sys[b]].frozen), W);}
         }
     }
     if(NF)

@@ -71,6 +71,17 @@ template<> struct Acc<P_MIXED>
         ovf |= !(m < FX_LIMIT * FX_INV_SCALE);
         x += fx_from_double(fx); y += fx_from_double(fy); z += fx_from_double(fz);
     }
+    // the same from FP32 factors (the mixed form's plain potentials): f = c r
+    // rounded once to FP32, then to the fixed-point grid
+    __device__ __forceinline__ void add_f(float c, float dx, float dy, float dz, bool& ovf)
+    {
+        const float fx = c * dx, fy = c * dy, fz = c * dz;
+        const float m = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));
+        ovf |= !(m < (float)(FX_LIMIT * FX_INV_SCALE));
+        x += __float2ll_rn(fx * (float)FX_SCALE);
+        y += __float2ll_rn(fy * (float)FX_SCALE);
+        z += __float2ll_rn(fz * (float)FX_SCALE);
+    }
     __device__ __forceinline__ void shfl_add(int o)
     {
         x += __shfl_xor_sync(0xffffffffu, x, o);
@@ -293,7 +304,7 @@ struct PairEval {
             const double sigma = pi.w + pj.w;
             const double sigma_sq = sigma * sigma;
             const bool in = !(sigma_sq * crsq < l2);
-            if(PREC == P_FP64)
+            if constexpr(PREC == P_FP64)
             {
                 if(!in) {return;}
                 const double rcp = 1.0 / l2;
@@ -310,14 +321,14 @@ struct PairEval {
                 const float s2 = (float)sigma_sq * rcp;
                 const float s6 = s2 * s2 * s2;
                 const float cf = in ? -eps12f * s6 * s6 * rcp : 0.0f;
-                if(NF) {acc.add((double)cf, dx, dy, dz, ovf);}
+                if constexpr(NF) {acc.add_f(cf, (float)dx, (float)dy, (float)dz, ovf);}
                 if(count_e && in) {energy += (double)(epsf * (s6 * s6 - coefcf));}
             }
         }
         else if(G == G_DH)
         {
             const bool in = l2 < abs_cut_sq;
-            if(PREC == P_FP64)
+            if constexpr(PREC == P_FP64)
             {
                 if(!in) {return;}
                 const double qq = (qi * pj.w) * inv4pi;     // symmetric in i, j
@@ -337,7 +348,7 @@ struct PairEval {
                 const float l  = l2f * rl;
                 const float ex = __expf(-l * invdf);
                 const float cf = in ? -qq * (debf + l) * invdf * (rl * rl) * ex * rl : 0.0f;
-                if(NF) {acc.add((double)cf, dx, dy, dz, ovf);}
+                if constexpr(NF) {acc.add_f(cf, (float)dx, (float)dy, (float)dz, ovf);}
                 if(count_e && in) {energy += (double)(qq * (ex * rl - coefcf));}
             }
         }
@@ -353,7 +364,7 @@ struct PairEval {
             }
             const double sigma_sq = sigma * sigma;
             if(sigma_sq * crsq < l2) {return;}
-            if(PREC == P_FP64)
+            if constexpr(PREC == P_FP64)
             {
                 const double rcp = 1.0 / l2;
                 const double s2 = sigma_sq * rcp;
@@ -367,7 +378,7 @@ struct PairEval {
                 const float s2 = (float)sigma_sq * rcp;
                 const float s6 = s2 * s2 * s2;
                 const float ef = (float)epsilon;
-                if(NF) {acc.add((double)(24.0f * ef * (s6 - 2.0f * s6 * s6) * rcp), dx, dy, dz, ovf);}
+                if constexpr(NF) {acc.add_f(24.0f * ef * (s6 - 2.0f * s6 * s6) * rcp, (float)dx, (float)dy, (float)dz, ovf);}
                 if(count_e) {energy += (double)(4.0f * ef * (s6 * s6 - s6 - coefcf));}
             }
         }
@@ -378,24 +389,43 @@ struct PairEval {
 // 1 keeps one partner in flight ahead of the pair being evaluated; 2 and 4
 // issue the batch's list words, then its coordinates, before evaluating any
 // of them (more loads in flight per thread, more registers).
+// A slot's system and the number of partners its force launch walks (0 in a
+// frozen system, which keeps its forces): the two loads are independent, the
+// system's flag is read once they arrive, and only when the arena has a
+// frozen system.
+struct SlotHead {
+    int sys;
+    int n;
+};
+__device__ __forceinline__ SlotHead slot_head(const Arena& a, const TermArrays& t, long long s)
+{
+    const int sys = t.slot_sys[s];
+    const int n = t.nnb[s];
+    return {sys, a.any_frozen && a.sys[sys].frozen ? 0 : n};
+}
+
 // Counting sort of a block's slots by their list length (in units of `per`
 // partners, 32 bins): returns the block-local index of the slot this group of
-// threads takes.  Slot numbering is unchanged; only which threads walk which
-// list.  Every thread of the block must call it.
+// threads takes, with that slot's head (read once by the group that loaded
+// it, handed over in shared memory).  Slot numbering is unchanged; only
+// which threads walk which list.  Every thread of the block must call it.
 template<int GROUPS>
 __device__ __forceinline__ int sorted_group(const Arena& a, const TermArrays& t, long long first_slot,
-                                            int group, bool leader, int per)
+                                            int group, bool leader, int per, SlotHead& head)
 {
     constexpr int NB = 32;
     __shared__ int bin_count[NB];
     __shared__ int perm[GROUPS];
+    __shared__ SlotHead heads[GROUPS];
     if(threadIdx.x < NB) {bin_count[threadIdx.x] = 0;}
-    __syncthreads();
     const long long s = first_slot + group;
-    int nb = 0;
-    if(leader && s < t.np && !a.sys[t.slot_sys[s]].frozen) {nb = (t.nnb[s] + per - 1) / per;}
+    SlotHead h{0, 0};
+    if(leader && s < t.np) {h = slot_head(a, t, s);}
+    __syncthreads();
+    const int nb = (h.n + per - 1) / per;
     const int bin = nb < NB - 1 ? nb : NB - 1;
     const int rank = leader ? atomicAdd(&bin_count[bin], 1) : 0;
+    if(leader) {heads[group] = h;}
     __syncthreads();
     if(threadIdx.x < 32)
     {
@@ -412,11 +442,16 @@ __device__ __forceinline__ int sorted_group(const Arena& a, const TermArrays& t,
     __syncthreads();
     if(leader) {perm[bin_count[bin] + rank] = group;}
     __syncthreads();
-    return perm[group];
+    const int g = perm[group];
+    head = heads[g];
+    return g;
 }
 
+// Both pair kernels are held to 64 registers (four 256-thread blocks per SM):
+// they wait on memory, and the occupancy is worth more than the few words
+// spilled in the widest variants.
 template<int PREC, int G, bool NF, bool NE, int TPP, bool PER, int UNR, bool SORT = false>
-__global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
+__global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
 {
     // TPP consecutive threads share one slot; lane lg walks partners lg,
     // lg + TPP, ... which the blocked list layout stores next to each other.
@@ -424,13 +459,15 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
     const long long gt = (long long)blockIdx.x * TPB + threadIdx.x;
     long long s = gt / TPP;
     const int lg = (int)(threadIdx.x % TPP);
+    SlotHead head{0, 0};
     if(SORT)
     {
         const long long first = (long long)blockIdx.x * (TPB / TPP);
-        s = first + sorted_group<TPB / TPP>(a, t, first, (int)(threadIdx.x / TPP), lg == 0, TPP * UNR);
+        s = first + sorted_group<TPB / TPP>(a, t, first, (int)(threadIdx.x / TPP), lg == 0, TPP * UNR, head);
     }
     const bool active = s < t.np;
-    const int sys = active ? t.slot_sys[s] : 0;
+    if(!SORT && active) {head = slot_head(a, t, s);}
+    const int sys = head.sys;
     double energy = 0.0;
     bool ovf = false;
     Acc<PREC> acc;
@@ -438,17 +475,20 @@ __global__ void __launch_bounds__(TPB) k_pair(Arena a, TermArrays t)
     {
         const PairEval<PREC, G, NF, NE, PER> eval(a, t, s, sys);
         const long long np = t.np;
-        const int n = eval.S->frozen ? 0 : t.nnb[s];       // a frozen system keeps its forces
+        const int n = head.n;
         const int* __restrict__ nbr = t.nbr + s * TPP + lg;
         const double4* __restrict__ pd = t.slot_pd;
         if(UNR == 1)
         {
             // software pipeline: the next partner's index and coordinates are
             // requested before the current pair is evaluated
+            // the first list word is read whatever the list's length (every
+            // slot owns cap >= TPP words), so that its load does not wait for
+            // the length; a word past the length is never used as an index
             int k = lg;
-            int q = 0;
+            int q = __ldg(nbr);
             double4 pj = make_double4(0.0, 0.0, 0.0, 0.0);
-            if(k < n) {q = __ldg(nbr + (long long)(k / TPP) * np * TPP); pj = pd[q];}
+            if(k < n) {pj = pd[q];}
             for(; k < n; k += TPP)
             {
                 const int kn = k + TPP;
@@ -533,26 +573,31 @@ __device__ __forceinline__ void load_block(const int* __restrict__ p, int (&q)[L
 // walk lists of about the same length; the slots themselves, and with them
 // the spatial order of the partners, stay where they are.
 template<int PREC, int G, bool PER, int L, bool SORT>
-__global__ void __launch_bounds__(TPB) k_pair_vec(Arena a, TermArrays t)
+__global__ void __launch_bounds__(TPB, 4) k_pair_vec(Arena a, TermArrays t)
 {
     long long s = (long long)blockIdx.x * TPB + threadIdx.x;
+    SlotHead head{0, 0};
     if(SORT)
     {
         const long long first = (long long)blockIdx.x * TPB;
-        s = first + sorted_group<TPB>(a, t, first, (int)threadIdx.x, true, L);
+        s = first + sorted_group<TPB>(a, t, first, (int)threadIdx.x, true, L, head);
     }
     if(s >= t.np) {return;}
-    const int sys = t.slot_sys[s];
+    if(!SORT) {head = slot_head(a, t, s);}
+    const int sys = head.sys;
     double energy = 0.0;
     bool ovf = false;
     Acc<PREC> acc;
     const PairEval<PREC, G, true, false, PER> eval(a, t, s, sys);
     const long long np = t.np;
-    const int n = eval.S->frozen ? 0 : t.nnb[s];       // a frozen system keeps its forces
+    const int n = head.n;
     const double4* __restrict__ pd = t.slot_pd;
     constexpr int W = L < 4 ? L : 4;                 // partners requested together
+    // the first block is read whatever the list's length (every slot owns
+    // cap >= L words), so that its load does not wait for the length; words
+    // past the length are never used as indices
     int q[L];
-    if(n > 0) {load_block<L>(t.nbr + s * L, q);}
+    load_block<L>(t.nbr + s * L, q);
     for(int k = 0; k < n; k += L)
     {
         int qn[L];
@@ -593,8 +638,7 @@ __global__ void __launch_bounds__(TPB) k_pair_warp(Arena a, TermArrays t)
     int n_my = 0;
     if(gt < t.np)
     {
-        const int sys = t.slot_sys[gt];
-        n_my = a.sys[sys].frozen ? 0 : t.nnb[gt];    // a frozen system keeps its forces
+        n_my = slot_head(a, t, gt).n;                // 0 in a frozen system
     }
     int incl = n_my;
 #pragma unroll

@@ -221,3 +221,34 @@ def polymer_batch(nsys: int = 256, nmin: int = 500, nmax: int = 20000, seed: int
                                 temperature=float(temps[k]), ionic_strength=float(ions[k]),
                                 dt=dt, gamma=gamma, margin=margin, seed=seed * 100003 + k))
     return out
+
+
+def dimers(n: int = 20000, k: float = 0.5, r0: float = 3.8, temperature: float = 300.0,
+           dt: float = 0.05, gamma: float = 1.0, integrator: str = "BAOAB", seed: int = 1) -> SystemDesc:
+    """`n` independent harmonic dimers (mass 1, E = k (r - r0)^2, random
+    orientations, 20 A apart on a line, no pair terms) for sampling tests:
+    the bond length samples P(r) ~ r^2 exp(-k (r - r0)^2 / kB T).  For
+    G-JFLangevin `gamma` is used as alpha (mass 1)."""
+    rng = np.random.default_rng(seed)
+    centers = np.stack([np.arange(n) * 20.0, np.zeros(n), np.zeros(n)], 1)
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    pos = np.empty((2 * n, 3))
+    pos[0::2] = centers - 0.5 * r0 * u
+    pos[1::2] = centers + 0.5 * r0 * u
+    m = np.ones(2 * n)
+    idx = np.stack([np.arange(0, 2 * n, 2), np.arange(1, 2 * n, 2)], 1).astype(np.int64)
+    return SystemDesc(pos=pos, vel=maxwell_boltzmann(rng, m, KB_KCAL * temperature), mass=m,
+                      temperature=temperature, bonds=(idx, np.full(n, k), np.full(n, r0)),
+                      integrator=integrator, dt=dt, gamma=np.full(2 * n, gamma), seed=seed)
+
+
+def dimer_length_cdf(r: np.ndarray, k: float, r0: float, temperature: float) -> np.ndarray:
+    """Cumulative Boltzmann distribution of a harmonic dimer's bond length at
+    `r` (numerical integral of r^2 exp(-k (r - r0)^2 / kB T))."""
+    beta = 1.0 / (KB_KCAL * temperature)
+    w = 12.0 / np.sqrt(beta * k)
+    grid = np.linspace(max(0.0, r0 - w), r0 + w, 400001)
+    p = grid * grid * np.exp(-beta * k * (grid - r0) ** 2)
+    c = np.concatenate([[0.0], np.cumsum(0.5 * (p[1:] + p[:-1]))])
+    return np.interp(r, grid, c / c[-1])
