@@ -367,7 +367,7 @@ def run_b200(args, ws, rank, local, pg):
     # DRAM bytes (read + write) of one launch from the ncu capture summarised
     # in profiles/k_pair_batch256_mixed.md, per slot of the captured launch,
     # scaled to this launch by its slots
-    ncu_bytes_per_slot = {"exv": 177.8e6 / 1563757, "dh": 117.3e6 / 312662}
+    ncu_bytes_per_slot = {"exv": 194.5e6 / 1563757, "dh": 118.8e6 / 312662}
     traffic = ncu_bytes_per_slot[dom] * k["slots"] if dom in ncu_bytes_per_slot else None
     local_ms = {t: eng.time_kernel(t, reps=20) for t in ("bond", "angle", "dihedral")}
     shape = eng.get_pair_schedule(dom), eng.get_threads_per_particle(dom), eng.get_pair_unroll(dom)

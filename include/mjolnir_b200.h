@@ -279,6 +279,14 @@ MJG_API int mjg_get_pair_unroll(mjg_context* ctx, int term, int* unroll);
  * counterpart in the reference. */
 MJG_API int mjg_set_pair_schedule(mjg_context* ctx, int term, int schedule);
 MJG_API int mjg_get_pair_schedule(mjg_context* ctx, int term, int* schedule);
+/* Lanes per particle of a global term's list build (8, 16 or 32): fewer
+ * lanes build several lists per warp at once, which pays when a particle has
+ * few candidates in its 27 neighbouring cells.  Unless set here, each commit
+ * picks it from the candidates an even filling of the grids would give
+ * (below 24: 8, below 64: 16, else 32).  The lists are the same in every
+ * case.  No counterpart in the reference. */
+MJG_API int mjg_set_build_lanes(mjg_context* ctx, int term, int lanes);
+MJG_API int mjg_get_build_lanes(mjg_context* ctx, int term, int* lanes);
 /* Sets the per-particle neighbour capacity of a global term's lists.  A
  * capacity below what a later rebuild needs is detected on the device, the
  * current mjg_step chunk is rolled back, the lists grow and the chunk runs

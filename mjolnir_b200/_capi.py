@@ -77,6 +77,8 @@ SIGNATURES = {
     "mjg_get_pair_unroll": (C.c_int, [_ctx, C.c_int, C.POINTER(C.c_int)]),
     "mjg_set_pair_schedule": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "mjg_get_pair_schedule": (C.c_int, [_ctx, C.c_int, C.POINTER(C.c_int)]),
+    "mjg_set_build_lanes": (C.c_int, [_ctx, C.c_int, C.c_int]),
+    "mjg_get_build_lanes": (C.c_int, [_ctx, C.c_int, C.POINTER(C.c_int)]),
     "mjg_set_margin": (C.c_int, [_ctx, C.c_int, C.c_double]),
     "mjg_exv_force_noalloc": (C.c_int, [C.c_int64, C.c_int, _f64p, _f64p, C.c_void_p, C.c_void_p,
                                         C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),

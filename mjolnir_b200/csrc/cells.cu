@@ -361,6 +361,147 @@ __global__ void __launch_bounds__(TPB) k_build_list(Arena a, int g, TermArrays t
     }
 }
 
+// The same list build with LPS lanes per slot (8 or 16): a warp builds 32 /
+// LPS lists at once, so that short candidate sequences (a few partners per
+// stencil) do not leave most of a warp idle while it waits on memory.  A
+// group's 27 stencil ranges go through shared memory; candidate k of the
+// flattened sequence belongs to the last stencil cell whose range starts at
+// or before k; the ordered compaction within the group keeps the serial
+// walk's output order, so the lists are the same word for word.
+template<int LPS>
+__global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArrays t)
+{
+    constexpr int GROUPS = TPB / LPS;              // slot groups per block
+    constexpr int WG = 32 / LPS;                   // slot groups per warp
+    __shared__ int c_start[GROUPS][27];
+    __shared__ int c_excl[GROUPS][28];             // exclusive prefix; [27] = total
+    const int n = t.work[0];
+    const int cap = t.cap;
+    const long long np = t.np;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = threadIdx.x / LPS, gl = threadIdx.x % LPS;
+    const unsigned full = 0xffffffffu;
+    const unsigned gmask = ((LPS == 32) ? full : ((1u << LPS) - 1u)) << (lane - gl);
+    const long long nwork = (long long)n * CHUNK;
+    const long long stride = (long long)gridDim.x * GROUPS;
+    // warp-uniform loop over rounds; group (lane / LPS) of the warp takes item base + lane / LPS
+    for(long long base = (long long)blockIdx.x * GROUPS + warp * WG; base < nwork; base += stride)
+    {
+        const long long item = base + lane / LPS;
+        bool valid = item < nwork;
+        int s = 0, sys = 0;
+        if(valid)
+        {
+            const int4 w = t.part_chunks[item / CHUNK];
+            s = w.y + (int)(item % CHUNK);
+            sys = w.x;
+            valid = s < w.z;
+        }
+        const SysDev& S = a.sys[sys];
+        const GlobalParams& G = S.g[g];
+        const bool periodic = S.boundary == B_PERIODIC;
+        const int dx_ = G.dims[0], dy_ = G.dims[1], dz_ = G.dims[2];
+        const bool wrap = periodic || G.hashed;
+        const double rl2 = G.rl2;
+        int i = 0;
+        bool lead_i = false;
+        double4 ri = make_double4(0.0, 0.0, 0.0, 0.0);
+        if(valid)
+        {
+            i = t.slot_particle[s];
+            lead_i = t.slot_lead[s] != 0;
+            ri = t.slot_pd[s];
+            const int cx = cell_coord(ri.x, G, 0);
+            const int cy = cell_coord(ri.y, G, 1);
+            const int cz = cell_coord(ri.z, G, 2);
+            for(int k = gl; k < 27; k += LPS)
+            {
+                int x = cx + k % 3 - 1, y = cy + (k / 3) % 3 - 1, z = cz + k / 9 - 1;
+                bool inside = true;
+                if(wrap)
+                {
+                    x = x < 0 ? x + dx_ : (x >= dx_ ? x - dx_ : x);
+                    y = y < 0 ? y + dy_ : (y >= dy_ ? y - dy_ : y);
+                    z = z < 0 ? z + dz_ : (z >= dz_ ? z - dz_ : z);
+                }
+                else if(x < 0 || y < 0 || z < 0 || x >= dx_ || y >= dy_ || z >= dz_) {inside = false;}
+                int cs = 0, cc = 0;
+                if(inside)
+                {
+                    const int cell = G.cell_off + x + dx_ * (y + dy_ * z);
+                    cs = t.cell_start[cell];
+                    cc = t.cell_count[cell];
+                }
+                c_start[grp][k] = cs;
+                c_excl[grp][k] = cc;
+            }
+        }
+        __syncwarp();
+        if(valid && gl == 0)
+        {
+            int run = 0;
+            for(int k = 0; k < 27; ++k) {const int c = c_excl[grp][k]; c_excl[grp][k] = run; run += c;}
+            c_excl[grp][27] = run;
+        }
+        __syncwarp();
+        const int total = valid ? c_excl[grp][27] : 0;
+        int tmax = total;
+#pragma unroll
+        for(int o = LPS; o < 32; o <<= 1) {tmax = max(tmax, __shfl_xor_sync(full, tmax, o));}
+        int count = 0;
+        for(int b = 0; b < tmax; b += LPS)
+        {
+            const int k = b + gl;
+            bool keep = false;
+            int q = 0;
+            if(k < total)
+            {
+                int lo = 0, hi = 26;                   // the last cell whose range starts at or before k
+                while(lo < hi)
+                {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if(c_excl[grp][mid] <= k) {lo = mid;} else {hi = mid - 1;}
+                }
+                q = c_start[grp][lo] + (k - c_excl[grp][lo]);
+                if(q != s)
+                {
+                    const double4 rj = t.slot_pd[q];
+                    double ddx = __dsub_rn(rj.x, ri.x);
+                    double ddy = __dsub_rn(rj.y, ri.y);
+                    double ddz = __dsub_rn(rj.z, ri.z);
+                    if(periodic)
+                    {
+                        ddx = min_image(ddx, S.halfw[0], S.width[0]);
+                        ddy = min_image(ddy, S.halfw[1], S.width[1]);
+                        ddz = min_image(ddz, S.halfw[2], S.width[2]);
+                    }
+                    const double l2 = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
+                    if(l2 < rl2)
+                    {
+                        const int j = t.slot_particle[q];
+                        const bool lead_lo = (i < j) ? lead_i : (t.slot_lead[q] != 0);
+                        keep = lead_lo && !is_excluded(a, g, G.ignore_mol, i < j ? i : j, i < j ? j : i);
+                    }
+                }
+            }
+            const unsigned m = __ballot_sync(full, keep) & gmask;
+            if(keep)
+            {
+                const int pos = count + __popc(m & ((1u << lane) - 1u));
+                if(pos < cap) {t.nbr[nbr_index(pos, s, np, t.tpp)] = q;}
+            }
+            count += __popc(m);
+        }
+        if(valid && gl == 0)
+        {
+            t.nnb[s] = count < cap ? count : cap;
+            atomicMax(t.max_count, count);
+            if(count > cap) {atomicOr(&a.sys[sys].status, ST_LIST_OVERFLOW);}
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void k_rebuild_done(Arena a, int g, TermArrays t, int forced)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -404,7 +545,9 @@ void launch_rebuild(const Arena& a, int g, TermArrays& t, int force_all, cudaStr
     k_cells_scatter<<<GRID, TPB, 0, s>>>(t, t.slot_particle);
     k_cells_sort  <<<GRID, TPB, 0, s>>>(t, t.slot_particle);
     k_slots_setup <<<GRID, TPB, 0, s>>>(a, t);
-    k_build_list  <<<GRID, TPB, 0, s>>>(a, g, t);
+    if(t.build_lanes == 8)       {k_build_list_sub<8> <<<GRID, TPB, 0, s>>>(a, g, t);}
+    else if(t.build_lanes == 16) {k_build_list_sub<16><<<GRID, TPB, 0, s>>>(a, g, t);}
+    else                         {k_build_list        <<<GRID, TPB, 0, s>>>(a, g, t);}
     k_rebuild_done<<<blocks(a.nsys, 128), 128, 0, s>>>(a, g, t, force_all);
     note_launches(9);
 }

@@ -142,6 +142,8 @@ struct TermDev {
     int schedule_choice = 0;     // force launch schedule (0 slot per threads, 1 warp-balanced,
                                  // 2 block-vector, 3 block-vector with length-sorted threads,
                                  // 4 slot per threads with length-sorted groups)
+    int build_lanes_choice = 32; // lanes per slot of the list build (8, 16, 32)
+    bool build_lanes_fixed = false;  // ... chosen by the caller (else from the expected candidates)
     TermArrays t{};
 };
 
@@ -1133,6 +1135,22 @@ void commit(mjg_context* c)
         t.tpp = T.tpp_fixed ? T.tpp_choice : 1;
         t.unroll = T.unroll_choice;
         t.schedule = T.schedule_choice;
+        if(!T.build_lanes_fixed)
+        {
+            // candidates per slot if the participants filled their grids
+            // evenly: 27 cells x participants per cell, weighted by slots
+            double cand = 0.0, slots = 0.0;
+            for(int k = 0; k < nsys; ++k)
+            {
+                const GlobalParams& G = hs[k].g[g];
+                if(!G.on || G.ncell == 0) {continue;}
+                cand += 27.0 * (double)G.nslot * (double)G.nslot / (double)G.ncell;
+                slots += (double)G.nslot;
+            }
+            const double per = slots > 0 ? cand / slots : 0.0;
+            T.build_lanes_choice = per < 24.0 ? 8 : (per < 64.0 ? 16 : 32);
+        }
+        t.build_lanes = T.build_lanes_choice;
         t.any_periodic = 0;
         for(int id : ids)
         {
@@ -2145,6 +2163,30 @@ int mjg_set_pair_schedule(mjg_context* c, int term, int schedule)
         T.t.schedule = schedule;
         release_graph(c);
     }
+    ABI_END(c)
+}
+
+int mjg_set_build_lanes(mjg_context* c, int term, int lanes)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "build lanes apply to global terms");}
+    if(lanes != 8 && lanes != 16 && lanes != 32) {throw Error(MJG_EINVAL, "lanes must be 8, 16 or 32");}
+    TermDev& T = c->term[term - MJG_TERM_EXV];
+    T.build_lanes_fixed = true;
+    T.build_lanes_choice = lanes;
+    if(T.t.build_lanes != lanes)
+    {
+        T.t.build_lanes = lanes;    // same lists, another kernel: recapture the step
+        release_graph(c);
+    }
+    ABI_END(c)
+}
+
+int mjg_get_build_lanes(mjg_context* c, int term, int* lanes)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !lanes) {throw Error(MJG_EINVAL, "bad query");}
+    *lanes = c->term[term - MJG_TERM_EXV].build_lanes_choice;
     ABI_END(c)
 }
 

@@ -47,6 +47,7 @@ struct TermArrays {
                                 // 3 = as 2 with a block's threads ordered by list length,
                                 // 4 = as 0 with a block's thread groups ordered by list length
     int        any_periodic;    // some system with this term has a periodic box
+    int        build_lanes;     // lanes per slot of the list build (8, 16 or 32)
     const int* part_particle;   // [np] global particle index
     const double* part_p0;      // [np] radius / charge / sigma
     const double* part_p1;      // [np] LJ epsilon

@@ -279,6 +279,17 @@ class Engine:
         self._c(self.lib.mjg_get_pair_schedule(self.ctx, t, C.byref(v)))
         return v.value
 
+    def set_build_lanes(self, term, lanes: int):
+        """Lanes per particle of the term's list build (8, 16 or 32)."""
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        self._c(self.lib.mjg_set_build_lanes(self.ctx, t, int(lanes)))
+
+    def get_build_lanes(self, term) -> int:
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        v = C.c_int()
+        self._c(self.lib.mjg_get_build_lanes(self.ctx, t, C.byref(v)))
+        return v.value
+
     def set_margin(self, term, margin: float):
         t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
         self._c(self.lib.mjg_set_margin(self.ctx, t, float(margin)))

@@ -284,3 +284,33 @@ def test_simulated_annealing_matches_oracle():
     assert np.abs(p - po).max() <= 1e-9
     assert np.abs(v - vo).max() <= 1e-8
     e.close()
+
+
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+@pytest.mark.parametrize("case", ["melt", "fluid"])
+def test_build_lanes_give_the_same_lists(case, lanes):
+    """Every lanes-per-particle choice of the list build gives the reference's
+    lists (a forced rebuild after dynamics) and, through the rebuilds during
+    the dynamics, the same trajectory bit for bit (mixed form)."""
+    if case == "melt":
+        d = S.polymer_melt(nchains=10, nbeads=50, radius=60.0, seed=52)
+    else:
+        d = S.bead_fluid(n=4000, density=0.003, seed=53, dt=0.3)
+    e, sid = engine_for(d, "mixed")
+    for t in ("exv", "dh"):
+        e.set_build_lanes(t, lanes)
+        assert e.get_build_lanes(t) == lanes
+    e.step(300)
+    assert e.rebuild_count(sid, "exv") >= 1
+    o = oracle.Oracle(d)
+    traj = e.state(sid)
+    e.rebuild()
+    p = e.positions(sid)
+    for t in ("exv", "dh"):
+        assert np.array_equal(e.neighbors(sid, t), o.neighbors(t, p)), (t, lanes)
+    e.close()
+    e32, sid32 = engine_for(d, "mixed")
+    e32.step(300)
+    for a, b in zip(traj, e32.state(sid32)):
+        assert np.array_equal(a, b), lanes
+    e32.close()
