@@ -86,6 +86,9 @@ struct SysDev {
     unsigned long long max_disp2;   // bits of a non-negative double (atomicMax)
     int    status;
     int    frozen;          // 1: the system does not advance (set by the host between chunks)
+    int    uniform_coef;    // 1: every particle has the integrator coefficients `coef` (the per-particle
+                            // array is then not read)
+    double4 coef;
     double energy[NTERMS];
     GlobalParams g[NGLOBAL];
 };

@@ -905,6 +905,15 @@ void commit(mjg_context* c)
             psys[gi] = (int)k;
             mol[gi] = (int)(mol_base[k] + s.mol_local[i]);
         }
+        // one set of coefficients for the whole system (uniform masses and
+        // frictions): the integrator reads it from the system record
+        bool uniform = s.n > 0;
+        for(int64_t i = 1; i < s.n && uniform; ++i)
+        {
+            uniform = std::memcmp(&coef[off + i], &coef[off], sizeof(double4)) == 0;
+        }
+        hs[k].uniform_coef = uniform ? 1 : 0;
+        hs[k].coef = uniform ? coef[off] : make_double4(0.0, 0.0, 0.0, 0.0);
         for(int g = 0; g < NGLOBAL; ++g)
         {
             long long* exs = (long long*)at(c_exs[g]);
@@ -1520,6 +1529,14 @@ int mjg_system_set_temperature(mjg_context* c, int sys, double T)
     CK(cudaMemcpyAsync(stg, z.data(), sizeof(double) * s.n, cudaMemcpyHostToDevice, c->stream));
     launch_set_noise(c->arena, stg, s.off, s.n, c->stream);
     CK(cudaStreamSynchronize(c->stream));
+    download_sys(c);
+    SysDev& d = c->h_sys[s.arena_slot];
+    if(d.uniform_coef && s.n > 0)
+    {
+        d.coef.z = z[0];
+        upload_sys(c);
+        CK(cudaStreamSynchronize(c->stream));
+    }
     ABI_END(c)
 }
 

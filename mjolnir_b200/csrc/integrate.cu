@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
         const SysDev& S = a.sys[s];
         double4 p = a.pos[i];
         double4 v = a.vel[i];
-        const double4 c = a.coef[i];     // per integrator: see Arena::coef
+        const double4 c = S.uniform_coef ? S.coef : a.coef[i];     // per integrator: see Arena::coef
         double fx, fy, fz;
         load_force<PREC>(a.force, i, fx, fy, fz);
         const bool uld = AUX && S.integrator == I_UNDERDAMPED;
@@ -238,12 +238,12 @@ __global__ void __launch_bounds__(TPB) k_integrate_last(Arena a)
     if(S.integrator == I_UNDERDAMPED)
     {
         double4 acc = a.accel[i];
-        underdamped_close(S, i, v, acc, a.coef[i], fx, fy, fz, S.step);
+        underdamped_close(S, i, v, acc, S.uniform_coef ? S.coef : a.coef[i], fx, fy, fz, S.step);
         a.accel[i] = acc;
         a.vel[i] = v;
         return;
     }
-    const double c = a.coef[i].x;
+    const double c = S.uniform_coef ? S.coef.x : a.coef[i].x;
     v.x = __dadd_rn(v.x, __dmul_rn(c, fx));
     v.y = __dadd_rn(v.y, __dmul_rn(c, fy));
     v.z = __dadd_rn(v.z, __dmul_rn(c, fz));
@@ -263,7 +263,7 @@ __global__ void k_init_accel(Arena a, long long first, long long count)
     if(S.integrator != I_UNDERDAMPED) {return;}
     double fx, fy, fz;
     load_force<PREC>(a.force, i, fx, fy, fz);
-    const double4 c = a.coef[i];
+    const double4 c = S.uniform_coef ? S.coef : a.coef[i];
     double r0, r1, r2;
     gaussian3(S.seed, (unsigned long long)(i - S.off), S.step, r0, r1, r2);
     a.accel[i] = make_double4(__dadd_rn(__dmul_rn(fx, c.x), __dmul_rn(r0, c.z)),
