@@ -190,3 +190,44 @@ def test_equipartition(integrator):
         kin.append(0.5 * float(np.sum(d.mass[:, None] * v * v)))
     e.close()
     assert np.mean(kin) == pytest.approx(1.5 * d.n * _stationary_kT(d), rel=0.01)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("integrator", ["BAOAB", "VelocityVerlet"] + INTEGRATORS)
+def test_per_particle_masses_and_frictions(integrator, precision):
+    """Masses and frictions that differ per particle (the per-particle
+    coefficient array) beside a system with uniform ones (coefficients held
+    in the system record), each against the oracle, across a temperature
+    change."""
+    rng = np.random.default_rng(46)
+    mixed_d = S.polymer_melt(nchains=4, nbeads=40, radius=40.0, seed=46)
+    mixed_d.mass = rng.uniform(0.5, 2.0, mixed_d.n)
+    mixed_d.gamma = rng.uniform(0.2, 1.5, mixed_d.n)
+    uniform_d = S.polymer_melt(nchains=3, nbeads=40, radius=40.0, seed=47)
+    descs = []
+    for d in (mixed_d, uniform_d):
+        d = d.copy()
+        d.integrator = integrator
+        if integrator == "VelocityVerlet":
+            d.dt = 0.005
+        descs.append(d)
+    e = Engine(precision)
+    sids = [e.add_system(d) for d in descs]
+    e.commit()
+    e.step(30)
+    if integrator != "VelocityVerlet":
+        for sid in sids:
+            e.set_temperature(sid, 380.0)
+    e.step(30)
+    for d, sid in zip(descs, sids):
+        o = oracle.Oracle(d)
+        o.init_dynamics()
+        o.run(30)
+        if integrator != "VelocityVerlet":
+            o.set_temperature(380.0)
+        o.run(30)
+        po, vo, _ = o.state()
+        p, v, _ = e.state(sid)
+        assert np.abs(p - po).max() <= TOL[precision], (integrator, precision)
+        assert np.abs(v - vo).max() <= 10 * TOL[precision], (integrator, precision)
+    e.close()
