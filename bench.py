@@ -281,6 +281,35 @@ def fluid_pair_roofline(local, peak, steps=200):
     return out
 
 
+def force_error(eng, descs, sids, local, nsample=16):
+    """Per term, the largest relative RMS force error (sqrt(sum |dF|^2 /
+    sum |F|^2)) of the mixed-form engine against the FP64 form evaluated on
+    the mixed engine's own current coordinates, over `nsample` systems spread
+    across the batch's sizes.  The FP64 form matches the reference's
+    arithmetic (lists bit-exact, forces within 1e-12), so it stands in for the
+    reference on coordinates the CPU never reaches."""
+    from mjolnir_b200.engine import Engine
+    order = sorted(range(len(descs)), key=lambda k: descs[k].n)
+    pick = sorted({order[int(round(q * (len(order) - 1) / max(1, nsample - 1)))] for q in range(nsample)})
+    fp = Engine("fp64", device=local)
+    fsids = [fp.add_system(descs[k]) for k in pick]
+    fp.commit()
+    terms = ("bond", "angle", "dihedral", "exv", "dh")
+    worst = {t: 0.0 for t in terms}
+    for k, fs in zip(pick, fsids):
+        pos, vel, _ = eng.state(sids[k])
+        fp.set_state(fs, pos, vel)
+        for t in terms:
+            fm, _ = eng.term_force(sids[k], t)
+            fd, _ = fp.term_force(fs, t)
+            den = float(np.sum(fd * fd))
+            err = float(np.sqrt(np.sum((fm - fd) ** 2) / den)) if den > 0 else 0.0
+            worst[t] = max(worst[t], err)
+    fp.close()
+    return {"max_rel_rms": worst, "bound": 1e-5, "systems": len(pick),
+            "reference": "FP64 form on the mixed trajectory's coordinates after the timed steps"}
+
+
 def workload_config(descs, precision, chunk):
     return {
         "workload": "batch of 256 independent polymer melts (bonds, angles, dihedrals, "
@@ -302,8 +331,7 @@ def run_b200(args, ws, rank, local, pg):
     descs = build_batch(args.nsys)
     ntot = sum(d.n for d in descs)
     eng = Engine("mixed", device=local)
-    for d in descs:
-        eng.add_system(d)
+    sids = [eng.add_system(d) for d in descs]
     eng.commit()
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
     tuned = None
@@ -407,6 +435,9 @@ def run_b200(args, ws, rank, local, pg):
                  "sample": f"{len(sample)} systems run one at a time, FP64, {CHUNK} steps each",
                  "batched_over_plain": value / ws / (tot_ps / tot_t)}
 
+    # ---- force error of the timed mixed-form run against the FP64 form
+    ferr = force_error(eng, descs, sids, local) if rank == 0 else None
+
     # ---- pair kernels on the 1,048,576-bead periodic fluid, plain FP64 and mixed
     fluid = None
     if not args.no_fluid and rank == 0:
@@ -449,6 +480,7 @@ def run_b200(args, ws, rank, local, pg):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_fp64_single_system": plain,
+            "force_error": ferr,
             "fluid_1m_pair_kernels": fluid,
             "serving": serving,
         }
