@@ -66,6 +66,12 @@ MJG_API int  mjg_context_set_graphs(mjg_context* ctx, int enable);
 /* Options: the per-step work of mjg_step is also checked for list overflow
  * and rolled back when it happens (default 1). */
 MJG_API int  mjg_context_set_rollback(mjg_context* ctx, int enable);
+/* Reserves the page-locked host buffers that commits pack into for an
+ * arena of up to `particles` particles (about 450 bytes per particle), so
+ * that a server which fills its arena over many commits does not page-lock
+ * memory again and again while it serves.  Optional; buffers still grow
+ * when a commit needs more. */
+MJG_API int  mjg_context_reserve(mjg_context* ctx, int64_t particles);
 
 /* ---------------------------------------------------------------- systems */
 

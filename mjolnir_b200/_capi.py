@@ -63,6 +63,7 @@ SIGNATURES = {
     "mjg_neighbors": (C.c_int, [_ctx, C.c_int, C.c_int, _i64p, C.c_int64, _i64p]),
     "mjg_rebuild_count": (C.c_int, [_ctx, C.c_int, C.c_int, _i64p]),
     "mjg_step_count": (C.c_int, [_ctx, C.c_int, _i64p]),
+    "mjg_context_reserve": (C.c_int, [_ctx, C.c_int64]),
     "mjg_molecule_count": (C.c_int, [_ctx, C.c_int, _i64p]),
     "mjg_particle_count": (C.c_int, [_ctx, C.c_int, _i64p]),
     "mjg_device_bytes": (C.c_int, [_ctx, _i64p]),

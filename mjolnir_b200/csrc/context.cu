@@ -65,14 +65,15 @@ struct DevBuf {
         CK(cudaMalloc(&p, b));
         bytes = cap = b;
     }
-    // keeps the allocation when it is large enough, else grows it with a
-    // quarter of headroom (arenas that are re-packed often change size)
+    // keeps the allocation when it is large enough, else grows it to twice
+    // the request (a serving arena that fills up over its first commits
+    // then reallocates a few times, not at every commit)
     void ensure(size_t b)
     {
         if(b > cap)
         {
             release();
-            const size_t want = b + b / 4;
+            const size_t want = 2 * b;
             CK(cudaMalloc(&p, want));
             cap = want;
         }
@@ -363,11 +364,11 @@ int default_tpp(int max_count)
 // a slot's first block before they know its length
 size_t list_words(int cap) {return (size_t)std::max(cap, 16);}
 
-// (re)allocates the neighbour arrays of term g for capacity cap
+// sizes the neighbour arrays of term g for capacity cap (the buffer only grows)
 void alloc_lists(mjg_context* c, int g, int cap)
 {
     TermDev& T = c->term[g];
-    T.nbr.alloc(sizeof(int) * list_words(cap) * (size_t)(T.t.np > 0 ? T.t.np : 1));
+    T.nbr.ensure(sizeof(int) * list_words(cap) * (size_t)(T.t.np > 0 ? T.t.np : 1));
     T.t.nbr = T.nbr.as<int>();
     T.t.cap = cap;
     T.cap_alloc = cap;
@@ -455,8 +456,8 @@ double* pinned(mjg_context* c, size_t bytes)
     if(bytes > c->h_pinned_bytes)
     {
         if(c->h_pinned) {cudaFreeHost(c->h_pinned); c->h_pinned = nullptr; c->h_pinned_bytes = 0;}
-        CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_pinned), bytes));
-        c->h_pinned_bytes = bytes;
+        CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_pinned), 2 * bytes));   // grow rarely
+        c->h_pinned_bytes = 2 * bytes;
     }
     return c->h_pinned;
 }
@@ -841,7 +842,7 @@ void commit(mjg_context* c)
     if(cv.total > c->h_pack_bytes)
     {
         if(c->h_pack) {cudaFreeHost(c->h_pack); c->h_pack = nullptr; c->h_pack_bytes = 0;}
-        const size_t want = cv.total + cv.total / 4;
+        const size_t want = 2 * cv.total;          // page-locking is slow: grow rarely
         CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_pack), want));
         c->h_pack_bytes = want;
     }
@@ -1466,6 +1467,23 @@ int mjg_context_set_rollback(mjg_context* c, int enable)
     ABI_BEGIN(c)
     if(c->committed) {throw Error(MJG_ESTATE, "set rollback before mjg_commit");}
     c->rollback = enable != 0;
+    ABI_END(c)
+}
+
+int mjg_context_reserve(mjg_context* c, int64_t particles)
+{
+    ABI_BEGIN(c)
+    if(particles < 0) {throw Error(MJG_EINVAL, "negative particle count");}
+    // the commit's packing buffer: state, coefficients, exclusions, pair
+    // participants and bonded terms come to about 400 bytes per particle
+    const size_t pack = (size_t)particles * 400;
+    if(pack > c->h_pack_bytes)
+    {
+        if(c->h_pack) {cudaFreeHost(c->h_pack); c->h_pack = nullptr; c->h_pack_bytes = 0;}
+        CK(cudaMallocHost(&c->h_pack, pack));
+        c->h_pack_bytes = pack;
+    }
+    pinned(c, (size_t)particles * 3 * sizeof(double) / 2);   // grows to twice: one field of state
     ABI_END(c)
 }
 

@@ -38,6 +38,10 @@ class Engine:
         A.check(self.ctx, self.lib.mjg_context_set_graphs(self.ctx, 1 if graphs else 0))
         A.check(self.ctx, self.lib.mjg_context_set_rollback(self.ctx, 1 if rollback else 0))
 
+    def reserve(self, particles: int):
+        """Page-locks the commit buffers for an arena of up to `particles`."""
+        self._c(self.lib.mjg_context_reserve(self.ctx, int(particles)))
+
     def close(self):
         if getattr(self, "ctx", None):
             self.lib.mjg_context_destroy(self.ctx)

@@ -69,6 +69,7 @@ class Server:
                  chunk_seconds: Optional[float] = None, lookahead: int = 64,
                  tuned: Optional[dict] = None):
         self.eng = Engine(precision, device=device)
+        self.eng.reserve(max_particles)          # page-lock once, at start-up
         # per global term: {"margin", "schedule", "threads_per_particle", "unroll"}
         # as :func:`mjolnir_b200.autotune.tune` returns them; the margin
         # replaces each admitted job's, the launch shape is set after every
