@@ -48,7 +48,8 @@ enum { MJG_UNLIMITED = 0, MJG_PERIODIC_CUBOID = 1 };
 enum { MJG_TERM_BOND = 0, MJG_TERM_ANGLE = 1, MJG_TERM_DIHEDRAL = 2,
        MJG_TERM_EXV = 3, MJG_TERM_DH = 4, MJG_TERM_LJ = 5 };
 enum { MJG_IGNORE_NOTHING = 0, MJG_IGNORE_SELF = 1, MJG_IGNORE_OTHERS = 2 };
-enum { MJG_BAOAB = 0, MJG_VELOCITY_VERLET = 1, MJG_UNDERDAMPED_LANGEVIN = 2, MJG_GJF_LANGEVIN = 3 };
+enum { MJG_BAOAB = 0, MJG_VELOCITY_VERLET = 1, MJG_UNDERDAMPED_LANGEVIN = 2, MJG_GJF_LANGEVIN = 3,
+       MJG_GBAOAB_LANGEVIN = 4 };
 
 /* ---------------------------------------------------------------- context */
 
@@ -192,7 +193,10 @@ MJG_API int mjg_dihedrals_set(mjg_context* ctx, int sys, const char* topology, i
  * is carried from step to step, across commits and rollbacks; replacing a
  * system's positions starts it again as Integrator::initialize does) or
  * GJFNVTLangevinIntegrator(dt, alphas) (core/GJFNVTLangevinIntegrator.hpp,
- * "G-JFLangevin"; input/read_integrator.hpp:242-300).
+ * "G-JFLangevin"; input/read_integrator.hpp:242-300) or
+ * gBAOABLangevinIntegrator(dt, gammas) (core/gBAOABLangevinIntegrator.hpp,
+ * "g-BAOABLangevin"; :189-239) without constraints: BAOAB whose two half
+ * drifts each move the position.
  * gamma[n]: the friction gammas, or the G-JF alphas (ignored for Verlet).  The Langevin noise is Philox4x32-10 keyed
  * by `seed` and counted by (particle, step), in place of the reference's
  * mt19937 stream (core/RandomNumberGenerator.hpp:13-86); the underdamped

@@ -17,7 +17,7 @@ UNLIMITED, PERIODIC_CUBOID = 0, 1
 TERM_BOND, TERM_ANGLE, TERM_DIHEDRAL, TERM_EXV, TERM_DH, TERM_LJ = range(6)
 TERM_NAMES = ("bond", "angle", "dihedral", "exv", "dh", "lj")
 IGNORE = {"Nothing": 0, "Self": 1, "Intra": 1, "Others": 2, "Inter": 2}
-BAOAB, VELOCITY_VERLET, UNDERDAMPED_LANGEVIN, GJF_LANGEVIN = 0, 1, 2, 3
+BAOAB, VELOCITY_VERLET, UNDERDAMPED_LANGEVIN, GJF_LANGEVIN, GBAOAB_LANGEVIN = 0, 1, 2, 3, 4
 
 _i64p = C.POINTER(C.c_int64)
 _f64p = C.POINTER(C.c_double)

@@ -19,7 +19,7 @@ namespace mjg {
 enum Term : int { T_BOND = 0, T_ANGLE = 1, T_DIHEDRAL = 2, T_EXV = 3, T_DH = 4, T_LJ = 5, NTERMS = 6 };
 enum { G_EXV = 0, G_DH = 1, G_LJ = 2, NGLOBAL = 3 };
 enum Boundary : int { B_UNLIMITED = 0, B_PERIODIC = 1 };
-enum Integrator : int { I_BAOAB = 0, I_VV = 1, I_UNDERDAMPED = 2, I_GJF = 3 };
+enum Integrator : int { I_BAOAB = 0, I_VV = 1, I_UNDERDAMPED = 2, I_GJF = 3, I_GBAOAB = 4 };
 enum IgnoreMol : int { IGN_NOTHING = 0, IGN_SELF = 1, IGN_OTHERS = 2 };
 enum Precision : int { P_FP64 = 0, P_MIXED = 1 };
 

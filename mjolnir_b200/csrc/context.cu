@@ -893,7 +893,8 @@ void commit(mjg_context* c)
                 coef[gi] = make_double4(halfdt * rmass, 1.0 - alpha * b * s.dt / m,
                                         std::sqrt(2 * alpha * kBT * s.dt), s.dt);
             }
-            else if(s.integrator == I_BAOAB)   // reset_parameters (:73-99)
+            else if(s.integrator == I_BAOAB || s.integrator == I_GBAOAB)   // reset_parameters (:73-99;
+                                                                            // gBAOAB :80-106)
             {
                 const double gamma_dt = -1 * s.gamma[i] * s.dt;
                 coef[gi] = make_double4(halfdt * rmass, std::exp(gamma_dt),
@@ -1819,14 +1820,15 @@ int mjg_integrator_set(mjg_context* c, int sys, int kind, double dt, const doubl
     HostSystem& s = get_sys(c, sys);
     if(s.resident) {throw Error(MJG_ESTATE, "the integrator is fixed once committed");}
     if(kind != MJG_BAOAB && kind != MJG_VELOCITY_VERLET && kind != MJG_UNDERDAMPED_LANGEVIN &&
-       kind != MJG_GJF_LANGEVIN)
+       kind != MJG_GJF_LANGEVIN && kind != MJG_GBAOAB_LANGEVIN)
     {
         throw Error(MJG_EINVAL, "unknown integrator");
     }
     if(!(dt > 0)) {throw Error(MJG_EINVAL, "dt must be positive");}
     if(kind != MJG_VELOCITY_VERLET && !gamma) {throw Error(MJG_EINVAL, "Langevin integrators need gammas");}
     s.integrator = kind == MJG_BAOAB ? I_BAOAB : kind == MJG_VELOCITY_VERLET ? I_VV :
-                   kind == MJG_UNDERDAMPED_LANGEVIN ? I_UNDERDAMPED : I_GJF;
+                   kind == MJG_UNDERDAMPED_LANGEVIN ? I_UNDERDAMPED : kind == MJG_GJF_LANGEVIN ? I_GJF :
+                   I_GBAOAB;
     s.dt = dt;
     s.gamma = gamma ? std::vector<double>(gamma, gamma + s.n) : std::vector<double>(s.n, 0.0);
     s.seed = seed;

@@ -85,6 +85,8 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
             v.z = __dadd_rn(v.z, __dmul_rn(c.x, fz));
         }
         double dx, dy, dz;
+        double4 pn = p;     // g-BAOAB: the new position, moved by its two half drifts
+        bool direct = false;
         if(uld)             // core/UnderdampedLangevinIntegrator.hpp:198-221
         {
             double4 acc = a.accel[i];
@@ -120,8 +122,12 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
             v.y = __dadd_rn(__dmul_rn(c.y, __dadd_rn(v.y, __dmul_rn(c.x, fy))), __dmul_rn(x.y, b1));
             v.z = __dadd_rn(__dmul_rn(c.y, __dadd_rn(v.z, __dmul_rn(c.x, fz))), __dmul_rn(x.y, b2));
         }
-        else if(S.integrator == I_BAOAB)
+        else if(S.integrator == I_BAOAB || S.integrator == I_GBAOAB)
         {
+            // g-BAOAB without constraints (gBAOABLangevinIntegrator.hpp:318-420,
+            // one correction step): the same B-A-O-A, but each half drift moves
+            // the position itself and the displacement is new minus old position
+            const bool split = S.integrator == I_GBAOAB;
             double r0, r1, r2;
             gaussian3(S.seed, (unsigned long long)(i - S.off), S.step, r0, r1, r2);
             v.x = __dadd_rn(v.x, __dmul_rn(c.x, fx));          // v += halfdt*rm*f
@@ -130,15 +136,29 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
             dx = __dmul_rn(c.w, v.x);                          // dp  = halfdt*v
             dy = __dmul_rn(c.w, v.y);
             dz = __dmul_rn(c.w, v.z);
+            if(split) {pn = make_double4(__dadd_rn(p.x, dx), __dadd_rn(p.y, dy), __dadd_rn(p.z, dz), p.w);}
             v.x = __dmul_rn(v.x, c.y);                         // v  *= exp(-gamma dt)
             v.y = __dmul_rn(v.y, c.y);
             v.z = __dmul_rn(v.z, c.y);
             v.x = __dadd_rn(v.x, __dmul_rn(c.z, r0));          // v  += noise*R
             v.y = __dadd_rn(v.y, __dmul_rn(c.z, r1));
             v.z = __dadd_rn(v.z, __dmul_rn(c.z, r2));
-            dx = __dadd_rn(dx, __dmul_rn(c.w, v.x));           // dp += halfdt*v
-            dy = __dadd_rn(dy, __dmul_rn(c.w, v.y));
-            dz = __dadd_rn(dz, __dmul_rn(c.w, v.z));
+            if(split)
+            {
+                pn.x = __dadd_rn(pn.x, __dmul_rn(c.w, v.x));
+                pn.y = __dadd_rn(pn.y, __dmul_rn(c.w, v.y));
+                pn.z = __dadd_rn(pn.z, __dmul_rn(c.w, v.z));
+                dx = __dsub_rn(pn.x, p.x);                     // displacement = new - old
+                dy = __dsub_rn(pn.y, p.y);
+                dz = __dsub_rn(pn.z, p.z);
+                direct = true;
+            }
+            else
+            {
+                dx = __dadd_rn(dx, __dmul_rn(c.w, v.x));       // dp += halfdt*v
+                dy = __dadd_rn(dy, __dmul_rn(c.w, v.y));
+                dz = __dadd_rn(dz, __dmul_rn(c.w, v.z));
+            }
         }
         else
         {
@@ -149,9 +169,13 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
             dy = __dmul_rn(c.w, v.y);
             dz = __dmul_rn(c.w, v.z);
         }
-        p.x = __dadd_rn(p.x, dx);
-        p.y = __dadd_rn(p.y, dy);
-        p.z = __dadd_rn(p.z, dz);
+        if(direct) {p = pn;}
+        else
+        {
+            p.x = __dadd_rn(p.x, dx);
+            p.y = __dadd_rn(p.y, dy);
+            p.z = __dadd_rn(p.z, dz);
+        }
         if(S.boundary == B_PERIODIC)                           // adjust_position
         {
             if(p.x < S.lower[0]) {p.x = __dadd_rn(p.x, S.width[0]);} else if(p.x >= S.upper[0]) {p.x = __dsub_rn(p.x, S.width[0]);}

@@ -126,7 +126,7 @@ class Engine:
             v0 = _arr(d.dihedrals[3], np.float64)
             self._c(L.mjg_dihedrals_set(self.ctx, s, d.dihedral_topology.encode(), len(k), A.i64(idx), A.f64(k), A.i32(nn), A.f64(v0)))
         kind = {"VelocityVerlet": A.VELOCITY_VERLET, "UnderdampedLangevin": A.UNDERDAMPED_LANGEVIN,
-                "G-JFLangevin": A.GJF_LANGEVIN}.get(d.integrator, A.BAOAB)
+                "G-JFLangevin": A.GJF_LANGEVIN, "g-BAOABLangevin": A.GBAOAB_LANGEVIN}.get(d.integrator, A.BAOAB)
         gam = _arr(d.gamma if d.gamma is not None else np.zeros(d.n), np.float64)
         self._c(L.mjg_integrator_set(self.ctx, s, kind, float(d.dt), A.f64(gam), int(d.seed) & ((1 << 64) - 1)))
         if d.start_step:

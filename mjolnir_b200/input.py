@@ -20,8 +20,9 @@ ready for :meth:`Engine.add_system`:
   ``integrator.seed``), ``delta_t``, ``total_step``, ``save_step``,
   ``integrator.type`` = ``"BAOABLangevin"`` or ``"UnderdampedLangevin"``
   (``gammas`` or the deprecated ``parameters``, input/read_integrator.hpp:55-187),
-  ``"G-JFLangevin"`` (``alphas`` or ``parameters``, :242-300) or
-  ``"VelocityVerlet"``;
+  ``"G-JFLangevin"`` (``alphas`` or ``parameters``, :242-300),
+  ``"g-BAOABLangevin"`` (``gammas``, :189-239; without constraints, which the
+  reader rejects) or ``"VelocityVerlet"``;
 * ``[[systems]]`` (the first): ``attributes``, ``boundary_shape``,
   ``particles`` with ``mass|m``, ``position|pos``, ``velocity|vel``, ``name``,
   ``group`` (input/read_system.hpp:93-290), or ``file_name = "x.msg"``, a
@@ -248,7 +249,7 @@ def _integrator(integ, n):
         return "VelocityVerlet", np.zeros(n)
     if kind not in _LANGEVIN:
         raise InputError(f'integrator type "{kind}": only "BAOABLangevin", "UnderdampedLangevin", '
-                         '"G-JFLangevin" and "VelocityVerlet" are supported')
+                         '"G-JFLangevin", "g-BAOABLangevin" and "VelocityVerlet" are supported')
     name, plural, single, alt = _LANGEVIN[kind]
     _check_keys(integ, {"type", "seed", "remove", "env", "parameters", plural}, "[simulator.integrator]")
     if "parameters" in integ and plural in integ:
@@ -271,7 +272,8 @@ def _integrator(integ, n):
 # alternative spelling); input/read_integrator.hpp:55-187, 242-300
 _LANGEVIN = {"BAOABLangevin": ("BAOAB", "gammas", "gamma", "γ"),
              "UnderdampedLangevin": ("UnderdampedLangevin", "gammas", "gamma", "γ"),
-             "G-JFLangevin": ("G-JFLangevin", "alphas", "alpha", None)}
+             "G-JFLangevin": ("G-JFLangevin", "alphas", "alpha", None),
+             "g-BAOABLangevin": ("g-BAOABLangevin", "gammas", "gamma", "γ")}
 
 
 def _system(sysd, boundary):

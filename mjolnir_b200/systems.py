@@ -63,6 +63,7 @@ class SystemDesc:
     angle_topology: str = "none"
     dihedral_topology: str = "none"
     integrator: str = "BAOAB"          # "BAOAB" | "VelocityVerlet" | "UnderdampedLangevin" | "G-JFLangevin"
+                                       # | "g-BAOABLangevin"
     dt: float = 0.01
     gamma: Optional[np.ndarray] = None # friction per particle (G-JFLangevin: its alpha)
     seed: int = 12345

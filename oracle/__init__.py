@@ -158,7 +158,8 @@ def make_spec(desc):
         s.dihd_k = _ptr(arr(k, np.float64), C.c_double)
         s.dihd_n = _ptr(arr(nn, np.int32), C.c_int32)
         s.dihd_v0 = _ptr(arr(v0, np.float64), C.c_double)
-    s.integrator = {"BAOAB": 0, "VelocityVerlet": 1, "UnderdampedLangevin": 2, "G-JFLangevin": 3}[desc.integrator]
+    s.integrator = {"BAOAB": 0, "VelocityVerlet": 1, "UnderdampedLangevin": 2, "G-JFLangevin": 3,
+                    "g-BAOABLangevin": 4}[desc.integrator]
     s.dt = desc.dt
     gam = desc.gamma if desc.gamma is not None else np.zeros(desc.n)
     s.gamma = _ptr(arr(gam, np.float64), C.c_double)

@@ -1387,6 +1387,32 @@ int orc_run(orc_state* st, int64_t nsteps)
                 largest_disp2 = largest_disp2 < d2 ? d2 : largest_disp2;
             }
         }
+        else if(st->s.integrator == ORC_GBAOAB)   /* gBAOABLangevinIntegrator.hpp:318-420, no constraints */
+        {
+            for(int64_t i=0; i<n; ++i)
+            {
+                double R[3], dp[3];
+                orc_gaussian3(st->s.seed, (uint64_t)i, st->step, R);
+                const double rm = st->rmass[i];
+                double* p = st->pos + 3*i;
+                double* v = st->vel + 3*i;
+                for(int d=0; d<3; ++d) {v[d] += halfdt * rm * st->force[3*i+d];}            /* B */
+                double q[3];
+                for(int d=0; d<3; ++d) {q[d] = p[d] + halfdt * v[d];}                        /* A */
+                for(int d=0; d<3; ++d) {v[d] *= st->exp_gamma_dt[i];}                        /* O */
+                for(int d=0; d<3; ++d) {v[d] += st->noise_coeff[i] * R[d];}
+                for(int d=0; d<3; ++d) {q[d] = q[d] + halfdt * v[d];}                        /* A */
+                for(int d=0; d<3; ++d)
+                {
+                    dp[d] = q[d] - p[d];              /* position(i) - old_position_[i] */
+                    p[d] = q[d];
+                    st->force[3*i+d] = 0;
+                }
+                adjust_position(st, p);
+                const double d2 = length_sq(dp);
+                largest_disp2 = largest_disp2 < d2 ? d2 : largest_disp2;
+            }
+        }
         else                              /* BAOABLangevinIntegrator.hpp:170-240 */
         {
             for(int64_t i=0; i<n; ++i)

@@ -11,7 +11,8 @@
 //   - trajectories                   (BAOABLangevinIntegrator::step,
 //                                     VelocityVerletIntegrator::step,
 //                                     UnderdampedLangevinIntegrator::step,
-//                                     GJFNVTLangevinIntegrator::step),
+//                                     GJFNVTLangevinIntegrator::step,
+//                                     gBAOABLangevinIntegrator::step),
 //   - timings of its sequential and OpenMP paths.
 // The objects are put together the way the input readers do it
 // (input/read_global_interaction.hpp:25-98, input/read_local_interaction.hpp,
@@ -35,6 +36,7 @@
 #include <mjolnir/core/VelocityVerletIntegrator.hpp>
 #include <mjolnir/core/UnderdampedLangevinIntegrator.hpp>
 #include <mjolnir/core/GJFNVTLangevinIntegrator.hpp>
+#include <mjolnir/core/gBAOABLangevinIntegrator.hpp>
 #include <mjolnir/core/PeriodicGridCellList.hpp>
 #include <mjolnir/core/UnlimitedGridCellList.hpp>
 #include <mjolnir/forcefield/global/GlobalPairInteraction.hpp>
@@ -144,6 +146,7 @@ struct RefSim final : public RefSimBase
     std::unique_ptr<VelocityVerletIntegrator<traitsT>> vv;
     std::unique_ptr<UnderdampedLangevinIntegrator<traitsT>> ul;
     std::unique_ptr<GJFNVTLangevinIntegrator<traitsT>> gjf;
+    std::unique_ptr<gBAOABLangevinIntegrator<traitsT>> gbaoab;
     local_base*  locals [3] = {nullptr, nullptr, nullptr};
     global_base* globals[3] = {nullptr, nullptr, nullptr};
     double time = 0.0;
@@ -376,6 +379,11 @@ struct RefSim final : public RefSimBase
             gjf = make_unique<GJFNVTLangevinIntegrator<traitsT>>(s.dt,
                         std::move(gam), remover_type(false, false, false));
         }
+        else if(s.integrator == ORC_GBAOAB)
+        {
+            gbaoab = make_unique<gBAOABLangevinIntegrator<traitsT>>(s.dt,
+                        std::move(gam), remover_type(false, false, false));
+        }
         else
         {
             baoab = make_unique<BAOABLangevinIntegrator<traitsT>>(s.dt,
@@ -529,6 +537,7 @@ struct RefSim final : public RefSimBase
         if(baoab)   {baoab->initialize(*sys, ff, rng);}
         else if(ul) {ul->initialize(*sys, ff, rng);}
         else if(gjf){gjf->initialize(*sys, ff, rng);}
+        else if(gbaoab) {gbaoab->initialize(*sys, ff, rng);}
         else        {vv->initialize(*sys, ff, rng);}
     }
     void run(long long nsteps) override
@@ -538,6 +547,7 @@ struct RefSim final : public RefSimBase
             time = baoab ? baoab->step(time, *sys, ff, rng)
                  : ul    ? ul->step(time, *sys, ff, rng)
                  : gjf   ? gjf->step(time, *sys, ff, rng)
+                 : gbaoab ? gbaoab->step(time, *sys, ff, rng)
                          : vv->step(time, *sys, ff, rng);
         }
     }

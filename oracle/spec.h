@@ -19,7 +19,7 @@ extern "C" {
 #endif
 
 enum { ORC_UNLIMITED = 0, ORC_PERIODIC = 1 };
-enum { ORC_BAOAB = 0, ORC_VV = 1, ORC_UNDERDAMPED = 2, ORC_GJF = 3 };
+enum { ORC_BAOAB = 0, ORC_VV = 1, ORC_UNDERDAMPED = 2, ORC_GJF = 3, ORC_GBAOAB = 4 };
 enum { ORC_IGNORE_NOTHING = 0, ORC_IGNORE_SELF = 1, ORC_IGNORE_OTHERS = 2 };
 /* potential of the first global term (ExcludedVolume family) */
 enum { ORC_EXV = 0, ORC_INVERSE_POWER = 1, ORC_HARD_CORE_EXV = 2 };
@@ -69,7 +69,7 @@ typedef struct orc_spec
     const int32_t* dihd_n; const double* dihd_v0;
 
     /* integrator */
-    int32_t integrator;          /* ORC_BAOAB / _VV / _UNDERDAMPED / _GJF   */
+    int32_t integrator;          /* ORC_BAOAB / _VV / _UNDERDAMPED / _GJF / _GBAOAB */
     double  dt;
     const double* gamma;         /* [n] friction (G-JF: alpha)              */
     uint64_t seed;

@@ -1,4 +1,4 @@
-"""The UnderdampedLangevin and G-JF integrators on the GPU against the oracle
+"""The UnderdampedLangevin, G-JF and g-BAOAB integrators on the GPU against the oracle
 (the same Philox noise stream, so the trajectories agree to the precision's
 tolerance), across a checkpoint, a temperature change, and mixed with the
 other integrators in one arena."""
@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 TOL = {"fp64": 1e-9, "mixed": 1e-5}
 
 
-INTEGRATORS = ["UnderdampedLangevin", "G-JFLangevin"]
+INTEGRATORS = ["UnderdampedLangevin", "G-JFLangevin", "g-BAOABLangevin"]
 
 
 def _with(d, integrator):
@@ -167,9 +167,10 @@ def _stationary_kT(d):
     UnderdampedLangevin, g = gamma dt / 2: v' = c v + (dt/2)(1 - g)(a + a'),
     c = (1 - g)((1 - g)^2 + g), variance kB T / m * 2 (1 - g)^2 / (2 - 2 g + g^2),
     a bias of about -g.  G-JF: v' = a v + (b/m) beta with a = (1 - x) / (1 + x),
-    b = 1 / (1 + x), x = alpha dt / 2m: exactly kB T / m."""
+    b = 1 / (1 + x), x = alpha dt / 2m: exactly kB T / m; g-BAOAB's O step
+    likewise."""
     kT = S.KB_KCAL * d.temperature
-    if d.integrator == "G-JFLangevin":
+    if d.integrator in ("G-JFLangevin", "g-BAOABLangevin"):
         return kT
     g = float(np.mean(d.gamma)) * d.dt / 2
     return kT * 2 * (1 - g) ** 2 / (2 - 2 * g + g * g)

@@ -289,7 +289,7 @@ parameters = [{index = 0, radius = 1.0}, {index = 1, radius = 1.0}]
     assert d.exv.kind == "InversePower" and d.exv.exponent == 5 and d.exv.cutoff == 4.0   # 2^(12 // 5)
 
 
-@pytest.mark.parametrize("integrator", ["UnderdampedLangevin", "G-JFLangevin", "VelocityVerlet"])
+@pytest.mark.parametrize("integrator", ["UnderdampedLangevin", "G-JFLangevin", "g-BAOABLangevin", "VelocityVerlet"])
 def test_integrator_round_trip(integrator, tmp_path):
     """Every supported integrator type is written and read back with its
     per-particle parameters (gammas, or the G-JF alphas)."""

@@ -11,7 +11,7 @@ import pytest
 import oracle
 from mjolnir_b200 import systems as S
 
-INTEGRATORS = ["BAOAB", "UnderdampedLangevin", "G-JFLangevin"]
+INTEGRATORS = ["BAOAB", "UnderdampedLangevin", "G-JFLangevin", "g-BAOABLangevin"]
 
 
 def ks_distance(samples, d):
