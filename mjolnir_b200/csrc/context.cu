@@ -190,7 +190,9 @@ struct mjg_context {
     cudaGraphExec_t graph_exec = nullptr;
     cudaGraph_t graph2 = nullptr;           // later steps: closing kick fused in
     cudaGraphExec_t graph2_exec = nullptr;
-    long long graph_nodes = 0, graph2_nodes = 0;
+    cudaGraph_t graph4 = nullptr;           // four such steps in one graph (fewer launches)
+    cudaGraphExec_t graph4_exec = nullptr;
+    long long graph_nodes = 0, graph2_nodes = 0, graph4_nodes = 0;
     bool graph_dirty = true;
 };
 
@@ -250,6 +252,8 @@ void release_graph(mjg_context* c)
     if(c->graph) {cudaGraphDestroy(c->graph); c->graph = nullptr;}
     if(c->graph2_exec) {cudaGraphExecDestroy(c->graph2_exec); c->graph2_exec = nullptr;}
     if(c->graph2) {cudaGraphDestroy(c->graph2); c->graph2 = nullptr;}
+    if(c->graph4_exec) {cudaGraphExecDestroy(c->graph4_exec); c->graph4_exec = nullptr;}
+    if(c->graph4) {cudaGraphDestroy(c->graph4); c->graph4 = nullptr;}
     c->graph_dirty = true;
 }
 
@@ -302,10 +306,11 @@ void enqueue_step_body(mjg_context* c, bool kick)
 }
 
 
-void capture_one(mjg_context* c, bool kick, cudaGraph_t& g, cudaGraphExec_t& ge, long long& nodes)
+void capture_one(mjg_context* c, bool kick, cudaGraph_t& g, cudaGraphExec_t& ge, long long& nodes,
+                 int steps = 1)
 {
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step_body(c, kick);
+    for(int k = 0; k < steps; ++k) {enqueue_step_body(c, kick);}
     g = nullptr;
     CK(cudaStreamEndCapture(c->stream, &g));
     CK(cudaGraphInstantiate(&ge, g, 0));
@@ -320,6 +325,7 @@ void capture_graph(mjg_context* c)
     const long long before = g_launches.load();
     capture_one(c, false, c->graph, c->graph_exec, c->graph_nodes);
     capture_one(c, true, c->graph2, c->graph2_exec, c->graph2_nodes);
+    capture_one(c, true, c->graph4, c->graph4_exec, c->graph4_nodes, 4);
     // capture counted the launches once; graph replays add them per replay
     g_launches.fetch_sub(g_launches.load() - before);
     c->graph_dirty = false;
@@ -1344,7 +1350,9 @@ void run_steps(mjg_context* c, int64_t nsteps)
         {
             if(c->graph_dirty || !c->graph_exec) {capture_graph(c);}
             CK(cudaGraphLaunch(c->graph_exec, st));
-            for(int64_t k = 1; k < nsteps; ++k) {CK(cudaGraphLaunch(c->graph2_exec, st));}
+            int64_t k = 1;
+            for(; k + 4 <= nsteps; k += 4) {CK(cudaGraphLaunch(c->graph4_exec, st));}
+            for(; k < nsteps; ++k) {CK(cudaGraphLaunch(c->graph2_exec, st));}
             note_launches((int)std::min<long long>(c->graph_nodes + c->graph2_nodes * (nsteps - 1),
                                                    (1ll << 30)));
         }
