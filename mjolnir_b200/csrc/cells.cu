@@ -373,6 +373,7 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
 {
     constexpr int GROUPS = TPB / LPS;              // slot groups per block
     constexpr int WG = 32 / LPS;                   // slot groups per warp
+    constexpr int CPL = (27 + LPS - 1) / LPS;      // stencil cells per lane
     __shared__ int c_start[GROUPS][27];
     __shared__ int c_excl[GROUPS][28];             // exclusive prefix; [27] = total
     const int n = t.work[0];
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
             const int cx = cell_coord(ri.x, G, 0);
             const int cy = cell_coord(ri.y, G, 1);
             const int cz = cell_coord(ri.z, G, 2);
-            for(int k = gl; k < 27; k += LPS)
+            for(int k = gl * CPL; k < gl * CPL + CPL && k < 27; ++k)   // this lane's block of stencil cells
             {
                 int x = cx + k % 3 - 1, y = cy + (k / 3) % 3 - 1, z = cz + k / 9 - 1;
                 bool inside = true;
@@ -437,11 +438,34 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
             }
         }
         __syncwarp();
-        if(valid && gl == 0)
+        // exclusive prefix of the 27 counts: within each lane's block, then
+        // across the group's lanes with shuffles
         {
-            int run = 0;
-            for(int k = 0; k < 27; ++k) {const int c = c_excl[grp][k]; c_excl[grp][k] = run; run += c;}
-            c_excl[grp][27] = run;
+            int cnt[CPL];
+            int sum = 0;
+#pragma unroll
+            for(int j = 0; j < CPL; ++j)
+            {
+                const int k = gl * CPL + j;
+                cnt[j] = (valid && k < 27) ? c_excl[grp][k] : 0;
+                sum += cnt[j];
+            }
+            int incl = sum;
+#pragma unroll
+            for(int o = 1; o < LPS; o <<= 1)
+            {
+                const int y = __shfl_up_sync(full, incl, o, LPS);
+                if(gl >= o) {incl += y;}
+            }
+            int run = incl - sum;
+#pragma unroll
+            for(int j = 0; j < CPL; ++j)
+            {
+                const int k = gl * CPL + j;
+                if(valid && k < 27) {c_excl[grp][k] = run;}
+                run += cnt[j];
+            }
+            if(valid && gl == LPS - 1) {c_excl[grp][27] = incl;}
         }
         __syncwarp();
         const int total = valid ? c_excl[grp][27] : 0;
