@@ -293,7 +293,7 @@ MJG_API int mjg_get_pair_schedule(mjg_context* ctx, int term, int* schedule);
  * lanes build several lists per warp at once, which pays when a particle has
  * few candidates in its 27 neighbouring cells.  Unless set here, each commit
  * picks it from the candidates an even filling of the grids would give
- * (below 24: 8, below 64: 16, else 32).  The lists are the same in every
+ * (below 12: 8, below 64: 16, else 32).  The lists are the same in every
  * case.  No counterpart in the reference. */
 MJG_API int mjg_set_build_lanes(mjg_context* ctx, int term, int lanes);
 MJG_API int mjg_get_build_lanes(mjg_context* ctx, int term, int* lanes);

@@ -1165,7 +1165,7 @@ void commit(mjg_context* c)
                 slots += (double)G.nslot;
             }
             const double per = slots > 0 ? cand / slots : 0.0;
-            T.build_lanes_choice = per < 24.0 ? 8 : (per < 64.0 ? 16 : 32);
+            T.build_lanes_choice = per < 12.0 ? 8 : (per < 64.0 ? 16 : 32);
         }
         t.build_lanes = T.build_lanes_choice;
         t.any_periodic = 0;
