@@ -1308,7 +1308,7 @@ void check_status(mjg_context* c, bool& overflow)
 {
     overflow = false;
     // a truncated list makes every later force of the chunk meaningless, so
-    // a list overflow is handled (rolled back) before anything else is judged
+    // a list overflow is handled (rolled back) before anything else is checked
     for(const auto& d : c->h_sys) {if(d.status & ST_LIST_OVERFLOW) {overflow = true;}}
     if(overflow) {return;}
     for(size_t k = 0; k < c->h_sys.size(); ++k)

@@ -3,7 +3,7 @@
 Tolerances (force error = relative RMS over all particles,
 sqrt(sum|dF|^2 / sum|F|^2)):
   FP64 form    lists bit-exact; forces <= 1e-12; energies <= 1e-12 relative
-  mixed form   lists bit-exact; forces <= 1e-5 (the north-star bound);
+  mixed form   lists bit-exact; forces <= 1e-5 relative RMS (the mixed form's bound);
                energies <= 1e-5 relative
 """
 import numpy as np
