@@ -10,9 +10,11 @@ For every global term of an :class:`~mjolnir_b200.engine.Engine` it picks
     its list in blocks with vector loads; the first and last optionally with
     each block's threads ordered by list length), the threads per particle / list
     block (1, 2, 4, 8, 16) and the partners each thread requests per batch
-    (1, 2, 4).
-In the mixed form neither choice changes a result: the fixed-point force sums
-do not depend on list order or length.  The engine's systems keep stepping
+    (1, 2, 4);
+  * the lanes per particle of the list build (8, 16, 32), by timing whole
+    steps at the chosen margin and shape.
+In the mixed form none of the choices changes a result: the fixed-point force
+sums do not depend on list order or length, and the lists are the same.  The engine's systems keep stepping
 while the tuner measures (the tuning run is part of the warm-up).
 """
 from __future__ import annotations
@@ -33,7 +35,7 @@ def _time_steps(eng, nsteps: int) -> float:
 
 def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
          tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1, 2, 3, 4), steps: int = 60,
-         warm: int = 20, log=None) -> dict:
+         warm: int = 20, log=None, build_lanes=(8, 16, 32)) -> dict:
     present = []
     for t in terms:
         try:
@@ -58,8 +60,20 @@ def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
                 best = (ms, m, shape)
         eng.set_margin(t, best[1])
         _apply(eng, t, best[2])
+        # lanes per particle of the list build, at the chosen margin and shape
+        lanes_best = None
+        for lanes in build_lanes:
+            eng.set_build_lanes(t, lanes)
+            eng.step(warm)
+            ms = _time_steps(eng, steps)
+            if log:
+                log(f"autotune {t}: list build with {lanes} lanes: {ms:.4f} ms/step")
+            if lanes_best is None or ms < lanes_best[0]:
+                lanes_best = (ms, lanes)
+        eng.set_build_lanes(t, lanes_best[1])
         choice[t] = {"margin": best[1], "schedule": best[2][0], "threads_per_particle": best[2][1],
-                     "unroll": best[2][2], "ms_per_step": best[0]}
+                     "unroll": best[2][2], "build_lanes": lanes_best[1],
+                     "ms_per_step": min(best[0], lanes_best[0])}
     return choice
 
 

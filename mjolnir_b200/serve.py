@@ -182,6 +182,8 @@ class Server:
                 self.eng.set_threads_per_particle(key, cfg.get("threads_per_particle", 1))
             if self.eng.get_pair_unroll(key) != cfg.get("unroll", 1):
                 self.eng.set_pair_unroll(key, cfg.get("unroll", 1))
+            if "build_lanes" in cfg and self.eng.get_build_lanes(key) != cfg["build_lanes"]:
+                self.eng.set_build_lanes(key, cfg["build_lanes"])
         self.commits += 1
         self.commit_s += time.perf_counter() - t
         self.last_commit = self.now()
