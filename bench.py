@@ -281,6 +281,44 @@ def fluid_pair_roofline(local, peak, steps=200):
     return out
 
 
+def small_configs(local, steps=2000, cpu_budget_s=3.0):
+    """The two single-system configurations: the 4,096-particle Lennard-Jones
+    fluid (reduced density 0.8, cutoff 2.5, BAOAB dt 0.005) and the
+    10,000-bead polymer melt in unbounded space (50 chains x 200 beads), each
+    as one plain system on the GPU in both forms (`steps` MD steps after a
+    warm-up, CUDA events on the library's stream), beside the reference's own
+    OpenMP path stepping the same system (a bounded sample)."""
+    import torch
+    from mjolnir_b200 import systems as S
+    from mjolnir_b200.engine import Engine
+    out = {}
+    for name, d in (("lj_fluid_4096", S.lj_fluid(n=4096, density=0.8, margin=0.2, seed=1)),
+                    ("polymer_melt_10000", S.polymer_melt(nchains=50, nbeads=200, radius=300.0, seed=2))):
+        row = {"particles": d.n}
+        for prec in ("fp64", "mixed"):
+            e = Engine(prec, device=local)
+            e.add_system(d)
+            e.commit()
+            e.step(200)
+            e.synchronize()
+            st = torch.cuda.ExternalStream(e.stream_handle(), device=local)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            e.step(steps)
+            b.record(st)
+            b.synchronize()
+            row[prec] = d.n * steps / (a.elapsed_time(b) / 1e3)
+            e.close()
+        res = cpu_reference_rate([d], budget_s=cpu_budget_s) if cpu_budget_s > 0 else None
+        if res:
+            row["reference_cpu"] = {"value": res[0], "cores": res[2], "kind": "reference"}
+            row["fp64_over_reference"] = row["fp64"] / res[0]
+        out[name] = row
+    out["unit"] = "particle-steps/s"
+    return out
+
+
 def force_error(eng, descs, sids, local, nsample=16):
     """Per term, the largest relative RMS force error (sqrt(sum |dF|^2 /
     sum |F|^2)) of the mixed-form engine against the FP64 form evaluated on
@@ -438,6 +476,11 @@ def run_b200(args, ws, rank, local, pg):
     # ---- force error of the timed mixed-form run against the FP64 form
     ferr = force_error(eng, descs, sids, local) if rank == 0 else None
 
+    # ---- the single-system configurations (LJ fluid, 10k-bead melt), GPU and reference CPU
+    small = None
+    if not args.no_plain and rank == 0 and ws == 1:
+        small = small_configs(local, cpu_budget_s=0.0 if args.no_cpu_baseline else 3.0)
+
     # ---- pair kernels on the 1,048,576-bead periodic fluid, plain FP64 and mixed
     fluid = None
     if not args.no_fluid and rank == 0:
@@ -480,6 +523,7 @@ def run_b200(args, ws, rank, local, pg):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_fp64_single_system": plain,
+            "single_system_configs": small,
             "force_error": ferr,
             "fluid_1m_pair_kernels": fluid,
             "serving": serving,
