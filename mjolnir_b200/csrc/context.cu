@@ -160,6 +160,7 @@ struct mjg_context {
     // branches of the step: one per global term (rebuild, forces) and one for
     // the bonded terms, forked from and joined back into `stream`
     cudaStream_t side[mjg::NGLOBAL + 1] = {};
+    cudaStream_t gate_body[mjg::NGLOBAL] = {};  // captures the conditional rebuild bodies
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[mjg::NGLOBAL + 1] = {};
     std::string err;
@@ -274,13 +275,38 @@ void enqueue_forces(mjg_context* c, const Arena& a, bool nf, bool ne)
 // launches add with integer atomics (exact in any order), so all branches may
 // overlap; the FP64 form adds its pair forces after the join, one term after
 // the other.
-void enqueue_step_body(mjg_context* c, bool kick)
+// arenas with at most this many systems carrying a term put that term's
+// rebuild behind a graph conditional (measured: a 10,000-bead melt alone steps
+// 10-18 % faster, a 256-system batch 5 % slower with it)
+constexpr int GATE_MAX_SYSTEMS = 4;
+
+void enqueue_step_body(mjg_context* c, bool kick, bool capturing)
 {
     const Arena& a = c->arena;
     cudaStream_t st = c->stream;
     TermArrays ts[NGLOBAL] = {c->term[0].t, c->term[1].t, c->term[2].t};
+    // while capturing: one conditional handle per global term of this step,
+    // reset to 0 at each launch of the graph and set by the margin kernel
+    RebuildGate gate{};
+    if(capturing)
+    {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, nullptr, nullptr));
+        for(int g = 0; g < NGLOBAL; ++g)
+        {
+            if(!ts[g].on || ts[g].np == 0) {continue;}
+            // only in arenas of a few systems: with many, some system
+            // rebuilds nearly every step and the `if` node only adds latency
+            int with_term = 0;
+            for(int id : c->arena_ids) {with_term += c->sys[id].g[g].on ? 1 : 0;}
+            if(with_term > GATE_MAX_SYSTEMS) {continue;}
+            CK(cudaGraphConditionalHandleCreate(&gate.handle[g], graph, 0, cudaGraphCondAssignDefault));
+            gate.on[g] = 1;
+        }
+    }
     launch_integrate_first(a, st, kick);
-    launch_margin(a, ts, st);
+    launch_margin(a, ts, st, gate);
     const bool mixed = a.precision == P_MIXED;
     CK(cudaEventRecord(c->ev_fork, st));
     auto branch = [&](int b, auto&& body) {
@@ -294,7 +320,34 @@ void enqueue_step_body(mjg_context* c, bool kick)
         TermArrays& t = c->term[g].t;
         if(!t.on || t.np == 0) {continue;}
         branch(g, [&](cudaStream_t s) {
-            launch_rebuild(a, g, t, 0, s);
+            if(gate.on[g])
+            {
+                // an `if` node after the branch's current dependencies, its
+                // body captured from a stream of its own
+                cudaStreamCaptureStatus cs;
+                cudaGraph_t graph = nullptr;
+                const cudaGraphNode_t* deps = nullptr;
+                size_t ndeps = 0;
+                CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps));
+                cudaGraphNodeParams p{};
+                p.type = cudaGraphNodeTypeConditional;
+                p.conditional.handle = gate.handle[g];
+                p.conditional.type = cudaGraphCondTypeIf;
+                p.conditional.size = 1;
+                cudaGraphNode_t node = nullptr;
+                CK(cudaGraphAddNode(&node, graph, deps, ndeps, &p));
+                cudaGraph_t body = p.conditional.phGraph_out[0];
+                CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+                CK(cudaStreamBeginCaptureToGraph(c->gate_body[g], body, nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeThreadLocal));
+                launch_rebuild(a, g, t, 0, c->gate_body[g]);
+                cudaGraph_t done = nullptr;
+                CK(cudaStreamEndCapture(c->gate_body[g], &done));
+            }
+            else
+            {
+                launch_rebuild(a, g, t, 0, s);
+            }
             if(mixed) {launch_pair(a, g, t, true, false, 0, s, false);}
         });
     }
@@ -310,7 +363,7 @@ void capture_one(mjg_context* c, bool kick, cudaGraph_t& g, cudaGraphExec_t& ge,
                  int steps = 1)
 {
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    for(int k = 0; k < steps; ++k) {enqueue_step_body(c, kick);}
+    for(int k = 0; k < steps; ++k) {enqueue_step_body(c, kick, true);}
     g = nullptr;
     CK(cudaStreamEndCapture(c->stream, &g));
     CK(cudaGraphInstantiate(&ge, g, 0));
@@ -1358,7 +1411,7 @@ void run_steps(mjg_context* c, int64_t nsteps)
         }
         else
         {
-            for(int64_t k = 0; k < nsteps; ++k) {enqueue_step_body(c, k > 0);}
+            for(int64_t k = 0; k < nsteps; ++k) {enqueue_step_body(c, k > 0, false);}
         }
         launch_integrate_last(c->arena, st);
         CK(cudaGetLastError());
@@ -1423,6 +1476,10 @@ int mjg_context_create(int device, int precision, mjg_context** out)
     {
         ok = cudaStreamCreateWithFlags(&c->side[b], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->ev_join[b], cudaEventDisableTiming) == cudaSuccess;
+        if(ok && b < mjg::NGLOBAL)
+        {
+            ok = cudaStreamCreateWithFlags(&c->gate_body[b], cudaStreamNonBlocking) == cudaSuccess;
+        }
     }
     if(!ok)
     {
@@ -1454,6 +1511,7 @@ void mjg_context_destroy(mjg_context* c)
     for(int b = 0; b <= mjg::NGLOBAL; ++b)
     {
         if(c->side[b]) {cudaStreamSynchronize(c->side[b]); cudaStreamDestroy(c->side[b]);}
+        if(b < mjg::NGLOBAL && c->gate_body[b]) {cudaStreamDestroy(c->gate_body[b]);}
         if(c->ev_join[b]) {cudaEventDestroy(c->ev_join[b]);}
     }
     if(c->ev_fork) {cudaEventDestroy(c->ev_fork);}

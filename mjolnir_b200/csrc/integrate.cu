@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(TPB) k_integrate_first(Arena a)
 // reduce_margin(2 sqrt(max|dp|^2)) for every global term of every system;
 // a term whose skin is used up is flagged for a rebuild.  Also advances the
 // noise step counter.
-__global__ void k_margin(Arena a, int* any0, int* any1, int* any2)
+__global__ void k_margin(Arena a, int* any0, int* any1, int* any2, RebuildGate gate)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if(s >= a.nsys) {return;}
@@ -243,6 +243,7 @@ __global__ void k_margin(Arena a, int* any0, int* any1, int* any2)
         {
             G.rebuild = 1;
             if(any[g]) {atomicOr(any[g], 1);}
+            if(gate.on[g]) {cudaGraphSetConditional(gate.handle[g], 1u);}   // the term's rebuild runs
         }
     }
 }
@@ -381,12 +382,12 @@ void launch_integrate_first(const Arena& a, cudaStream_t s, bool kick)
     note_launches(1);
 }
 
-void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s)
+void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s, const RebuildGate& gate)
 {
     if(a.nsys == 0) {return;}
     k_margin<<<(a.nsys + 127) / 128, 128, 0, s>>>(a,
         t[0].on ? t[0].any_rebuild : nullptr, t[1].on ? t[1].any_rebuild : nullptr,
-        t[2].on ? t[2].any_rebuild : nullptr);
+        t[2].on ? t[2].any_rebuild : nullptr, gate);
     note_launches(1);
 }
 

@@ -86,7 +86,16 @@ void launch_integrate_first(const Arena& a, cudaStream_t s, bool kick = false);
 void launch_init_accel(const Arena& a, long long first, long long count, cudaStream_t s);
 // accel[first + k] = src[3k .. 3k + 2] (host-layout staging)
 void launch_set_accel(const Arena& a, const double* src, long long first, long long count, cudaStream_t s);
-void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s);
+// Graph-conditional rebuilds: in a captured step each global term's rebuild
+// sits in the body of an `if` node whose handle the margin kernel sets when
+// some system flags that term; a step in which no system of the term needs
+// new lists skips the rebuild's launches (on[g] = 0: no such node, the
+// rebuild always runs and filters the flagged systems itself).
+struct RebuildGate {
+    int on[NGLOBAL];
+    cudaGraphConditionalHandle handle[NGLOBAL];
+};
+void launch_margin(const Arena& a, TermArrays* t, cudaStream_t s, const RebuildGate& gate);
 void launch_integrate_last(const Arena& a, cudaStream_t s);
 void launch_zero_force(const Arena& a, cudaStream_t s);
 
