@@ -1949,14 +1949,6 @@ int mjg_get_state(mjg_context* c, int sys, double* pos, double* vel, double* for
     ABI_END(c)
 }
 
-[[maybe_unused]] static void mark_all_rebuild(mjg_context* c)
-{
-    download_sys(c);
-    for(auto& d : c->h_sys)
-        for(auto& g : d.g) {if(g.on) {g.rebuild = 1;}}
-    upload_sys(c);
-}
-
 int mjg_set_state(mjg_context* c, int sys, const double* pos, const double* vel)
 {
     ABI_BEGIN(c)
