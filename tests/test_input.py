@@ -314,3 +314,31 @@ def test_gjf_rejects_gammas(tmp_path):
     open(path, "w").write(text)
     with pytest.raises(I.InputError, match="gammas"):
         I.load(path)
+
+
+def test_names_groups_attributes_and_formats(tmp_path):
+    """Particle names and groups, the attributes as given and the output
+    formats reach the Input, and a checkpoint written with them carries the
+    names and groups the reference's saver would."""
+    from mjolnir_b200 import checkpoint as K
+    text = HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF
+    text = text.replace('output.format = "xyz"', 'output.format = ["xyz", "dcd", "trr"]')
+    inp = I.load(_write(tmp_path, "named.toml", text))
+    assert inp.names == ["X", "X", "X", "C"] and inp.groups == ["NONE"] * 4
+    assert inp.attributes == {"temperature": 300.0}
+    assert inp.output_formats == ["xyz", "dcd", "trr"]
+    assert inp.file_prefix.endswith("/" + inp.output_prefix)
+    d = inp.desc
+    path = str(tmp_path / "n_system.msg")
+    K.write_system(path, d.pos, d.vel, np.zeros_like(d.pos), d.mass, d.periodic, d.lower, d.upper,
+                   inp.attributes, inp.names, inp.groups)
+    back = K.read_system(path)
+    assert back["names"] == inp.names and back["groups"] == inp.groups
+    assert back["attributes"] == {"temperature": 300.0}
+
+
+def test_unknown_output_format_is_rejected(tmp_path):
+    text = HEAD.format(path=str(tmp_path) + "/") + SIM + SYSTEM + FF
+    text = text.replace('output.format = "xyz"', 'output.format = "pdb"')
+    with pytest.raises(I.InputError, match="pdb"):
+        I.load(_write(tmp_path, "bad_fmt.toml", text))
