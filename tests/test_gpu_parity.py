@@ -314,3 +314,38 @@ def test_build_lanes_give_the_same_lists(case, lanes):
     for a, b in zip(traj, e32.state(sid32)):
         assert np.array_equal(a, b), lanes
     e32.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_frozen_system_waits_and_resumes(precision):
+    """A frozen system keeps its state (positions, velocities, forces, step
+    counter) while the others advance; released, it continues as if it had
+    never paused (mixed form: bit for bit)."""
+    a = S.polymer_melt(nchains=3, nbeads=40, radius=40.0, seed=81)
+    b = S.polymer_melt(nchains=3, nbeads=40, radius=40.0, seed=82)
+    e = Engine(precision)
+    sa, sb = e.add_system(a), e.add_system(b)
+    e.commit()
+    e.step(20)
+    before = e.state(sa)
+    e.freeze(sa)
+    e.step(30)
+    after = e.state(sa)
+    for x, y in zip(before, after):
+        assert np.array_equal(x, y)
+    assert e.step_count(sa) == 20 and e.step_count(sb) == 50
+    e.freeze(sa, False)
+    e.step(25)
+    got = e.state(sa)
+    e.close()
+    ref_e = Engine(precision)
+    rid = ref_e.add_system(a)
+    ref_e.commit()
+    ref_e.step(45)
+    want = ref_e.state(rid)
+    ref_e.close()
+    for x, y in zip(got, want):
+        if precision == "mixed":
+            assert np.array_equal(x, y)
+        else:
+            assert np.abs(x - y).max() <= 1e-9 * max(1.0, np.abs(y).max())
