@@ -13,7 +13,9 @@ steps and at the end, ``<prefix>_system.msg`` and ``<prefix>_rng.msg``
 (:mod:`mjolnir_b200.checkpoint`).  The order of those calls is the one of
 core/MolecularDynamicsSimulator.hpp:72-125 and
 core/SimulatedAnnealingSimulator.hpp:121-150: observers and checkpoint before
-the step, the temperature update of an annealing run after it.
+the step, the temperature update of an annealing run after it.  The frames
+are formatted and written on a second thread, in order, while the GPU runs
+the next chunk.
 ``precision = "double"`` in the input selects the FP64 form unless
 ``--precision`` says otherwise (and sets the real type of the .trr file).
 """
@@ -21,7 +23,9 @@ from __future__ import annotations
 
 import argparse
 import os
+import queue
 import sys
+import threading
 import time
 
 import numpy as np
@@ -57,6 +61,42 @@ def present_terms(desc):
     return out
 
 
+class _Writer:
+    """Writes the observers' frames on a thread of its own, in order, while
+    the GPU runs the next chunk; at most `depth` frames wait.  An error in
+    the writer is raised at the next call."""
+
+    def __init__(self, observers, dt, depth=2):
+        self.obs, self.dt = observers, dt
+        self.q = queue.Queue(maxsize=depth)
+        self.err = None
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def _run(self):
+        while True:
+            item = self.q.get()
+            if item is None:
+                return
+            if self.err is None:
+                try:
+                    for o in self.obs:
+                        o.output(item[0], self.dt, item[1])
+                except Exception as e:          # re-raised in the caller's thread
+                    self.err = e
+
+    def put(self, step, frame):
+        if self.err is not None:
+            raise self.err
+        self.q.put((step, frame))
+
+    def close(self):
+        self.q.put(None)
+        self.t.join()
+        if self.err is not None:
+            raise self.err
+
+
 def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) -> dict:
     inp = load(path)
     d = inp.desc
@@ -81,7 +121,7 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
         p, v, f = eng.state(sid)
         e = eng.energies(sid)
         return O.Frame(pos=p, vel=v, force=f, mass=d.mass, energies=[(title, e[key]) for key, title in terms],
-                       attributes=attrs, names=inp.names, periodic=d.periodic, width=width,
+                       attributes=dict(attrs), names=inp.names, periodic=d.periodic, width=width,
                        molecules=molecules)
 
     def save_checkpoint():
@@ -94,12 +134,11 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
     fr = frame()
     for o in obs:
         o.initialize(total, save, d.dt, fr)
+    writer = _Writer(obs, d.dt)             # frames are formatted and written while the GPU steps
     done = 0
     while done < total:
         if done % save == 0:
-            fr = frame()
-            for o in obs:
-                o.output(done, d.dt, fr)
+            writer.put(done, frame())
         if done % ckpt == 0:
             save_checkpoint()
         k = min(save - done % save, ckpt - done % ckpt, total - done)
@@ -111,8 +150,8 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
             attrs["temperature"] = current(anneal[0], anneal[1], done * r_total)
             eng.set_temperature(sid, attrs["temperature"])
     fr = frame()                             # finalize: the last frame, then the checkpoint
-    for o in obs:
-        o.output(total, d.dt, fr)
+    writer.put(total, fr)
+    writer.close()
     for o in obs:
         o.finalize(total, d.dt, fr)
     save_checkpoint()
