@@ -148,78 +148,109 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def build_batch(nsys):
+def build_batch(nsys, synth=None):
     from mjolnir_b200 import systems as S
-    return S.polymer_batch(nsys=nsys, seed=SEED)
+    return S.polymer_batch(nsys=nsys, seed=SEED, synth=synth)
 
 
 # ---------------------------------------------------------------- reference
-def cpu_reference_rate(descs, budget_s=15.0, threads=None):
-    """The reference's own OpenMP path (oracle/_ref, OpenMPSimulatorTraits)
-    stepping the batch's systems one after another, as the reference would
-    run 256 separate simulations; returns (particle-steps/s, sample text,
-    threads).  Only the integrator steps are timed."""
+class ReferenceBatch:
+    """The reference's own OpenMP path (oracle/_ref: OpenMPSimulatorTraits,
+    BAOAB, cell lists, the unmodified reference headers) holding every system
+    of a batch, stepped one system after another as the reference would run
+    separate simulations.  Both the reference arm and the cpu_baseline leg
+    time the batch through this class, so the two agree by construction."""
+
+    def __init__(self, descs):
+        import oracle
+        self.descs = descs
+        self.n = sum(d.n for d in descs)
+        self.sims = []
+        for d in descs:
+            r = oracle.Reference(d, parallel=True)
+            r.initialize()
+            self.sims.append(r)
+        self.threads = oracle.Reference.max_threads()
+
+    def run(self, md_steps):
+        """Advances every system by md_steps; returns the seconds spent in
+        the reference's integrator steps (input and initialisation excluded)."""
+        return sum(r.run(md_steps) for r in self.sims)
+
+    def close(self):
+        for r in self.sims:
+            r.close()
+
+
+def omp_setup():
+    """OpenMP placement of the reference's threads: every host thread, bound
+    close (set before the reference library starts its runtime)."""
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    return {"omp_num_threads": os.environ["OMP_NUM_THREADS"], "omp_proc_bind": os.environ["OMP_PROC_BIND"]}
+
+
+def reference_descs(nsys):
+    """The benchmark batch built with the seeded builders as compiled into
+    the reference driver (oracle/_ref), so the reference arm never loads the
+    product library; the same source makes the same systems."""
+    import oracle
+    return build_batch(nsys, synth=oracle.synthetic_library())
+
+
+def cpu_reference_rate(descs, budget_s=12.0):
+    """cpu_baseline leg: a bounded sample of the timed workload on the
+    reference's OpenMP path -- every system of the batch, CHUNK-step rounds
+    until `budget_s` of integrator time; returns (particle-steps/s, sample
+    text, threads)."""
     import oracle
     if not oracle.reference_available():
         return None
-    sims, total_n, t_run, steps_done = [], 0, 0.0, 0
-    for d in descs:
-        r = oracle.Reference(d, parallel=True)
-        r.initialize()
-        sims.append(r)
-    nthreads = oracle.Reference.max_threads()
-    rounds = 0
-    while t_run < budget_s:
-        for r, d in zip(sims, descs):
-            t_run += r.run(1)
-            total_n += d.n
-        rounds += 1
-    for r in sims:
-        r.close()
-    sample = (f"{len(descs)} of the {NSYS} systems ({sum(d.n for d in descs)} beads), "
-              f"{rounds} MD steps each through OpenMPSimulatorTraits BAOAB")
-    return total_n / t_run, sample, nthreads
+    rb = ReferenceBatch(descs)
+    t, steps = 0.0, 0
+    md = max(1, CHUNK // 10)
+    while t < budget_s:
+        t += rb.run(md)
+        steps += md
+    rb.close()
+    sample = (f"all {len(descs)} systems ({rb.n} beads), {steps} MD steps each, one system after another "
+              f"through OpenMPSimulatorTraits BAOAB ({rb.threads} threads)")
+    return rb.n * steps / t, sample, rb.threads
 
 
 def run_reference_arm(args, ws, rank, pg):
-    """--impl reference: the reference's own CPU implementation on this
-    workload; each bench step = one MD step of every system of the batch."""
+    """--impl reference: the reference's own CPU implementation on the same
+    workload and config as the B200 arm; one bench step = CHUNK MD steps of
+    every system of the batch.  Under torchrun only rank 0 runs it."""
     if rank != 0:
         return
     import oracle
-    os.environ.setdefault("OMP_PROC_BIND", "close")
-    descs = build_batch(args.nsys)
+    omp = omp_setup()
     if not oracle.reference_available():
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference driver oracle/_ref was not built (reference tree absent at build time)"}))
         return
-    sims = []
-    for d in descs:
-        r = oracle.Reference(d, parallel=True)
-        r.initialize()
-        sims.append(r)
-    ntot = sum(d.n for d in descs)
+    descs = reference_descs(args.nsys)
+    rb = ReferenceBatch(descs)
     for _ in range(args.warmup):
-        for r in sims:
-            r.run(1)
+        rb.run(CHUNK)
     t = 0.0
     for _ in range(args.steps):
-        for r in sims:
-            t += r.run(1)
-    value = ntot * args.steps / t
-    threads = oracle.Reference.max_threads()
+        t += rb.run(CHUNK)
+    value = rb.n * CHUNK * args.steps / t
     line = {
         "metric": "particle-steps/s (batched polymer systems)", "value": value, "unit": "particle-steps/s",
         "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(descs, precision="fp64 (reference CPU)", chunk=1),
-        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
-                         "sample": f"all {len(descs)} systems, 1 MD step per bench step, OpenMPSimulatorTraits"},
+        "config": workload_config(descs),
+        "precision": "fp64 (the reference's OpenMP CPU path)",
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": rb.threads, "kind": "reference",
+                         "sample": f"all {len(descs)} systems, {CHUNK} MD steps per bench step, one system "
+                                   f"after another through OpenMPSimulatorTraits", **omp},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    for r in sims:
-        r.close()
+    rb.close()
     print(json.dumps(line))
 
 
@@ -348,14 +379,16 @@ def force_error(eng, descs, sids, local, nsample=16):
             "reference": "FP64 form on the mixed trajectory's coordinates after the timed steps"}
 
 
-def workload_config(descs, precision, chunk):
+def workload_config(descs):
+    """The workload both arms run (identical dicts in both JSON lines)."""
     return {
         "workload": "batch of 256 independent polymer melts (bonds, angles, dihedrals, "
                     "ExcludedVolume, DebyeHuckel), log-uniform 500-20000 beads, "
                     "T U[280,360] K, I U[0.05,0.3] M",
         "systems": len(descs), "particles": int(sum(d.n for d in descs)),
-        "md_steps_per_bench_step": chunk, "precision": precision,
-        "integrator": "BAOAB dt=0.01 gamma=1", "partition": "cell lists, margin 0.5",
+        "md_steps_per_bench_step": CHUNK,
+        "integrator": "BAOAB dt=0.01 gamma=1",
+        "partition": "cell lists (PeriodicGridCellList / UnlimitedGridCellList), relative margin per term",
         "l2": "inputs larger than L2 (resident arena of several hundred MB)",
     }
 
@@ -499,11 +532,12 @@ def run_b200(args, ws, rank, local, pg):
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
         try:
-            res = cpu_reference_rate(descs[:32], budget_s=12.0)
+            omp = omp_setup()
+            res = cpu_reference_rate(descs, budget_s=12.0)
             if res:
                 rate, sample, threads = res
                 cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
-                       "sample": sample}
+                       "sample": sample, **omp}
         except Exception as ex:  # the baseline must not sink the GPU line
             cpu = {"value": None, "error": str(ex)[:200]}
 
@@ -514,8 +548,10 @@ def run_b200(args, ws, rank, local, pg):
             "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 pair math, f64 state, i64 fixed-point forces",
             "data": "synthetic",
-            "config": {**workload_config(descs, precision="mixed", chunk=CHUNK),
-                       "autotuned": tuned},
+            "config": workload_config(descs),
+            "precision": "mixed: FP32 pair and bonded math from FP64 displacements, int64 fixed-point "
+                         "force sums, FP64 state and integrator",
+            "autotuned": tuned,
             "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,

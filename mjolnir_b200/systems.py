@@ -119,14 +119,28 @@ def lj_fluid(n: int = 4096, density: float = 0.8, jitter: float = 0.05,
                       single_molecule=True, dt=dt, gamma=np.full(n, gamma), seed=seed)
 
 
-def _random_walk_chains(nchains, nbeads, bond, min_dist, radius, seed):
+def _synth(lib):
+    """The library holding the seeded builders (include/mjolnir_b200_synthetic.h):
+    `lib` when given (any ctypes library exporting the mjg_synth_* symbols),
+    else libmjolnir_b200.so."""
+    if lib is not None:
+        return lib
+    from . import _capi as A
+    return A.lib()
+
+
+def _f64(a):
+    import ctypes as C
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _random_walk_chains(nchains, nbeads, bond, min_dist, radius, seed, synth=None):
     """Random-walk chains with `bond`-long steps from seed-drawn directions,
     rejecting any bead closer than `min_dist` to a bead other than the one it
     is bonded to, or outside the sphere of `radius` (native builder)."""
-    from . import _capi as A
     out = np.empty((nchains * nbeads, 3))
-    code = A.lib().mjg_synth_polymer_chains(nchains, nbeads, bond, min_dist, radius,
-                                            int(seed) & ((1 << 64) - 1), A.f64(out))
+    code = _synth(synth).mjg_synth_polymer_chains(nchains, nbeads, bond, min_dist, radius,
+                                                  int(seed) & ((1 << 64) - 1), _f64(out))
     if code != 0:
         raise RuntimeError(f"mjg_synth_polymer_chains failed ({code}); lower the density")
     return out
@@ -135,13 +149,14 @@ def _random_walk_chains(nchains, nbeads, bond, min_dist, radius, seed):
 def polymer_melt(nchains: int = 50, nbeads: int = 200, radius: float = 300.0,
                  charged_fraction: float = 0.2, temperature: float = 300.0,
                  ionic_strength: float = 0.1, dt: float = 0.01, gamma: float = 1.0,
-                 margin: float = 0.5, seed: int = 2, mass: float = 1.0) -> SystemDesc:
+                 margin: float = 0.5, seed: int = 2, mass: float = 1.0, synth=None) -> SystemDesc:
     """Coarse-grained polymer melt in unbounded space: harmonic bonds (k=100,
     r0=3.8), harmonic angles (k=10, 110 deg), cosine dihedrals (k=0.5, n=3,
     v0=0), ExcludedVolume (radius 2, eps 0.2, cutoff 2), DebyeHuckel on a
-    random `charged_fraction` of beads with charges +-1 and zero net charge."""
+    random `charged_fraction` of beads with charges +-1 and zero net charge.
+    `synth`: the library of the seeded builders (default libmjolnir_b200.so)."""
     rng = np.random.default_rng(seed)
-    pos = _random_walk_chains(nchains, nbeads, 3.8, 4.0, radius, seed)
+    pos = _random_walk_chains(nchains, nbeads, 3.8, 4.0, radius, seed, synth)
     n = pos.shape[0]
     m = np.full(n, mass)
     vel = maxwell_boltzmann(rng, m, KB_KCAL * temperature)
@@ -175,15 +190,15 @@ def polymer_melt(nchains: int = 50, nbeads: int = 200, radius: float = 300.0,
 def bead_fluid(n: int = 1 << 20, density: float = 0.003, charged_fraction: float = 0.3,
                temperature: float = 300.0, ionic_strength: float = 0.15,
                dt: float = 0.3, gamma: float = 1.0, margin: float = 0.5,
-               min_dist: float = 4.0, mass: float = 100.0, seed: int = 3) -> SystemDesc:
+               min_dist: float = 4.0, mass: float = 100.0, seed: int = 3, synth=None) -> SystemDesc:
     """Periodic EXV + Debye-Hueckel bead fluid: cubic box at number density
     `density`, uniform positions with overlaps below `min_dist` redrawn, charges
-    +-1 on `charged_fraction` of the beads with zero net charge."""
-    from . import _capi as A
+    +-1 on `charged_fraction` of the beads with zero net charge.  `synth`: the
+    library of the seeded builders (default libmjolnir_b200.so)."""
     rng = np.random.default_rng(seed)
     L = (n / density) ** (1.0 / 3.0)
     pos = np.empty((n, 3))
-    code = A.lib().mjg_synth_uniform_fluid(n, L, min_dist, int(seed) & ((1 << 64) - 1), A.f64(pos))
+    code = _synth(synth).mjg_synth_uniform_fluid(n, L, min_dist, int(seed) & ((1 << 64) - 1), _f64(pos))
     if code != 0:
         raise RuntimeError(f"mjg_synth_uniform_fluid failed ({code})")
     m = np.full(n, mass)
@@ -204,11 +219,12 @@ def bead_fluid(n: int = 1 << 20, density: float = 0.003, charged_fraction: float
 
 def polymer_batch(nsys: int = 256, nmin: int = 500, nmax: int = 20000, seed: int = 4,
                   beads_per_chain: int = 200, dt: float = 0.01, gamma: float = 1.0,
-                  margin: float = 0.5):
+                  margin: float = 0.5, synth=None):
     """Independent polymer melts built like :func:`polymer_melt`, sizes drawn
     log-uniform in [nmin, nmax] (chains of ~200 beads; the sphere radius keeps
     the 10,000-beads-in-300-A density), temperature U[280, 360] K and ionic
-    strength U[0.05, 0.3] M per system."""
+    strength U[0.05, 0.3] M per system.  `synth`: the library of the seeded
+    builders (default libmjolnir_b200.so)."""
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsys))
     temps = rng.uniform(280.0, 360.0, nsys)
@@ -220,7 +236,8 @@ def polymer_batch(nsys: int = 256, nmin: int = 500, nmax: int = 20000, seed: int
         radius = 300.0 * (nchains * nbeads / 10000.0) ** (1.0 / 3.0)
         out.append(polymer_melt(nchains=nchains, nbeads=nbeads, radius=radius,
                                 temperature=float(temps[k]), ionic_strength=float(ions[k]),
-                                dt=dt, gamma=gamma, margin=margin, seed=seed * 100003 + k))
+                                dt=dt, gamma=gamma, margin=margin, seed=seed * 100003 + k,
+                                synth=synth))
     return out
 
 

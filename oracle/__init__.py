@@ -168,14 +168,15 @@ def make_spec(desc):
 
 
 def build(reference_root: str | None = None) -> None:
-    """Compiles liboracle.so and, when the reference tree exists, the
-    reference driver into _ref/."""
+    """Compiles liboracle.so and, when `reference_root` (the root of the
+    reference tree; default: the environment variable MJOLNIR_REFERENCE_ROOT)
+    names a tree that exists, the reference driver into _ref/."""
     env = dict(os.environ)
     env.pop("CC", None)
     env.pop("CXX", None)
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True, env=env)
-    ref = reference_root or "/root/reference"
-    if os.path.isdir(os.path.join(ref, "mjolnir")):
+    ref = reference_root or os.environ.get("MJOLNIR_REFERENCE_ROOT")
+    if ref and os.path.isdir(os.path.join(ref, "mjolnir")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref}"], check=True, env=env)
 
 
@@ -464,3 +465,18 @@ class Reference(_Common):
     @staticmethod
     def max_threads():
         return _ref_lib().ref_max_threads()
+
+
+def synthetic_library():
+    """The seeded input builders (``mjg_synth_*`` of
+    include/mjolnir_b200_synthetic.h) as compiled into the reference driver,
+    so that the reference arm of bench.py builds the benchmark's systems
+    without loading the product library.  The same source file is compiled
+    into both libraries, so the systems are identical."""
+    lib = _ref_lib()
+    for name in ("mjg_synth_polymer_chains", "mjg_synth_uniform_fluid"):
+        getattr(lib, name).restype = C.c_int
+    lib.mjg_synth_polymer_chains.argtypes = [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                             C.c_uint64, _f64p]
+    lib.mjg_synth_uniform_fluid.argtypes = [C.c_int64, C.c_double, C.c_double, C.c_uint64, _f64p]
+    return lib
