@@ -332,14 +332,17 @@ MJG_API int mjg_launch_count(mjg_context* ctx, int64_t* launches);
  * NULL for the default stream).  Every particle takes part, no pair is
  * excluded, FP64 arithmetic -- the quantity mjg_term_force gives for
  * MJG_TERM_EXV of a system without ignore rules.  lower/upper (host, 3 each)
- * give the periodic box for MJG_PERIODIC_CUBOID, whose positions must lie
- * inside it; they are ignored for MJG_UNLIMITED.
+ * give the periodic box for MJG_PERIODIC_CUBOID; positions may lie outside it
+ * by up to a quarter of its width on each side (cells wrap, and each
+ * displacement takes one periodic shift, as the reference's adjust_direction);
+ * they are ignored for MJG_UNLIMITED.
  *
  * The call allocates nothing: its cell list lives in one fixed device array of
  * about 1 MiB that every GPU loading the library keeps until the process
  * exits, which limits n to 65536 (larger n returns MJG_EINVAL and prints the
- * limit).  The first call on a device looks up that array's device address;
- * make this first call before any stream capture.  All calls share the array:
+ * limit).  The first call in a CUDA context (the first on a device, and the
+ * first after a device reset) looks up that array's device address; make it
+ * before any stream capture.  All calls share the array:
  * calls that overlap on the GPU (other streams, other threads) race and give
  * wrong results, so serialise them. */
 MJG_API int mjg_exv_force_noalloc(int64_t n, int boundary, const double* lower,

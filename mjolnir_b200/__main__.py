@@ -136,22 +136,24 @@ def run(path: str, precision=None, device: int = 0, steps=None, out=sys.stderr) 
         o.initialize(total, save, d.dt, fr)
     writer = _Writer(obs, d.dt)             # frames are formatted and written while the GPU steps
     done = 0
-    while done < total:
-        if done % save == 0:
-            writer.put(done, frame())
-        if done % ckpt == 0:
-            save_checkpoint()
-        k = min(save - done % save, ckpt - done % ckpt, total - done)
-        if anneal:
-            k = min(k, anneal[2] - done % anneal[2])
-        eng.step(k)
-        done += k
-        if anneal and done % anneal[2] == 0:    # core/SimulatedAnnealingSimulator.hpp:144-154
-            attrs["temperature"] = current(anneal[0], anneal[1], done * r_total)
-            eng.set_temperature(sid, attrs["temperature"])
-    fr = frame()                             # finalize: the last frame, then the checkpoint
-    writer.put(total, fr)
-    writer.close()
+    try:
+        while done < total:
+            if done % save == 0:
+                writer.put(done, frame())
+            if done % ckpt == 0:
+                save_checkpoint()
+            k = min(save - done % save, ckpt - done % ckpt, total - done)
+            if anneal:
+                k = min(k, anneal[2] - done % anneal[2])
+            eng.step(k)
+            done += k
+            if anneal and done % anneal[2] == 0:    # core/SimulatedAnnealingSimulator.hpp:144-154
+                attrs["temperature"] = current(anneal[0], anneal[1], done * r_total)
+                eng.set_temperature(sid, attrs["temperature"])
+        fr = frame()                         # finalize: the last frame, then the checkpoint
+        writer.put(total, fr)
+    finally:
+        writer.close()                       # frames already queued are written, even on an error
     for o in obs:
         o.finalize(total, d.dt, fr)
     save_checkpoint()

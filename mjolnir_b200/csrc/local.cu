@@ -467,9 +467,10 @@ void launch_local(const Arena& a, const LocalArrays& l, int mask, bool nf, bool 
     }
     else
     {
-        if(nf && ne) {run_all<P_MIXED, true, true>(a, l, mask, s);}
-        else if(nf)  {run_all<P_MIXED, true, false>(a, l, mask, s);}
-        else if(ne)  {run_all<P_MIXED, false, true>(a, l, mask, s);}
+        // mixed form: forces in FP32 (the per-step path); energies, an
+        // observable read between steps, in the reference's FP64 arithmetic
+        if(nf)       {run_all<P_MIXED, true, false>(a, l, mask, s);}
+        if(ne)       {run_all<P_FP64, false, true>(a, l, mask, s);}
     }
 }
 

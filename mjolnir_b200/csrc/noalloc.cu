@@ -104,8 +104,10 @@ __device__ __forceinline__ int na_coord(const NaScratch* sc, const NaBox& box, d
     const int d = sc->header[axis];
     if(box.periodic)
     {
-        long long c = (long long)floor((x - box.lower[axis]) / (box.width[axis] / d));
-        return (int)(c < 0 ? 0 : (c >= d ? d - 1 : c));
+        // wrapped: a particle a little outside [lower, upper) lands in the
+        // cell its periodic image occupies, next to its image neighbours
+        long long c = (long long)floor((x - box.lower[axis]) / (box.width[axis] / d)) % d;
+        return (int)(c < 0 ? c + d : c);
     }
     long long c = (long long)floor(x * sc->inv_w) % d;
     return (int)(c < 0 ? c + d : c);
@@ -225,9 +227,41 @@ __global__ void k_na_force(const NaScratch* sc, long long n, const double* pos, 
     if((threadIdx.x & 31) == 0 && e != 0.0) {atomicAdd(energy, e);}
 }
 
-// device address of the scratch array, looked up once per device
+// Device address of the scratch array, looked up once per CUDA context: the
+// address belongs to the context that was current at the lookup, and a device
+// reset (cudaDeviceReset, or a host framework resetting the primary context)
+// makes a new context in which the array has a new address.  The current
+// context is read through the driver's cuCtxGetCurrent, found at run time so
+// that the library does not link against the driver.
 std::mutex g_na_mutex;
-NaScratch* g_na_ptr[64] = {};
+struct NaSlot {
+    void* ctx;
+    NaScratch* ptr;
+};
+NaSlot g_na_slots[64] = {};
+int g_na_nslots = 0;
+using CtxGetCurrent = int (*)(void**);
+CtxGetCurrent g_ctx_get_current = nullptr;
+
+// the current context (nullptr when none is current or the driver does not
+// say); called with g_na_mutex held
+void* current_context()
+{
+    if(!g_ctx_get_current)
+    {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if(cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+           q != cudaDriverEntryPointSuccess || !fn)
+        {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrent>(fn);
+    }
+    void* ctx = nullptr;
+    return g_ctx_get_current(&ctx) == 0 ? ctx : nullptr;
+}
 
 }  // namespace
 }  // namespace mjg
@@ -262,11 +296,22 @@ extern "C" MJG_API int mjg_exv_force_noalloc(int64_t n, int boundary, const doub
         }
     }
     int dev = 0;
-    if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {cudaGetLastError(); return MJG_ECUDA;}
+    if(cudaGetDevice(&dev) != cudaSuccess || dev < 0) {cudaGetLastError(); return MJG_ECUDA;}
     NaScratch* sc = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_na_mutex);
-        if(!g_na_ptr[dev])
+        // the first call in a context (the first on a device, or the first
+        // after a reset) has the runtime make the device's primary context
+        // current (cudaSetDevice initialises it), then looks the array's
+        // address up in it; without a context handle the address is looked
+        // up on every call
+        if(cudaSetDevice(dev) != cudaSuccess) {cudaGetLastError(); return MJG_ECUDA;}
+        void* ctx = current_context();
+        for(int k = 0; k < g_na_nslots && ctx; ++k)
+        {
+            if(g_na_slots[k].ctx == ctx) {sc = g_na_slots[k].ptr; break;}
+        }
+        if(!sc)
         {
             void* p = nullptr;
             if(cudaGetSymbolAddress(&p, g_na_scratch) != cudaSuccess || !p)
@@ -274,9 +319,15 @@ extern "C" MJG_API int mjg_exv_force_noalloc(int64_t n, int boundary, const doub
                 cudaGetLastError();
                 return MJG_ECUDA;
             }
-            g_na_ptr[dev] = static_cast<NaScratch*>(p);
+            sc = static_cast<NaScratch*>(p);
+            if(ctx)
+            {
+                // keep at most 64 contexts; the oldest entry gives way
+                if(g_na_nslots < 64) {++g_na_nslots;}
+                for(int k = g_na_nslots - 1; k > 0; --k) {g_na_slots[k] = g_na_slots[k - 1];}
+                g_na_slots[0] = NaSlot{ctx, sc};
+            }
         }
-        sc = g_na_ptr[dev];
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const unsigned nb = (unsigned)((n + NA_TPB - 1) / NA_TPB);

@@ -828,9 +828,22 @@ void launch_pair(const Arena& a, int g, TermArrays& t, bool need_force, bool nee
     }
     else
     {
-        if(g == G_EXV)     {dispatch<P_MIXED, G_EXV>(a, t, need_force, need_energy, s);}
-        else if(g == G_DH) {dispatch<P_MIXED, G_DH >(a, t, need_force, need_energy, s);}
-        else               {dispatch<P_MIXED, G_LJ >(a, t, need_force, need_energy, s);}
+        // mixed form: forces in FP32 with fixed-point sums (the per-step
+        // path); energies, an observable read between steps, in the
+        // reference's FP64 arithmetic
+        if(need_force)
+        {
+            if(g == G_EXV)     {dispatch<P_MIXED, G_EXV>(a, t, true, false, s);}
+            else if(g == G_DH) {dispatch<P_MIXED, G_DH >(a, t, true, false, s);}
+            else               {dispatch<P_MIXED, G_LJ >(a, t, true, false, s);}
+        }
+        if(need_energy)
+        {
+            if(need_force) {note_launches(1);}
+            if(g == G_EXV)     {dispatch<P_FP64, G_EXV>(a, t, false, true, s);}
+            else if(g == G_DH) {dispatch<P_FP64, G_DH >(a, t, false, true, s);}
+            else               {dispatch<P_FP64, G_LJ >(a, t, false, true, s);}
+        }
     }
 }
 

@@ -56,3 +56,29 @@ def rel_rms(a, b):
     den = float((np.asarray(b) ** 2).sum())
     num = float(((np.asarray(a) - np.asarray(b)) ** 2).sum())
     return (num / den) ** 0.5 if den > 0 else num ** 0.5
+
+
+def sha256(a) -> str:
+    import hashlib
+    import numpy as np
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def config_cases():
+    """{name: (SystemDesc, vv_dt, subset, fixture dict)} for the
+    configuration-size fixtures of tests/golden/make_configs.py; each system is
+    rebuilt by the same seeded builders, and its coordinates must hash to the
+    stored SHA-256 (the fixtures do not store the inputs)."""
+    import importlib.util
+    import numpy as np
+    path = os.path.join(ROOT, "tests", "golden", "make_configs.py")
+    spec = importlib.util.spec_from_file_location("make_configs", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    out = {}
+    for name, (d, dt, sub) in mod.cases().items():
+        fx = dict(np.load(os.path.join(ROOT, "tests", "golden", name + ".npz")))
+        assert sha256(d.pos) == str(fx["pos_sha"]) and sha256(d.vel) == str(fx["vel_sha"]), \
+            f"{name}: the seeded builders no longer make the fixture's system"
+        out[name] = (d, dt, sub, fx)
+    return out

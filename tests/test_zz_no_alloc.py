@@ -75,3 +75,51 @@ def test_noalloc_rejects_oversize():
     upper = (C.c_double * 3)(1, 1, 1)
     code = A.lib().mjg_exv_force_noalloc(65537, A.PERIODIC_CUBOID, lower, upper, 1, 1, 0.2, 2.0, 1, 1, None)
     assert code == A.EINVAL
+
+
+def test_noalloc_small_box_large_grid_and_outside_positions():
+    # a periodic box narrower than three cutoffs (the grid is held at 3 cells
+    # per axis), a box whose cutoff would ask for more cells than the scratch
+    # array holds (the grid is shrunk to fit), and particles pushed outside
+    # the box by up to a fifth of its width (their cells wrap): each against
+    # the context path on the same system with the positions wrapped back
+    small = S.bead_fluid(n=64, density=0.006, seed=63, dt=0.3)
+    small.dh = None
+    assert small.upper[0] - small.lower[0] < 3 * (2 * 2.0 * small.exv.cutoff)
+    big = S.bead_fluid(n=20000, density=0.0005, seed=64, dt=0.3)
+    big.dh = None
+    big.exv.cutoff = 1.2                  # rc = 4.8 A: 70 cells per axis asked, 64^3 > the limit
+    outside = S.bead_fluid(n=3000, density=0.003, seed=65, dt=0.3)
+    outside.dh = None
+    W = np.array(outside.upper) - np.array(outside.lower)
+    rng = np.random.default_rng(65)
+    shift = rng.integers(-1, 2, size=outside.pos.shape) * W
+    near_edge = (outside.pos < outside.lower[0] + 0.2 * W) | (outside.pos > outside.upper[0] - 0.2 * W)
+    moved = outside.pos + np.where(near_edge, shift, 0.0)
+    moved = np.where(np.abs(moved - outside.pos.mean()) < 0.7 * W, moved, outside.pos)
+    for d, tol in ((small, 1e-12), (big, 1e-12)):
+        f_ref, e_ref = context_exv(d)
+        f, e = noalloc_exv(d)
+        assert rel_rms(f, f_ref) <= tol
+        assert abs(e - e_ref) <= tol * max(abs(e_ref), 1e-12)
+    f_ref, e_ref = context_exv(outside)
+    out = outside.copy()
+    out.pos = moved
+    assert (moved < outside.lower[0]).any() or (moved >= outside.upper[0]).any()
+    f, e = noalloc_exv(out)
+    assert rel_rms(f, f_ref) <= 1e-10       # displacements taken across a shift round differently
+    assert abs(e - e_ref) <= 1e-10 * abs(e_ref)
+
+
+def test_noalloc_allocates_nothing_per_call():
+    import torch
+    d = S.bead_fluid(n=2000, density=0.003, seed=66, dt=0.3)
+    d.dh = None
+    noalloc_exv(d)                        # the first call may load the module holding the array
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for _ in range(3):
+        noalloc_exv(d)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
