@@ -53,6 +53,8 @@ def parse():
                     help="seconds of the Poisson serving run; 0 skips it")
     ap.add_argument("--no-fluid", action="store_true",
                     help="skip the pair-kernel roofline on the 1,048,576-bead periodic fluid")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the 2,000-step precision report on the 1,048,576-bead fluid")
     return ap.parse_args()
 
 
@@ -136,6 +138,23 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def ncu_traffic(key, schedule, slots):
+    """(DRAM bytes of one launch, source text) from profiles/ncu_traffic.json
+    for the kernel `key` captured with the same schedule, scaled by slots;
+    (None, reason) when no capture of that kernel and schedule is recorded."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            rec = json.load(f)[key]
+    except Exception:
+        return None, "no ncu capture recorded for this kernel"
+    if rec.get("schedule") != schedule:
+        return None, f"the recorded capture is of schedule {rec.get('schedule')}, this launch runs {schedule}"
+    b = (rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["slots"] * slots
+    return b, (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch ({rec['kernel']}, "
+               f"{rec['slots']} slots, commit {rec.get('commit', '?')}), scaled by slots; profiles/ncu_traffic.json")
 
 
 def measured_peaks():
@@ -463,36 +482,33 @@ def run_b200(args, ws, rank, local, pg):
     kern = pair_kernels(eng, descs, -1, "mixed")
     dom = max(kern, key=lambda k: kern[k]["ms"])
     k = kern[dom]
-    # DRAM bytes (read + write) of one launch from the ncu capture summarised
-    # in profiles/k_pair_batch256_mixed.md, per slot of the captured launch,
-    # scaled to this launch by its slots
-    ncu_bytes_per_slot = {"exv": 194.5e6 / 1563757, "dh": 118.8e6 / 312662}
-    traffic = ncu_bytes_per_slot[dom] * k["slots"] if dom in ncu_bytes_per_slot else None
+    # DRAM bytes (read + write) of one launch of this kernel as ncu measured
+    # them (profiles/ncu_traffic.json: per kernel and workload, the capture's
+    # bytes and slots), scaled to this launch by its slots
+    traffic, traffic_src = ncu_traffic(f"batch256_{dom}", eng.get_pair_schedule(dom), k["slots"])
     local_ms = {t: eng.time_kernel(t, reps=20) for t in ("bond", "angle", "dihedral")}
     shape = eng.get_pair_schedule(dom), eng.get_threads_per_particle(dom), eng.get_pair_unroll(dom)
     roofline = {"bound": "hbm", "kernel": f"pair force kernel of {dom} (schedule {shape[0]}, "
                 f"{shape[1]} threads or words per slot, {shape[2]} partners per batch)",
                 "achieved": k["gbs"], "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": k["gbs"] / peak, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                                  "profiles/k_pair_batch256_mixed.md, scaled by slots",
+                "traffic_source": traffic_src,
                 "timing": "CUDA events per launch on the library stream, L2 evicted before each launch",
                 "ms_per_launch": k["ms"], "pairs_in_cutoff": k["pcut"],
                 "algorithmic_bytes": k["bytes"], "other": {t: kern[t] for t in kern if t != dom},
                 "local_ms_per_launch": local_ms}
 
-    # ---- plain single-system FP64 path on a sample of the same systems
+    # ---- plain single-system FP64 path: every system of the batch, one at a time
     plain = None
     if not args.no_plain and rank == 0:
-        sample = descs[: min(16, len(descs))]
         tot_ps, tot_t = 0, 0.0
-        for d in sample:
-            pe = Engine("fp64", device=local)
-            pe.add_system(d)
+        pe = Engine("fp64", device=local)
+        ps = torch.cuda.ExternalStream(pe.stream_handle(), device=local)
+        for d in descs:
+            sid = pe.add_system(d)
             pe.commit()
             pe.step(5)
             pe.synchronize()
-            ps = torch.cuda.ExternalStream(pe.stream_handle(), device=local)
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(ps)
@@ -501,9 +517,11 @@ def run_b200(args, ws, rank, local, pg):
             b.synchronize()
             tot_t += a.elapsed_time(b) / 1e3
             tot_ps += d.n * CHUNK
-            pe.close()
+            pe.remove_system(sid)
+        pe.close()
         plain = {"value": tot_ps / tot_t, "unit": "particle-steps/s",
-                 "sample": f"{len(sample)} systems run one at a time, FP64, {CHUNK} steps each",
+                 "sample": f"all {len(descs)} systems run one at a time (one system per arena), FP64, "
+                           f"{CHUNK} MD steps each, CUDA events per system",
                  "batched_over_plain": value / ws / (tot_ps / tot_t)}
 
     # ---- force error of the timed mixed-form run against the FP64 form
@@ -518,6 +536,19 @@ def run_b200(args, ws, rank, local, pg):
     fluid = None
     if not args.no_fluid and rank == 0:
         fluid = fluid_pair_roofline(local, peak)
+
+    # ---- precision at scale: the fluid's mixed trajectory against the FP64 form
+    prec = None
+    if not args.no_precision and rank == 0:
+        from mjolnir_b200 import precision
+        res = precision.run(steps=2000, every=1000, device=local)
+        prec = {k: res[k] for k in ("beads", "steps", "every", "margin", "worst_force_rel_rms",
+                                    "worst_total_force_rel_rms", "worst_energy_rel", "rebuilds")}
+        prec["frames"] = [{"step": f["step"], **{t: f[t]["force_rel_rms"] for t in ("exv", "dh")},
+                           "total": f["total_force_rel_rms"]} for f in res["frames"]]
+        prec["bound"] = 1e-5
+        prec["note"] = ("forces: mixed form vs the FP64 form on the mixed trajectory's coordinates every "
+                        "1,000 steps; energies are evaluated in FP64 in both forms")
 
     # ---- serving: Poisson arrivals at 200 jobs/s, continuous batching
     serving = None
@@ -562,6 +593,7 @@ def run_b200(args, ws, rank, local, pg):
             "single_system_configs": small,
             "force_error": ferr,
             "fluid_1m_pair_kernels": fluid,
+            "precision_fluid_1m": prec,
             "serving": serving,
         }
         print(json.dumps(line))

@@ -52,13 +52,20 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     env.pop("CXX", None)
     objs = []
     extra = ["-Xptxas", "-v"] if ptxas_info else []
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) \
+        + glob.glob(os.path.join(INCLUDE, "*.h"))
+    newest_header = max((os.path.getmtime(h) for h in headers), default=0.0)
     for src in sources():
         obj = os.path.join(build_dir, os.path.basename(src) + ".o")
+        objs.append(obj)
+        # an object is recompiled when its source or any header is newer
+        if not force and not ptxas_info and os.path.exists(obj) and \
+                os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_header):
+            continue
         cmd = [nvcc(), *ARCH, *NVFLAGS, *extra, "-I", INCLUDE, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True, env=env)
-        objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     subprocess.run(cmd, check=True, env=env)

@@ -48,6 +48,10 @@ struct TermArrays {
                                 // 4 = as 0 with a block's thread groups ordered by list length
     int        any_periodic;    // some system with this term has a periodic box
     int        build_lanes;     // lanes per slot of the list build (8, 16 or 32)
+    int        fe_energy;       // energy-only launch: sum the energy as calc_force_and_energy does
+                                // (the generic pair loop skips pairs whose force is zero,
+                                // GlobalPairInteraction.hpp:148-213) instead of calc_energy's
+                                // every listed pair
     const int* part_particle;   // [np] global particle index
     const double* part_p0;      // [np] radius / charge / sigma
     const double* part_p1;      // [np] LJ epsilon

@@ -1,5 +1,7 @@
 // Local (bonded) terms; the FP64 form keeps the reference's formulas, the
-// mixed form evaluates them in FP32 from FP64 displacements (see below):
+// mixed form evaluates them in FP32 from FP64 displacements, and with the
+// FP64 formulas where a bond angle is within 11.5 degrees of collinear (see
+// below):
 //   BondLength + Harmonic   forcefield/local/BondLengthInteraction.hpp:126-199,
 //                           forcefield/local/HarmonicPotential.hpp:25-35 (V = k (v - v0)^2)
 //   BondAngle  + Harmonic   forcefield/local/BondAngleInteraction.hpp:129-188
@@ -156,15 +158,14 @@ __device__ __forceinline__ void do_bond(Arena& a, const LocalArrays& l, long lon
     if(NE) {reduce_energy(a, sys, active, e, T_BOND);}
 }
 
+// the reference's formulas for one (active) angle: adds its forces, returns
+// its energy (NE)
 template<int PREC, bool NF, bool NE>
-__device__ __forceinline__ void do_angle(Arena& a, const LocalArrays& l, long long b, bool active,
-                                         Window<PREC>& W)
+__device__ __forceinline__ double angle_fp64(Arena& a, const LocalArrays& l, long long b, Window<PREC>& W)
 {
-    const int sys = active ? l.angle_sys[b] : 0;
     double e = 0.0;
-    if(active)
+    const SysDev& S = a.sys[l.angle_sys[b]];
     {
-        const SysDev& S = a.sys[sys];
         const int i0 = l.angle_idx[3 * b], i1 = l.angle_idx[3 * b + 1], i2 = l.angle_idx[3 * b + 2];
         const double k = l.angle_k[b], v0 = l.angle_v0[b];
         const double4 p1 = a.pos[i1];
@@ -191,18 +192,26 @@ __device__ __forceinline__ void do_angle(Arena& a, const LocalArrays& l, long lo
             W.add(a.force, i2, Fk.x, Fk.y, Fk.z);
         }
     }
-    if(NE) {reduce_energy(a, sys, active, e, T_ANGLE);}
+    return e;
 }
 
 template<int PREC, bool NF, bool NE>
-__device__ __forceinline__ void do_dihedral(Arena& a, const LocalArrays& l, long long b, bool active,
+__device__ __forceinline__ void do_angle(Arena& a, const LocalArrays& l, long long b, bool active,
                                          Window<PREC>& W)
 {
-    const int sys = active ? l.dihd_sys[b] : 0;
+    const int sys = active ? l.angle_sys[b] : 0;
+    const double e = active ? angle_fp64<PREC, NF, NE>(a, l, b, W) : 0.0;
+    if(NE) {reduce_energy(a, sys, active, e, T_ANGLE);}
+}
+
+// the reference's formulas for one (active) dihedral: adds its forces,
+// returns its energy (NE)
+template<int PREC, bool NF, bool NE>
+__device__ __forceinline__ double dihedral_fp64(Arena& a, const LocalArrays& l, long long b, Window<PREC>& W)
+{
     double e = 0.0;
-    if(active)
+    const SysDev& S = a.sys[l.dihd_sys[b]];
     {
-        const SysDev& S = a.sys[sys];
         const int i0 = l.dihd_idx[4 * b], i1 = l.dihd_idx[4 * b + 1];
         const int i2 = l.dihd_idx[4 * b + 2], i3 = l.dihd_idx[4 * b + 3];
         const double K = l.dihd_k[b], v0 = l.dihd_v0[b];
@@ -241,10 +250,22 @@ __device__ __forceinline__ void do_dihedral(Arena& a, const LocalArrays& l, long
             W.add(a.force, i3, Fl.x, Fl.y, Fl.z);
         }
     }
+    return e;
+}
+
+template<int PREC, bool NF, bool NE>
+__device__ __forceinline__ void do_dihedral(Arena& a, const LocalArrays& l, long long b, bool active,
+                                         Window<PREC>& W)
+{
+    const int sys = active ? l.dihd_sys[b] : 0;
+    const double e = active ? dihedral_fp64<PREC, NF, NE>(a, l, b, W) : 0.0;
     if(NE) {reduce_energy(a, sys, active, e, T_DIHEDRAL);}
 }
 
 // ----------------------------------------------------------- mixed form
+// sin of a bond angle below which an angle or dihedral is evaluated with the
+// FP64 formulas instead (ill-conditioned in FP32)
+constexpr float ILL_SIN = 0.2f;
 // The same terms in FP32 from FP64 displacements: bond stretch via
 // (r^2 - v0^2) / (r + v0) with r^2 - v0^2 in FP64, the angle from atan2 of the
 // cross and dot products, the dihedral from (cos phi, sin phi) of the normals
@@ -309,20 +330,29 @@ __device__ __forceinline__ void do_angle_f32(Arena& a, const LocalArrays& l, lon
         const float3 ekj = make_float3(rkj.x * inv_kj, rkj.y * inv_kj, rkj.z * inv_kj);
         const float3 cr = fcross(eij, ekj);
         const float sin_t = sqrtf(fdot(cr, cr));
-        const float cos_t = fdot(eij, ekj);
-        const float theta = atan2f(sin_t, cos_t);
-        const float dv = theta - kv.y;
-        if(NE) {e = (double)(kv.x * dv * dv);}
-        if(NF)
+        if(sin_t < ILL_SIN)
         {
-            const float cis = -(2.0f * kv.x * dv) / fmaxf(sin_t, 1e-8f);
-            const float ci = cis * inv_ij, ck = cis * inv_kj;
-            const float cc = fminf(fmaxf(cos_t, -1.0f), 1.0f);
-            const double3 Fi = make_double3(ci * (cc * eij.x - ekj.x), ci * (cc * eij.y - ekj.y), ci * (cc * eij.z - ekj.z));
-            const double3 Fk = make_double3(ck * (cc * ekj.x - eij.x), ck * (cc * ekj.y - eij.y), ck * (cc * ekj.z - eij.z));
-            W.add(a.force, i0, Fi.x, Fi.y, Fi.z);
-            W.add(a.force, i1, -Fi.x - Fk.x, -Fi.y - Fk.y, -Fi.z - Fk.z);
-            W.add(a.force, i2, Fk.x, Fk.y, Fk.z);
+            // within 11.5 degrees of collinear the FP32 cross products and
+            // differences of unit vectors lose the force: the FP64 formulas
+            e = angle_fp64<PREC, NF, NE>(a, l, b, W);
+        }
+        else
+        {
+            const float cos_t = fdot(eij, ekj);
+            const float theta = atan2f(sin_t, cos_t);
+            const float dv = theta - kv.y;
+            if(NE) {e = (double)(kv.x * dv * dv);}
+            if(NF)
+            {
+                const float cis = -(2.0f * kv.x * dv) / fmaxf(sin_t, 1e-8f);
+                const float ci = cis * inv_ij, ck = cis * inv_kj;
+                const float cc = fminf(fmaxf(cos_t, -1.0f), 1.0f);
+                const double3 Fi = make_double3(ci * (cc * eij.x - ekj.x), ci * (cc * eij.y - ekj.y), ci * (cc * eij.z - ekj.z));
+                const double3 Fk = make_double3(ck * (cc * ekj.x - eij.x), ck * (cc * ekj.y - eij.y), ck * (cc * ekj.z - eij.z));
+                W.add(a.force, i0, Fi.x, Fi.y, Fi.z);
+                W.add(a.force, i1, -Fi.x - Fk.x, -Fi.y - Fk.y, -Fi.z - Fk.z);
+                W.add(a.force, i2, Fk.x, Fk.y, Fk.z);
+            }
         }
     }
     if(NE) {reduce_energy(a, sys, active, e, T_ANGLE);}
@@ -353,40 +383,50 @@ __device__ __forceinline__ void do_dihedral_f32(Arena& a, const LocalArrays& l, 
         const float3 n = fcross(r_kj, r_kl);
         const float m_lensq = fdot(m, m);
         const float n_lensq = fdot(n, n);
-        // (cos phi, sin phi) of the reference's phi = copysign(acos(m.n), r_ij.n)
-        const float x = fdot(m, n);
-        const float y = r_kj_len * fdot(r_ij, n);
-        const float h = rsqrtf(x * x + y * y);
-        const float c1 = x * h, s1 = y * h;
-        float cn = 1.0f, sn = 0.0f;
-        const int na = nn < 0 ? -nn : nn;
-        for(int q = 0; q < na; ++q)
+        if(m_lensq < ILL_SIN * ILL_SIN * fdot(r_ij, r_ij) * r_kj_lensq ||
+           n_lensq < ILL_SIN * ILL_SIN * fdot(r_kl, r_kl) * r_kj_lensq)
         {
-            const float c2 = cn * c1 - sn * s1;
-            sn = sn * c1 + cn * s1;
-            cn = c2;
+            // a bond angle of the dihedral within 11.5 degrees of collinear:
+            // the normals m, n lose their direction in FP32
+            e = dihedral_fp64<PREC, NF, NE>(a, l, b, W);
         }
-        if(nn < 0) {sn = -sn;}
-        // cos, sin of n (phi - v0)
-        const float cd = cn * p.y + sn * p.z;
-        const float sd = sn * p.y - cn * p.z;
-        if(NE) {e = (double)(p.x * (1.0f + cd));}
-        if(NF)
+        else
         {
-            const float coef = p.x * (float)nn * sd;     // -dV/dphi
-            const float cfi =  coef * r_kj_len / m_lensq;
-            const float cfl = -coef * r_kj_len / n_lensq;
-            const float3 Fi = make_float3(cfi * m.x, cfi * m.y, cfi * m.z);
-            const float3 Fl = make_float3(cfl * n.x, cfl * n.y, cfl * n.z);
-            const float rl2 = r_kj_rlen * r_kj_rlen;
-            const float cijk = fdot(r_ij, r_kj) * rl2;
-            const float cjkl = fdot(r_kl, r_kj) * rl2;
-            W.add(a.force, i0, Fi.x, Fi.y, Fi.z);
-            W.add(a.force, i1, (cijk - 1.0f) * Fi.x - cjkl * Fl.x, (cijk - 1.0f) * Fi.y - cjkl * Fl.y,
-                  (cijk - 1.0f) * Fi.z - cjkl * Fl.z);
-            W.add(a.force, i2, (cjkl - 1.0f) * Fl.x - cijk * Fi.x, (cjkl - 1.0f) * Fl.y - cijk * Fi.y,
-                  (cjkl - 1.0f) * Fl.z - cijk * Fi.z);
-            W.add(a.force, i3, Fl.x, Fl.y, Fl.z);
+            // (cos phi, sin phi) of the reference's phi = copysign(acos(m.n), r_ij.n)
+            const float x = fdot(m, n);
+            const float y = r_kj_len * fdot(r_ij, n);
+            const float h = rsqrtf(x * x + y * y);
+            const float c1 = x * h, s1 = y * h;
+            float cn = 1.0f, sn = 0.0f;
+            const int na = nn < 0 ? -nn : nn;
+            for(int q = 0; q < na; ++q)
+            {
+                const float c2 = cn * c1 - sn * s1;
+                sn = sn * c1 + cn * s1;
+                cn = c2;
+            }
+            if(nn < 0) {sn = -sn;}
+            // cos, sin of n (phi - v0)
+            const float cd = cn * p.y + sn * p.z;
+            const float sd = sn * p.y - cn * p.z;
+            if(NE) {e = (double)(p.x * (1.0f + cd));}
+            if(NF)
+            {
+                const float coef = p.x * (float)nn * sd;     // -dV/dphi
+                const float cfi =  coef * r_kj_len / m_lensq;
+                const float cfl = -coef * r_kj_len / n_lensq;
+                const float3 Fi = make_float3(cfi * m.x, cfi * m.y, cfi * m.z);
+                const float3 Fl = make_float3(cfl * n.x, cfl * n.y, cfl * n.z);
+                const float rl2 = r_kj_rlen * r_kj_rlen;
+                const float cijk = fdot(r_ij, r_kj) * rl2;
+                const float cjkl = fdot(r_kl, r_kj) * rl2;
+                W.add(a.force, i0, Fi.x, Fi.y, Fi.z);
+                W.add(a.force, i1, (cijk - 1.0f) * Fi.x - cjkl * Fl.x, (cijk - 1.0f) * Fi.y - cjkl * Fl.y,
+                      (cijk - 1.0f) * Fi.z - cjkl * Fl.z);
+                W.add(a.force, i2, (cjkl - 1.0f) * Fl.x - cijk * Fi.x, (cjkl - 1.0f) * Fl.y - cijk * Fi.y,
+                      (cjkl - 1.0f) * Fl.z - cijk * Fi.z);
+                W.add(a.force, i3, Fl.x, Fl.y, Fl.z);
+            }
         }
     }
     if(NE) {reduce_energy(a, sys, active, e, T_DIHEDRAL);}
@@ -398,8 +438,11 @@ __device__ __forceinline__ void do_dihedral_f32(Arena& a, const LocalArrays& l, 
 // block's shared accumulator of SEG + HALO particles, which is flushed once
 // per particle.  The trip counts are uniform over the block, so the warp
 // energy reductions see whole warps.
+// The mixed form is held to 48 registers (five blocks per SM): its FP64
+// fallback for near-collinear geometry would otherwise set the register count
+// (and the occupancy) of every thread; the rare fallback spills instead.
 template<int PREC, bool NF, bool NE>
-__global__ void __launch_bounds__(TPB) k_local(Arena a, LocalArrays l, int mask)
+__global__ void __launch_bounds__(TPB, PREC == P_MIXED ? 5 : 3) k_local(Arena a, LocalArrays l, int mask)
 {
     __shared__ typename WinT<PREC>::type win[3 * WINDOW];
     const int w = blockIdx.x;

@@ -71,16 +71,18 @@ template<> struct Acc<P_MIXED>
         ovf |= !(m < FX_LIMIT * FX_INV_SCALE);
         x += fx_from_double(fx); y += fx_from_double(fy); z += fx_from_double(fz);
     }
-    // the same from FP32 factors (the mixed form's plain potentials): f = c r
-    // rounded once to FP32, then to the fixed-point grid
-    __device__ __forceinline__ void add_f(float c, float dx, float dy, float dz, bool& ovf)
+    // the mixed form's plain potentials: the FP32 pair coefficient c times
+    // the FP64 displacement, each component rounded to the fixed-point grid
+    // on the FP64 pipe (one conversion per pair instead of one per component
+    // and coordinate); `bound` >= |c| |r| (|c| max(|r|^2, 1) or |c| |r|, in
+    // FP32) flags a force outside the fixed-point range
+    __device__ __forceinline__ void add_c(float c, float bound, double dx, double dy, double dz, bool& ovf)
     {
-        const float fx = c * dx, fy = c * dy, fz = c * dz;
-        const float m = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));
-        ovf |= !(m < (float)(FX_LIMIT * FX_INV_SCALE));
-        x += __float2ll_rn(fx * (float)FX_SCALE);
-        y += __float2ll_rn(fy * (float)FX_SCALE);
-        z += __float2ll_rn(fz * (float)FX_SCALE);
+        const double cd = (double)c;
+        ovf |= !(bound < (float)(FX_LIMIT * FX_INV_SCALE));
+        x += fx_from_double(cd * dx);
+        y += fx_from_double(cd * dy);
+        z += fx_from_double(cd * dz);
     }
     __device__ __forceinline__ void shfl_add(int o)
     {
@@ -110,8 +112,9 @@ struct PairEval {
     long long s;
     bool periodic;
     double crsq, coefc, eps, eps12, debye, inv_debye, abs_cut_sq, qi, inv4pi, epsi, cr;
-    float eps12f, epsf, coefcf, debf, invdf;
+    float eps12f, epsf, coefcf, debf, invdf, crsqf, wif;
     int kind, power;
+    bool fe;                    // energy-only: the force-and-energy rule of the generic loop
     const double* slot_p1;
 
     __device__ __forceinline__ PairEval(const Arena& a, const TermArrays& t, long long slot, int sys)
@@ -136,6 +139,8 @@ struct PairEval {
         epsi  = (G == G_LJ || (G == G_EXV && kind == EXV_HARD_CORE)) ? t.slot_p1[slot] : 0.0;
         eps12f = (float)eps12; epsf = (float)eps; coefcf = (float)coefc;
         debf = (float)debye; invdf = (float)inv_debye;
+        crsqf = (float)crsq; wif = (float)pi.w;
+        fe = !NF && t.fe_energy != 0;
     }
 
     // WCA, LennardJonesAttractive and UniformLennardJones through the generic
@@ -204,13 +209,13 @@ struct PairEval {
                                            double& energy, bool& ovf) const
     {
         using T = typename std::conditional<PREC == P_FP64, double, float>::type;
-        if(NF)
+        if(NF || fe)
         {
             const T rl = PREC == P_FP64 ? T(rsqrt(l2)) : T(rsqrtf((float)l2));
             const T l  = T(l2) * rl;
             const T f_mag = fam_derivative<T>(k, l, T(sigma), T(epsilon), T(cr));
             if(f_mag == T(0)) {return;}
-            acc.add((double)(f_mag * rl), dx, dy, dz, ovf);
+            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf);}
             if(count_e) {energy += (double)fam_potential<T>(k, l, T(sigma), T(epsilon), T(cr), T(coefc));}
         }
         else if(count_e)
@@ -265,13 +270,13 @@ struct PairEval {
                                                bool& ovf) const
     {
         using T = typename std::conditional<PREC == P_FP64, double, float>::type;
-        if(NF)
+        if(NF || fe)
         {
             const T rl = PREC == P_FP64 ? T(rsqrt(l2)) : T(rsqrtf((float)l2));
             const T l  = T(l2) * rl;
             const T f_mag = exv_derivative<T>(l, T(sigma), T(radius));
             if(f_mag == T(0)) {return;}
-            acc.add((double)(f_mag * rl), dx, dy, dz, ovf);
+            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf);}
             if(count_e) {energy += (double)exv_potential<T>(l, T(sigma), T(radius));}
         }
         else if(count_e)
@@ -316,12 +321,14 @@ struct PairEval {
             else
             {
                 // branch-free: every lane evaluates, pairs outside the
-                // cutoff add an exact zero
-                const float rcp = __frcp_rn((float)l2);
-                const float s2 = (float)sigma_sq * rcp;
+                // cutoff add an exact zero; sigma in FP32 from the two radii
+                const float l2f = (float)l2;
+                const float rcp = __frcp_rn(l2f);
+                const float sg = wif + (float)pj.w;
+                const float s2 = sg * sg * rcp;
                 const float s6 = s2 * s2 * s2;
                 const float cf = in ? -eps12f * s6 * s6 * rcp : 0.0f;
-                if constexpr(NF) {acc.add_f(cf, (float)dx, (float)dy, (float)dz, ovf);}
+                if constexpr(NF) {acc.add_c(cf, fabsf(cf) * fmaxf(l2f, 1.0f), dx, dy, dz, ovf);}
                 if(count_e && in) {energy += (double)(epsf * (s6 * s6 - coefcf));}
             }
         }
@@ -342,14 +349,20 @@ struct PairEval {
             {
                 // branch-free like ExcludedVolume: outside the cutoff the
                 // distance is replaced by the cutoff and the force is zero
-                const float qq = (float)((qi * pj.w) * inv4pi);
+                // the charge product stays in FP64 and scales the FP32
+                // coefficient of the unit-charge potential
+                const double qq = (qi * pj.w) * inv4pi;
                 const float l2f = in ? (float)l2 : (float)abs_cut_sq;
                 const float rl = rsqrtf(l2f);
                 const float l  = l2f * rl;
                 const float ex = __expf(-l * invdf);
-                const float cf = in ? -qq * (debf + l) * invdf * (rl * rl) * ex * rl : 0.0f;
-                if constexpr(NF) {acc.add_f(cf, (float)dx, (float)dy, (float)dz, ovf);}
-                if(count_e && in) {energy += (double)(qq * (ex * rl - coefcf));}
+                const float cu = in ? -(debf + l) * invdf * (rl * rl) * ex * rl : 0.0f;
+                if constexpr(NF)
+                {
+                    const float cf = (float)qq * cu;
+                    acc.add_c(cf, fabsf(cf) * l, dx, dy, dz, ovf);
+                }
+                if(count_e && in) {energy += qq * (double)(ex * rl - coefcf);}
             }
         }
         else   // G_LJ
@@ -374,16 +387,31 @@ struct PairEval {
             }
             else
             {
-                const float rcp = __frcp_rn((float)l2);
+                const float l2f = (float)l2;
+                const float rcp = __frcp_rn(l2f);
                 const float s2 = (float)sigma_sq * rcp;
                 const float s6 = s2 * s2 * s2;
                 const float ef = (float)epsilon;
-                if constexpr(NF) {acc.add_f(24.0f * ef * (s6 - 2.0f * s6 * s6) * rcp, (float)dx, (float)dy, (float)dz, ovf);}
+                if constexpr(NF)
+                {
+                    const float cf = 24.0f * ef * (s6 - 2.0f * s6 * s6) * rcp;
+                    acc.add_c(cf, fabsf(cf) * fmaxf(l2f, 1.0f), dx, dy, dz, ovf);
+                }
                 if(count_e) {energy += (double)(4.0f * ef * (s6 * s6 - s6 - coefcf));}
             }
         }
     }
 };
+
+// List words PF_ROWS block rows ahead of the walk are requested into L2
+// (prefetch.global.L2: no register, no wait), so that the walk's own loads of
+// those words hit L2 instead of waiting on DRAM: a long list is a chain of
+// dependent loads, and the rows a warp reads are np * TPP words apart.
+constexpr int PF_ROWS = 8;
+__device__ __forceinline__ void prefetch_l2(const void* p)
+{
+    asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+}
 
 // One slot per TPP consecutive threads.  UNR: partners requested per batch.
 // 1 keeps one partner in flight ahead of the pair being evaluated; 2 and 4
@@ -492,6 +520,8 @@ __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
             for(; k < n; k += TPP)
             {
                 const int kn = k + TPP;
+                const int kp = k + PF_ROWS * TPP;
+                if(kp < n) {prefetch_l2(nbr + (long long)(kp / TPP) * np * TPP);}
                 int qn = q;
                 double4 pn = pj;
                 if(kn < n) {qn = __ldg(nbr + (long long)(kn / TPP) * np * TPP); pn = pd[qn];}
@@ -506,6 +536,12 @@ __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
             {
                 int qv[UNR];
                 double4 pv[UNR];
+#pragma unroll
+                for(int u = 0; u < UNR; ++u)
+                {
+                    const int kp = k + (PF_ROWS + u) * TPP;
+                    if(kp < n) {prefetch_l2(nbr + (long long)(kp / TPP) * np * TPP);}
+                }
 #pragma unroll
                 for(int u = 0; u < UNR; ++u)
                 {
@@ -602,6 +638,7 @@ __global__ void __launch_bounds__(TPB, 4) k_pair_vec(Arena a, TermArrays t)
     {
         int qn[L];
         if(k + L < n) {load_block<L>(t.nbr + ((long long)(k / L + 1) * np + s) * L, qn);}
+        if(k + PF_ROWS * L < n) {prefetch_l2(t.nbr + ((long long)(k / L + PF_ROWS) * np + s) * L);}
         const int m = min(L, n - k);
 #pragma unroll
         for(int u0 = 0; u0 < L; u0 += W)
@@ -839,10 +876,13 @@ void launch_pair(const Arena& a, int g, TermArrays& t, bool need_force, bool nee
         }
         if(need_energy)
         {
+            // with the forces: the energy of calc_force_and_energy
+            TermArrays te = t;
+            te.fe_energy = need_force ? 1 : 0;
             if(need_force) {note_launches(1);}
-            if(g == G_EXV)     {dispatch<P_FP64, G_EXV>(a, t, false, true, s);}
-            else if(g == G_DH) {dispatch<P_FP64, G_DH >(a, t, false, true, s);}
-            else               {dispatch<P_FP64, G_LJ >(a, t, false, true, s);}
+            if(g == G_EXV)     {dispatch<P_FP64, G_EXV>(a, te, false, true, s);}
+            else if(g == G_DH) {dispatch<P_FP64, G_DH >(a, te, false, true, s);}
+            else               {dispatch<P_FP64, G_LJ >(a, te, false, true, s);}
         }
     }
 }

@@ -51,13 +51,21 @@ class Job:
 
     @property
     def latency(self) -> Optional[float]:
+        """Completion latency: arrival to completion (queueing included)."""
         return None if self.finished is None else self.finished - self.arrival
+
+    @property
+    def service(self) -> Optional[float]:
+        """Service latency: admission to completion (on the GPU)."""
+        return None if self.finished is None or self.admitted is None else self.finished - self.admitted
 
 
 class Server:
     """Admission control: a queued job is admitted (in arrival order) when the
-    resident particles stay within ``max_particles`` and the estimated device
-    footprint within ``hbm_fraction`` of device memory.  ``max_particles`` is
+    resident particles stay within ``max_particles`` and the device footprint
+    within ``hbm_fraction`` of device memory, the footprint counted at the
+    arena's measured bytes per particle (mjg_device_bytes after the last
+    commit).  ``max_particles`` is
     the concurrency at which the arena's throughput has saturated: admitting
     more raises no throughput, only every running job's latency.  Chunks are
     sized so one lasts about ``chunk_seconds`` (at most ``chunk`` steps), which
@@ -83,7 +91,9 @@ class Server:
         self.lookahead = int(lookahead)
         total = self._device_total(device)
         self.budget = hbm_fraction * total
-        self.bpp = bytes_per_particle           # refined after every commit
+        # device bytes per resident particle: this estimate until the first
+        # commit, then the arena's measured footprint (mjg_device_bytes)
+        self.bpp = bytes_per_particle
         self.queue = collections.deque()        # arrived, not admitted
         self.running = {}                       # sid -> Job
         self.retiring = []                      # finished sids awaiting the next commit
@@ -190,7 +200,7 @@ class Server:
         self.sec_per_step = None
         n = self._resident_particles()
         if n > 0:
-            self.bpp = max(self.bpp * 0.5, self.eng.device_bytes() / n)
+            self.bpp = self.eng.device_bytes() / n      # measured after this commit
 
     def _chunk_steps(self, live) -> int:
         k = min(self.chunk, min(j.nsteps - j.done for j in live))
@@ -244,11 +254,14 @@ class Server:
 
     def stats(self, wall: float) -> dict:
         lat = sorted(j.latency for j in self.finished)
-        q = lambda p: lat[min(len(lat) - 1, int(p * len(lat)))] if lat else None  # noqa: E731
+        svc = sorted(j.service for j in self.finished)
+        q = lambda v, p: v[min(len(v) - 1, int(p * len(v)))] if v else None  # noqa: E731
         return {"completed": len(lat), "queued": len(self.queue), "running": len(self.running),
                 "resident_particles": self._resident_particles(), "max_queue": self.max_queue,
-                "latency_p50_s": q(0.50), "latency_p90_s": q(0.90), "latency_p99_s": q(0.99),
+                "latency_p50_s": q(lat, 0.50), "latency_p90_s": q(lat, 0.90), "latency_p99_s": q(lat, 0.99),
                 "latency_mean_s": statistics.mean(lat) if lat else None,
+                "service_p50_s": q(svc, 0.50), "service_p90_s": q(svc, 0.90), "service_p99_s": q(svc, 0.99),
+                "device_bytes_per_particle": self.bpp,
                 "particle_steps_per_s": self.particle_steps / wall if wall > 0 else None,
                 "commits": self.commits, "commit_s": self.commit_s, "step_s": self.step_s,
                 "md_steps": self.steps_run}
