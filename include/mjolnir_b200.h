@@ -285,8 +285,10 @@ MJG_API int mjg_get_pair_unroll(mjg_context* ctx, int term, int* unroll);
  * threads-per-particle words with vector loads (with threads-per-particle 1
  * it is schedule 0); 3 = as 2, with the threads of each 256-particle block
  * handed its particles in order of list length; 4 = as 0, with the thread
- * groups of each block handed its particles in order of list length.  No
- * counterpart in the reference. */
+ * groups of each block handed its particles in order of list length; 5 = as
+ * 0 on lists stored particle by particle (contiguous), each particle's list
+ * requested into L2 by one bulk prefetch as its group starts (switching to or
+ * from 5 rebuilds every list of the term).  No counterpart in the reference. */
 MJG_API int mjg_set_pair_schedule(mjg_context* ctx, int term, int schedule);
 MJG_API int mjg_get_pair_schedule(mjg_context* ctx, int term, int* schedule);
 /* Lanes per particle of a global term's list build (8, 16 or 32): fewer

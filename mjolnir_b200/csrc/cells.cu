@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(TPB) k_build_list(Arena a, int g, TermArrays t
                 if(keep)
                 {
                     const int pos = count + __popc(m & ((1u << lane) - 1u));
-                    if(pos < cap) {t.nbr[nbr_index(pos, s, np, t.tpp)] = q;}
+                    if(pos < cap) {t.nbr[nbr_pos(pos, s, np, t.tpp, cap, t.slot_major)] = q;}
                 }
                 count += __popc(m);
             }
@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
             if(keep)
             {
                 const int pos = count + __popc(m & ((1u << lane) - 1u));
-                if(pos < cap) {t.nbr[nbr_index(pos, s, np, t.tpp)] = q;}
+                if(pos < cap) {t.nbr[nbr_pos(pos, s, np, t.tpp, cap, t.slot_major)] = q;}
             }
             count += __popc(m);
         }

@@ -160,6 +160,13 @@ __host__ __device__ __forceinline__ long long nbr_index(long long k, long long s
 {
     return ((k / tpp) * np + s) * tpp + (k % tpp);
 }
+// Slot-major layout (dense terms): each slot's list contiguous, `cap` words
+// per slot, so that one bulk copy engine request brings a whole list to L2.
+__host__ __device__ __forceinline__ long long nbr_pos(long long k, long long s, long long np, int tpp, int cap,
+                                                      int slot_major)
+{
+    return slot_major ? s * cap + k : nbr_index(k, s, np, tpp);
+}
 
 // Cell coordinate of x along one axis (PeriodicGridCellList::calc_index for a
 // periodic system; a wrapped hash of the unbounded grid otherwise).

@@ -1205,6 +1205,7 @@ void commit(mjg_context* c)
         t.tpp = T.tpp_fixed ? T.tpp_choice : 1;
         t.unroll = T.unroll_choice;
         t.schedule = T.schedule_choice;
+        t.slot_major = t.schedule == 5 ? 1 : 0;
         if(!T.build_lanes_fixed)
         {
             // candidates per slot if the participants filled their grids
@@ -2093,7 +2094,7 @@ int mjg_neighbors(mjg_context* c, int sys, int term, int64_t* pairs, int64_t cap
     {
         for(int k = 0; k < nnb[q]; ++k)
         {
-            const int r = all[(size_t)nbr_index(k, q, t.np, t.tpp)];
+            const int r = all[(size_t)nbr_pos(k, q, t.np, t.tpp, t.cap, t.slot_major)];
             const int64_t i = part[q] - s.off, j = part[r] - s.off;
             if(i < j) {out.emplace_back(i, j);}
         }
@@ -2250,13 +2251,23 @@ int mjg_set_pair_schedule(mjg_context* c, int term, int schedule)
 {
     ABI_BEGIN(c)
     if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "the schedule applies to global terms");}
-    if(schedule < 0 || schedule > 4) {throw Error(MJG_EINVAL, "schedule must be 0 .. 4");}
+    if(schedule < 0 || schedule > 5) {throw Error(MJG_EINVAL, "schedule must be 0 .. 5");}
     TermDev& T = c->term[term - MJG_TERM_EXV];
     T.schedule_choice = schedule;
     if(T.t.schedule != schedule)
     {
+        const int layout = schedule == 5 ? 1 : 0;
         T.t.schedule = schedule;
         release_graph(c);
+        if(T.t.on && T.t.slot_major != layout)
+        {
+            T.t.slot_major = layout;    // the list layout changes: rebuild every list
+            if(c->committed)
+            {
+                rebuild_all(c);
+                CK(cudaStreamSynchronize(c->stream));
+            }
+        }
     }
     ABI_END(c)
 }

@@ -45,9 +45,12 @@ struct TermArrays {
     int        schedule;        // force launch: 0 = slot per tpp threads, 1 = warp-balanced (mixed),
                                 // 2 = one thread per slot reading tpp-word blocks of its list,
                                 // 3 = as 2 with a block's threads ordered by list length,
-                                // 4 = as 0 with a block's thread groups ordered by list length
+                                // 4 = as 0 with a block's thread groups ordered by list length,
+                                // 5 = as 0 on the slot-major layout, each group's list brought
+                                //     to L2 by one bulk prefetch when the group starts
     int        any_periodic;    // some system with this term has a periodic box
     int        build_lanes;     // lanes per slot of the list build (8, 16 or 32)
+    int        slot_major;      // list layout: 0 blocked by tpp (nbr_index), 1 slot-major (nbr_pos)
     int        fe_energy;       // energy-only launch: sum the energy as calc_force_and_energy does
                                 // (the generic pair loop skips pairs whose force is zero,
                                 // GlobalPairInteraction.hpp:148-213) instead of calc_energy's

@@ -412,6 +412,12 @@ __device__ __forceinline__ void prefetch_l2(const void* p)
 {
     asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
 }
+// One request to the bulk copy engine for `bytes` (a multiple of 16) from p
+// (16-byte aligned) into L2; nothing waits on it.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(p), "r"(bytes) : "memory");
+}
 
 // One slot per TPP consecutive threads.  UNR: partners requested per batch.
 // 1 keeps one partner in flight ahead of the pair being evaluated; 2 and 4
@@ -504,7 +510,14 @@ __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
         const PairEval<PREC, G, NF, NE, PER> eval(a, t, s, sys);
         const long long np = t.np;
         const int n = head.n;
-        const int* __restrict__ nbr = t.nbr + s * TPP + lg;
+        // word k = lg + r TPP of the slot's list: blocked layout, rows np TPP
+        // words apart; slot-major layout, the slot's cap words in a row, the
+        // whole list requested into L2 (16-byte aligned: cap is a multiple of
+        // 16 words) before the walk starts
+        const bool sm = t.slot_major != 0;
+        const long long rs = sm ? TPP : np * TPP;
+        const int* __restrict__ nbr = t.nbr + (sm ? s * t.cap : s * TPP) + lg;
+        if(sm && lg == 0 && n > 0) {bulk_prefetch_l2(t.nbr + s * t.cap, (unsigned)((n + 3) / 4) * 16u);}
         const double4* __restrict__ pd = t.slot_pd;
         if(UNR == 1)
         {
@@ -521,10 +534,10 @@ __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
             {
                 const int kn = k + TPP;
                 const int kp = k + PF_ROWS * TPP;
-                if(kp < n) {prefetch_l2(nbr + (long long)(kp / TPP) * np * TPP);}
+                if(!sm && kp < n) {prefetch_l2(nbr + (long long)(kp / TPP) * rs);}
                 int qn = q;
                 double4 pn = pj;
-                if(kn < n) {qn = __ldg(nbr + (long long)(kn / TPP) * np * TPP); pn = pd[qn];}
+                if(kn < n) {qn = __ldg(nbr + (long long)(kn / TPP) * rs); pn = pd[qn];}
                 eval(pj, q, acc, energy, ovf);
                 q = qn;
                 pj = pn;
@@ -540,13 +553,13 @@ __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
                 for(int u = 0; u < UNR; ++u)
                 {
                     const int kp = k + (PF_ROWS + u) * TPP;
-                    if(kp < n) {prefetch_l2(nbr + (long long)(kp / TPP) * np * TPP);}
+                    if(!sm && kp < n) {prefetch_l2(nbr + (long long)(kp / TPP) * rs);}
                 }
 #pragma unroll
                 for(int u = 0; u < UNR; ++u)
                 {
                     const int kk = k + u * TPP;
-                    qv[u] = kk < n ? __ldg(nbr + (long long)(kk / TPP) * np * TPP) : -1;
+                    qv[u] = kk < n ? __ldg(nbr + (long long)(kk / TPP) * rs) : -1;
                 }
 #pragma unroll
                 for(int u = 0; u < UNR; ++u) {pv[u] = qv[u] >= 0 ? pd[qv[u]] : eval.pi;}
@@ -604,6 +617,7 @@ __device__ __forceinline__ void load_block(const int* __restrict__ p, int (&q)[L
     }
 }
 
+// Schedules 2 and 3 (blocked list layout only).
 // SORT: the block's threads take its 256 slots in order of their number of
 // list blocks (a counting sort in shared memory), so that the lanes of a warp
 // walk lists of about the same length; the slots themselves, and with them
@@ -656,7 +670,8 @@ __global__ void __launch_bounds__(TPB, 4) k_pair_vec(Arena a, TermArrays t)
     if(ovf) {atomicOr(&a.sys[sys].status, ST_FIXED_OVERFLOW);}
 }
 
-// Warp-balanced schedule of the mixed form's force launch: a warp owns 32
+// Warp-balanced schedule of the mixed form's force launch (schedule 1,
+// blocked list layout only): a warp owns 32
 // consecutive slots and splits the concatenation of their lists into 32 equal
 // contiguous chunks, one per lane, so every lane evaluates the same number of
 // pairs whatever the list lengths (one slot per thread leaves the lanes of
@@ -756,7 +771,7 @@ __global__ void k_count_cut(Arena a, TermArrays t, int sys_filter, unsigned long
         const int n = t.nnb[s];
         for(int k = 0; k < n; ++k)
         {
-            const int q = t.nbr[nbr_index(k, s, t.np, t.tpp)];
+            const int q = t.nbr[nbr_pos(k, s, t.np, t.tpp, t.cap, t.slot_major)];
             if(q <= s) {continue;}
             const double4 pj = t.slot_pd[q];
             double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;

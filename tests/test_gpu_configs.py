@@ -120,3 +120,26 @@ def test_config_velocity_verlet_1000_steps(name):
                 L = np.array(d.upper) - np.array(d.lower)
                 dp -= L * np.round(dp / L)
             assert np.abs(dp).max() <= VV_POS_TOL[name], (name, np.abs(dp).max())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_config_slot_major_lists(precision):
+    """The slot-major list layout (schedule 5) on the fluid cut: the same
+    lists bit for bit, the reference's forces within the form's tolerance,
+    and in the mixed form the same forces as the default layout bit for bit."""
+    d, _dt, _sub, fx = CASES["config3_fluid32768"]
+    e = Engine(precision)
+    sid = e.add_system(d)
+    e.commit()
+    base = {t: e.term_force(sid, t)[0] for t in ("exv", "dh")}
+    for t in ("exv", "dh"):
+        e.set_pair_schedule(t, 5)
+        e.set_threads_per_particle(t, 8)
+    for t in ("exv", "dh"):
+        pairs = e.neighbors(sid, t)
+        assert sha256(pairs.astype(np.int64)) == str(fx[f"pairs_sha_{t}"]), t
+        f, _ = e.term_force(sid, t)
+        assert rel_rms(f, fx[f"force_{t}"]) <= FORCE_TOL[precision], (precision, t)
+        if precision == "mixed":
+            assert np.array_equal(f, base[t]), t
+    e.close()

@@ -239,6 +239,7 @@ def test_launch_shapes_give_the_same_trajectory(precision):
     shapes = [(0, tpp, unr) for tpp in (1, 2, 4, 8, 16) for unr in (1, 2, 4)]
     shapes += [(sch, tpp, 1) for sch in (2, 3) for tpp in (2, 4, 8, 16)]
     shapes += [(4, tpp, unr) for tpp in (1, 4, 16) for unr in (1, 2)]
+    shapes += [(5, tpp, unr) for tpp in (1, 8, 16) for unr in (1, 2, 4)]      # slot-major lists
     if precision == "mixed":
         shapes += [(1, tpp, unr) for tpp in (1, 16) for unr in (1, 2, 4)]
     for sch, tpp, unr in shapes:
