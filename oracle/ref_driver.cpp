@@ -83,6 +83,9 @@ void set_units_once()
 
     using phys_type = physics::constants<double>;
     using unit_type = unit::constants<double>;
+    // the constants are process-wide (template statics are shared by every
+    // library that includes the reference headers): convert them only once
+    if(phys_type::energy_unit() == "kcal/mol") {return;}
     phys_type::set_kB(phys_type::kB() * (unit_type::J_to_cal() / 1000.0) *
                       unit_type::avogadro_constant());
     phys_type::set_eps0(phys_type::eps0() * (1000.0 / unit_type::J_to_cal()) /
