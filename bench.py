@@ -154,7 +154,7 @@ def ncu_traffic(key, schedule, slots):
         return None, f"the recorded capture is of schedule {rec.get('schedule')}, this launch runs {schedule}"
     b = (rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["slots"] * slots
     return b, (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch ({rec['kernel']}, "
-               f"{rec['slots']} slots, commit {rec.get('commit', '?')}), scaled by slots; profiles/ncu_traffic.json")
+               f"{rec['slots']} slots, {rec['workload']}), scaled by slots; profiles/ncu_traffic.json")
 
 
 def measured_peaks():
@@ -322,6 +322,9 @@ def fluid_pair_roofline(local, peak, steps=200):
         b.synchronize()
         step_ms = a.elapsed_time(b) / steps
         k = pair_kernels(e, [d], 0, prec, label="fluid")
+        for term, v in k.items():
+            v["traffic"], v["traffic_source"] = ncu_traffic(f"fluid1m_{term}" if prec == "mixed" else "",
+                                                            e.get_pair_schedule(term), v["slots"])
         tot_b = sum(v["bytes"] for v in k.values())
         tot_ms = sum(v["ms"] for v in k.values())
         out[prec] = {"terms": k, "tuned": tuned, "gbs": tot_b / (tot_ms * 1e-3) / 1e9,
