@@ -229,6 +229,47 @@ __global__ void __launch_bounds__(TPB) k_slots_setup(Arena a, TermArrays t)
     }
 }
 
+// A slot's exclusion row staged in shared memory once per slot: the CSR row of
+// particle i holds every particle excluded together with i (the relation is
+// symmetric: topology distance and molecule rules; i itself included), so
+// is_excluded(min(i, j), max(i, j)) is "j is in i's row" -- a comparison
+// against the staged row instead of a chain of dependent loads per candidate.
+// Rows longer than EXMAX are scanned in global memory as before.
+constexpr int EXMAX = 16;
+struct ExRow {
+    int n;              // entries staged, or -1: the row is longer than EXMAX
+    int mol;            // molecule of particle i
+    int v[EXMAX];       // sorted excluded partners of i
+};
+// lanes [0, nl) of the slot's group stage particle i's row (every lane of the
+// group must call it, then synchronise the group before reading the row)
+__device__ __forceinline__ void stage_ex_row(const Arena& a, int g, int i, int gl, int nl, ExRow& r)
+{
+    const long long b = a.ex_start[g][i], e = a.ex_start[g][i + 1];
+    const int n = (int)(e - b);
+    if(gl == 0) {r.n = n <= EXMAX ? n : -1; r.mol = a.mol[i];}
+    if(n <= EXMAX) {for(int k = gl; k < n; k += nl) {r.v[k] = a.ex_idx[g][b + k];}}
+}
+__device__ __forceinline__ bool is_excluded(const Arena& a, int g, int ignore_mol, int i, int j);
+// is_excluded(min(i, j), max(i, j)) for the slot's particle i and candidate j
+__device__ __forceinline__ bool excluded_staged(const Arena& a, int g, int ignore_mol, const ExRow& r, int i, int j)
+{
+    if(ignore_mol != IGN_NOTHING)
+    {
+        const int mj = a.mol[j];
+        if(ignore_mol == IGN_SELF   && r.mol == mj) {return true;}
+        if(ignore_mol == IGN_OTHERS && r.mol != mj) {return true;}
+    }
+    if(r.n < 0) {return is_excluded(a, g, IGN_NOTHING, i < j ? i : j, i < j ? j : i);}
+    for(int k = 0; k < r.n; ++k)
+    {
+        const int x = r.v[k];
+        if(x > j) {break;}
+        if(x == j) {return true;}
+    }
+    return false;
+}
+
 __device__ __forceinline__ bool is_excluded(const Arena& a, int g, int ignore_mol, int i, int j)
 {
     if(ignore_mol == IGN_SELF   && a.mol[i] == a.mol[j]) {return true;}
@@ -258,6 +299,8 @@ __global__ void __launch_bounds__(TPB) k_build_list(Arena a, int g, TermArrays t
     const unsigned full = 0xffffffffu;
     // every warp of the grid takes the next (chunk, slot) pair, so that all
     // warps have work even when only a few systems rebuild
+    __shared__ ExRow ex_rows[TPB / 32];
+    ExRow& exr = ex_rows[threadIdx.x >> 5];
     const long long nwork = (long long)n * CHUNK;
     const long long wstride = (long long)gridDim.x * (TPB / 32);
     for(long long gw = (long long)blockIdx.x * (TPB / 32) + (threadIdx.x >> 5); gw < nwork; gw += wstride)
@@ -276,6 +319,9 @@ __global__ void __launch_bounds__(TPB) k_build_list(Arena a, int g, TermArrays t
             const int i = t.slot_particle[s];
             const bool lead_i = t.slot_lead[s] != 0;
             const double4 ri = t.slot_pd[s];
+            __syncwarp();                        // the previous slot's row is no longer read
+            stage_ex_row(a, g, i, lane, 32, exr);
+            __syncwarp();
             const int cx = cell_coord(ri.x, G, 0);
             const int cy = cell_coord(ri.y, G, 1);
             const int cz = cell_coord(ri.z, G, 2);
@@ -340,7 +386,7 @@ __global__ void __launch_bounds__(TPB) k_build_list(Arena a, int g, TermArrays t
                     {
                         const int j = t.slot_particle[q];
                         const bool lead_lo = (i < j) ? lead_i : (t.slot_lead[q] != 0);
-                        keep = lead_lo && !is_excluded(a, g, G.ignore_mol, i < j ? i : j, i < j ? j : i);
+                        keep = lead_lo && !excluded_staged(a, g, G.ignore_mol, exr, i, j);
                     }
                 }
                 const unsigned m = __ballot_sync(full, keep);
@@ -376,6 +422,7 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
     constexpr int CPL = (27 + LPS - 1) / LPS;      // stencil cells per lane
     __shared__ int c_start[GROUPS][27];
     __shared__ int c_excl[GROUPS][28];             // exclusive prefix; [27] = total
+    __shared__ ExRow ex_rows[GROUPS];
     const int n = t.work[0];
     const int cap = t.cap;
     const long long np = t.np;
@@ -412,6 +459,7 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
             i = t.slot_particle[s];
             lead_i = t.slot_lead[s] != 0;
             ri = t.slot_pd[s];
+            stage_ex_row(a, g, i, gl, LPS, ex_rows[grp]);
             const int cx = cell_coord(ri.x, G, 0);
             const int cy = cell_coord(ri.y, G, 1);
             const int cz = cell_coord(ri.z, G, 2);
@@ -504,7 +552,7 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
                     {
                         const int j = t.slot_particle[q];
                         const bool lead_lo = (i < j) ? lead_i : (t.slot_lead[q] != 0);
-                        keep = lead_lo && !is_excluded(a, g, G.ignore_mol, i < j ? i : j, i < j ? j : i);
+                        keep = lead_lo && !excluded_staged(a, g, G.ignore_mol, ex_rows[grp], i, j);
                     }
                 }
             }
