@@ -55,6 +55,8 @@ def parse():
                     help="skip the pair-kernel roofline on the 1,048,576-bead periodic fluid")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the 2,000-step precision report on the 1,048,576-bead fluid")
+    ap.add_argument("--no-fluid-reference", action="store_true",
+                    help="skip timing the reference's OpenMP path on the 1,048,576-bead fluid (about a minute)")
     return ap.parse_args()
 
 
@@ -235,6 +237,33 @@ def cpu_reference_rate(descs, budget_s=12.0):
     sample = (f"all {len(descs)} systems ({rb.n} beads), {steps} MD steps each, one system after another "
               f"through OpenMPSimulatorTraits BAOAB ({rb.threads} threads)")
     return rb.n * steps / t, sample, rb.threads
+
+
+def fluid_reference(steps=20, margins=(0.2, 0.2)):
+    """The reference's OpenMP path on the 1,048,576-bead fluid (the
+    precision-at-scale configuration, at the precision report's margins), a
+    bounded sample: building the reference's objects (which makes its
+    exclusion and cell lists once) is timed apart, then `steps` MD steps,
+    which include the list rebuilds its margin logic triggers."""
+    import time
+    import oracle
+    from mjolnir_b200 import systems as S
+    if not oracle.reference_available():
+        return None
+    omp = omp_setup()
+    d = S.bead_fluid(n=1 << 20, density=0.003, seed=3, synth=oracle.synthetic_library())
+    d.exv.margin, d.dh.margin = margins
+    t0 = time.perf_counter()
+    r = oracle.Reference(d, parallel=True)
+    r.initialize()
+    t_build = time.perf_counter() - t0
+    t_steps = r.run(steps)
+    r.close()
+    return {"value": d.n * steps / t_steps, "unit": "particle-steps/s", "kind": "reference",
+            "cores": oracle.Reference.max_threads(), **omp, "beads": d.n, "steps_timed": steps,
+            "s_per_step": t_steps / steps, "setup_s": t_build,
+            "sample": f"{steps} MD steps of the 1,048,576-bead fluid (margins {margins[0]} / {margins[1]}) "
+                      "through OpenMPSimulatorTraits BAOAB, list rebuilds included; setup timed apart"}
 
 
 def run_reference_arm(args, ws, rank, pg):
@@ -552,6 +581,13 @@ def run_b200(args, ws, rank, local, pg):
         prec["bound"] = 1e-5
         prec["note"] = ("forces: mixed form vs the FP64 form on the mixed trajectory's coordinates every "
                         "1,000 steps; energies are evaluated in FP64 in both forms")
+
+    # ---- the reference's OpenMP path on the 1 M fluid, a bounded sample
+    if not args.no_fluid_reference and not args.no_cpu_baseline and rank == 0 and ws == 1:
+        fref = fluid_reference()
+        if fluid is not None and fref is not None:
+            fluid["reference_cpu"] = fref
+            fluid["mixed_over_reference"] = fluid["mixed"]["particle_steps_per_s"] / fref["value"]
 
     # ---- serving: Poisson arrivals at 200 jobs/s, continuous batching
     serving = None
