@@ -86,7 +86,9 @@ MJG_API int mjg_system_create(mjg_context* ctx, int64_t n, int boundary,
                       const double* pos, const double* vel, const double* mass,
                       int* sys_id);
 /* system.attributes temperature [K] and ionic_strength [mol/L]
- * (core/System.hpp:151-156). */
+ * (core/System.hpp:151-156).  Temperature 0 runs without thermal noise (a
+ * system with DebyeHuckel needs a positive temperature for its Debye length,
+ * checked at mjg_commit); the ionic strength must be positive. */
 MJG_API int mjg_system_set_attributes(mjg_context* ctx, int sys, double temperature,
                               double ionic_strength);
 /* Topology::add_connection for m pairs of the connection kind `kind`

@@ -521,6 +521,8 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
 #pragma unroll
         for(int o = LPS; o < 32; o <<= 1) {tmax = max(tmax, __shfl_xor_sync(full, tmax, o));}
         int count = 0;
+        int lo = 0;         // the last stencil cell whose range starts at or before k: k only grows, so
+                            // the lane walks forward from its previous cell
         for(int b = 0; b < tmax; b += LPS)
         {
             const int k = b + gl;
@@ -528,12 +530,7 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
             int q = 0;
             if(k < total)
             {
-                int lo = 0, hi = 26;                   // the last cell whose range starts at or before k
-                while(lo < hi)
-                {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if(c_excl[grp][mid] <= k) {lo = mid;} else {hi = mid - 1;}
-                }
+                while(lo < 26 && c_excl[grp][lo + 1] <= k) {++lo;}
                 q = c_start[grp][lo] + (k - c_excl[grp][lo]);
                 if(q != s)
                 {

@@ -781,6 +781,7 @@ void make_sysdev(const HostSystem& s, SysDev& d)
         }
         else if(g == G_DH)         // DebyeHuckelPotential.hpp:126-167,245-248
         {
+            if(!(s.T > 0)) {throw Error(MJG_EINVAL, "DebyeHuckel needs a positive temperature (its Debye length)");}
             const DHParams p = dh_params(s.T, s.I, H.cutoff_ratio);
             G.debye = p.debye; G.inv_debye = p.inv_debye; G.abs_cutoff = p.abs_cutoff;
             G.coef_at_cutoff = p.coef_at_cutoff; G.inv4pi = p.inv4pi;
@@ -1588,7 +1589,7 @@ int mjg_system_set_temperature(mjg_context* c, int sys, double T)
 {
     ABI_BEGIN(c)
     HostSystem& s = get_sys(c, sys);
-    if(!(T > 0)) {throw Error(MJG_EINVAL, "temperature must be positive");}
+    if(!(T >= 0)) {throw Error(MJG_EINVAL, "temperature must not be negative");}
     s.T = T;
     if(!c->committed || !s.resident || s.integrator == I_VV) {return MJG_OK;}
     // BAOABLangevinIntegrator::update -> reset_parameters (:47-58, :73-99),
@@ -1631,7 +1632,10 @@ int mjg_system_set_attributes(mjg_context* c, int sys, double T, double I)
     ABI_BEGIN(c)
     HostSystem& s = get_sys(c, sys);
     if(s.resident) {throw Error(MJG_ESTATE, "attributes are fixed once committed");}
-    if(!(T > 0) || !(I > 0)) {throw Error(MJG_EINVAL, "temperature and ionic strength must be positive");}
+    // temperature 0 is a run without thermal noise, as in the reference's
+    // input; DebyeHuckel needs a positive one for its Debye length (checked
+    // at commit)
+    if(!(T >= 0) || !(I > 0)) {throw Error(MJG_EINVAL, "temperature must not be negative, ionic strength must be positive");}
     s.T = T; s.I = I;
     ABI_END(c)
 }
