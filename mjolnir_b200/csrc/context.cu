@@ -408,14 +408,16 @@ void upload_sys(mjg_context* c)
 // tiles the blocked layout
 int list_capacity(int max_count) {return ((max_count + max_count / 4 + 16) + 15) / 16 * 16;}
 
-// threads per slot of the pair kernel from the longest list (refined by the
-// autotuner through mjg_set_threads_per_particle)
-int default_tpp(int max_count)
+// threads per slot of the pair kernel from the longest list, widened for
+// arenas with few slots until the launch fills the GPU (about 148 SMs x 1,024
+// threads; a small system otherwise leaves most SMs idle and each thread
+// walks a long chain of dependent loads); refined by the autotuner through
+// mjg_set_threads_per_particle
+int default_tpp(int max_count, long long slots)
 {
-    if(max_count >= 192) {return 8;}
-    if(max_count >= 48)  {return 4;}
-    if(max_count >= 12)  {return 2;}
-    return 1;
+    int tpp = max_count >= 192 ? 8 : (max_count >= 48 ? 4 : (max_count >= 12 ? 2 : 1));
+    while(tpp < 16 && tpp < max_count && slots * tpp < 148LL * 1024) {tpp *= 2;}
+    return tpp;
 }
 
 // words per slot the neighbour buffer holds for capacity cap: at least 16
@@ -449,7 +451,7 @@ void rebuild_all(mjg_context* c)
             CK(cudaMemcpyAsync(&mx, T.t.max_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
             if(mx <= T.t.cap) {break;}
-            if(!T.tpp_fixed) {T.t.tpp = default_tpp(mx);}
+            if(!T.tpp_fixed) {T.t.tpp = default_tpp(mx, T.t.np);}
             alloc_lists(c, g, list_capacity(mx));
         }
     }

@@ -2,6 +2,7 @@
 
     python -m mjolnir_b200.probe batch            # the 256-system polymer batch, mixed form
     python -m mjolnir_b200.probe fluid [--precision fp64] [--n 1048576]
+    python -m mjolnir_b200.probe lj [--precision fp64]   # the 4,096-particle Lennard-Jones fluid
 
 `batch` builds the benchmark's 256 independent polymer melts with the launch
 shapes the autotuner picks for them (ExcludedVolume: margin 0.3, block-vector
@@ -97,13 +98,28 @@ def fluid(precision: str = "mixed", n: int = 1 << 20, device: int = 0) -> dict:
     return out
 
 
+def lj(precision: str = "mixed", device: int = 0) -> dict:
+    d = S.lj_fluid(n=4096, density=0.8, margin=0.2, seed=1)
+    e = Engine(precision, device=device)
+    e.add_system(d)
+    e.commit()
+    e.step(200)
+    out = {"workload": f"4,096-particle Lennard-Jones fluid, {precision} form", "particles": d.n}
+    out["ms_per_md_step"] = _steps_ms(e, 2000)
+    out["rebuilds"] = e.rebuild_count(0, "lj")
+    _ranges(e, out, ("lj",))
+    e.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(prog="python -m mjolnir_b200.probe")
-    ap.add_argument("workload", choices=["batch", "fluid"])
+    ap.add_argument("workload", choices=["batch", "fluid", "lj"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--n", type=int, default=1 << 20)
     a = ap.parse_args()
-    res = batch() if a.workload == "batch" else fluid(a.precision, a.n)
+    res = batch() if a.workload == "batch" else (fluid(a.precision, a.n) if a.workload == "fluid"
+                                                 else lj(a.precision))
     print(json.dumps(res))
 
 
