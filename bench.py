@@ -142,10 +142,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def ncu_traffic(key, schedule, slots):
+def ncu_traffic(key, schedule, slots, half=False):
     """(DRAM bytes of one launch, source text) from profiles/ncu_traffic.json
-    for the kernel `key` captured with the same schedule, scaled by slots;
-    (None, reason) when no capture of that kernel and schedule is recorded."""
+    for the kernel `key` captured with the same schedule and list form, scaled
+    by slots; (None, reason) when no capture of that kernel, schedule and list
+    form is recorded."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
@@ -154,6 +155,10 @@ def ncu_traffic(key, schedule, slots):
         return None, "no ncu capture recorded for this kernel"
     if rec.get("schedule") != schedule:
         return None, f"the recorded capture is of schedule {rec.get('schedule')}, this launch runs {schedule}"
+    if bool(rec.get("half_lists", False)) != bool(half):
+        form = lambda h: "half" if h else "full"
+        return None, (f"the recorded capture walks {form(rec.get('half_lists', False))} lists, "
+                      f"this launch {form(half)} lists")
     b = (rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["slots"] * slots
     return b, (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch ({rec['kernel']}, "
                f"{rec['slots']} slots, {rec['workload']}), scaled by slots; profiles/ncu_traffic.json")
@@ -372,7 +377,8 @@ def fluid_pair_roofline(local, peak, steps=200):
         k = pair_kernels(e, [d], 0, prec, label="fluid")
         for term, v in k.items():
             v["traffic"], v["traffic_source"] = ncu_traffic(f"fluid1m_{term}" if prec == "mixed" else "",
-                                                            e.get_pair_schedule(term), v["slots"])
+                                                            e.get_pair_schedule(term), v["slots"],
+                                                            prec == "mixed" and e.get_half_lists(term))
         tot_b = sum(v["bytes"] for v in k.values())
         tot_ms = sum(v["ms"] for v in k.values())
         out[prec] = {"terms": k, "tuned": tuned, "gbs": tot_b / (tot_ms * 1e-3) / 1e9,
@@ -536,11 +542,13 @@ def run_b200(args, ws, rank, local, pg):
     # DRAM bytes (read + write) of one launch of this kernel as ncu measured
     # them (profiles/ncu_traffic.json: per kernel and workload, the capture's
     # bytes and slots), scaled to this launch by its slots
-    traffic, traffic_src = ncu_traffic(f"batch256_{dom}", eng.get_pair_schedule(dom), k["slots"])
+    traffic, traffic_src = ncu_traffic(f"batch256_{dom}", eng.get_pair_schedule(dom), k["slots"],
+                                       eng.get_half_lists(dom))
     local_ms = {t: eng.time_kernel(t, reps=20) for t in ("bond", "angle", "dihedral")}
     shape = eng.get_pair_schedule(dom), eng.get_threads_per_particle(dom), eng.get_pair_unroll(dom)
     roofline = {"bound": "hbm", "kernel": f"pair force kernel of {dom} (schedule {shape[0]}, "
-                f"{shape[1]} threads or words per slot, {shape[2]} partners per batch)",
+                f"{shape[1]} threads or words per slot, {shape[2]} partners per batch, "
+                f"{'half' if eng.get_half_lists(dom) else 'full'} lists)",
                 "achieved": k["gbs"], "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": k["gbs"] / peak, "traffic": traffic,
                 "traffic_source": traffic_src,

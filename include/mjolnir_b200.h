@@ -293,6 +293,18 @@ MJG_API int mjg_get_pair_unroll(mjg_context* ctx, int term, int* unroll);
  * from 5 rebuilds every list of the term).  No counterpart in the reference. */
 MJG_API int mjg_set_pair_schedule(mjg_context* ctx, int term, int schedule);
 MJG_API int mjg_get_pair_schedule(mjg_context* ctx, int term, int* schedule);
+/* Half Verlet lists for a global term (mixed form only; MJG_EINVAL in the
+ * FP64 form): a pair is stored in the list of its lower slot alone, and the
+ * force launch adds the pair's negated fixed-point force to the partner with
+ * integer atomics -- the same integer sums as the full lists, so forces and
+ * trajectories are identical bit for bit, with half the list words and pair
+ * evaluations for the atomics of the partners' shares.  Switching rebuilds
+ * every list of the term.  mjg_neighbors reports the same pairs either way.
+ * The reference's own lists are half lists (core/NeighborList.hpp:151-266,
+ * pairs j > i); its force loop adds f to i and subtracts it from j
+ * (GlobalPairInteraction.hpp:148-213). */
+MJG_API int mjg_set_half_lists(mjg_context* ctx, int term, int on);
+MJG_API int mjg_get_half_lists(mjg_context* ctx, int term, int* on);
 /* Lanes per particle of a global term's list build (8, 16 or 32): fewer
  * lanes build several lists per warp at once, which pays when a particle has
  * few candidates in its 27 neighbouring cells.  Unless set here, each commit

@@ -78,6 +78,8 @@ SIGNATURES = {
     "mjg_get_pair_unroll": (C.c_int, [_ctx, C.c_int, C.POINTER(C.c_int)]),
     "mjg_set_pair_schedule": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "mjg_get_pair_schedule": (C.c_int, [_ctx, C.c_int, C.POINTER(C.c_int)]),
+    "mjg_set_half_lists": (C.c_int, [_ctx, C.c_int, C.c_int]),
+    "mjg_get_half_lists": (C.c_int, [_ctx, C.c_int, C.POINTER(C.c_int)]),
     "mjg_set_build_lanes": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "mjg_get_build_lanes": (C.c_int, [_ctx, C.c_int, C.POINTER(C.c_int)]),
     "mjg_set_margin": (C.c_int, [_ctx, C.c_int, C.c_double]),

@@ -10,8 +10,8 @@ For every global term of an :class:`~mjolnir_b200.engine.Engine` it picks
     its list in blocks with vector loads; the first and last optionally with
     each block's threads ordered by list length; or the first on lists stored
     slot by slot, each brought to L2 by one bulk prefetch), the threads per
-    particle / list block (1, 2, 4, 8, 16) and the partners each thread
-    requests per batch (1, 2, 4);
+    particle / list block (1, 2, 4, 8, 16), the partners each thread
+    requests per batch (1, 2, 4) and, in the mixed form, full or half lists;
   * the lanes per particle of the list build (8, 16, 32), by timing whole
     steps at the chosen margin and shape.
 In the mixed form none of the choices changes a result: the fixed-point force
@@ -55,8 +55,8 @@ def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
             eng.step(warm)
             ms = _time_steps(eng, steps)
             if log:
-                log(f"autotune {t}: margin {m} schedule {shape[0]} tpp {shape[1]} unroll {shape[2]}: "
-                    f"{ms:.4f} ms/step")
+                log(f"autotune {t}: margin {m} schedule {shape[0]} tpp {shape[1]} unroll {shape[2]} "
+                    f"half lists {shape[3]}: {ms:.4f} ms/step")
             if best is None or ms < best[0]:
                 best = (ms, m, shape)
         eng.set_margin(t, best[1])
@@ -73,12 +73,14 @@ def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
                 lanes_best = (ms, lanes)
         eng.set_build_lanes(t, lanes_best[1])
         choice[t] = {"margin": best[1], "schedule": best[2][0], "threads_per_particle": best[2][1],
-                     "unroll": best[2][2], "build_lanes": lanes_best[1],
+                     "unroll": best[2][2], "half_lists": best[2][3], "build_lanes": lanes_best[1],
                      "ms_per_step": min(best[0], lanes_best[0])}
     return choice
 
 
 def _apply(eng, term, shape):
+    if eng.precision == "mixed":
+        eng.set_half_lists(term, shape[3])
     eng.set_pair_schedule(term, shape[0])
     eng.set_threads_per_particle(term, shape[1])
     eng.set_pair_unroll(term, shape[2])
@@ -86,19 +88,25 @@ def _apply(eng, term, shape):
 
 def _tune_shape(eng, term, tpps, unrolls, schedules):
     best = None
-    for sch in schedules:
-        eng.set_pair_schedule(term, sch)
-        for p in tpps:
-            if sch in (2, 3) and p == 1:
-                continue                  # the same launch as schedule 0
-            if sch == 5 and p < 8:
-                continue                  # slot-major lists want whole 32-byte sectors per group
-            eng.set_threads_per_particle(term, p)
-            for u in (unrolls if sch not in (2, 3) else (1,)):
-                eng.set_pair_unroll(term, u)
-                ms = eng.time_kernel(term, reps=10)
-                if best is None or ms < best[0]:
-                    best = (ms, (sch, p, u))
+    # half lists (mixed form): half the list words and pair evaluations, plus
+    # integer atomics for the partners' shares -- a gain where few listed
+    # pairs are inside the cutoff, a loss where most are
+    for half in ((False, True) if eng.precision == "mixed" else (False,)):
+        if eng.precision == "mixed":
+            eng.set_half_lists(term, half)
+        for sch in schedules:
+            eng.set_pair_schedule(term, sch)
+            for p in tpps:
+                if sch in (2, 3) and p == 1:
+                    continue                  # the same launch as schedule 0
+                if sch == 5 and p < 8:
+                    continue                  # slot-major lists want whole 32-byte sectors per group
+                eng.set_threads_per_particle(term, p)
+                for u in (unrolls if sch not in (2, 3) else (1,)):
+                    eng.set_pair_unroll(term, u)
+                    ms = eng.time_kernel(term, reps=10)
+                    if best is None or ms < best[0]:
+                        best = (ms, (sch, p, u, half))
     return best[1]
 
 
@@ -115,5 +123,6 @@ def tune_shapes(eng, terms=("exv", "dh", "lj"), tpps=(1, 2, 4, 8, 16), unrolls=(
         shape = _tune_shape(eng, t, tpps, unrolls,
                             tuple(x for x in schedules if eng.precision == "mixed" or x != 1))
         _apply(eng, t, shape)
-        out[t] = {"schedule": shape[0], "threads_per_particle": shape[1], "unroll": shape[2]}
+        out[t] = {"schedule": shape[0], "threads_per_particle": shape[1], "unroll": shape[2],
+                  "half_lists": shape[3]}
     return out

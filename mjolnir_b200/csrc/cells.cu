@@ -284,6 +284,19 @@ __device__ __forceinline__ bool is_excluded(const Arena& a, int g, int ignore_mo
     return false;
 }
 
+// Half lists keep a pair in the list of its lower slot only: a stencil cell's
+// slot range [start, start + count) is cut to the slots above s (slots are in
+// cell order, so a cell is one range), which leaves the full list's words
+// above s in their order.  The full lists are symmetric (the distance test,
+// the leading-participant rule and the exclusions do not depend on which
+// partner asks), so every pair of them is in exactly one half list.
+__device__ __forceinline__ void clip_half(int& start, int& count, int s)
+{
+    const int lo = max(start, s + 1);
+    count = max(0, start + count - lo);
+    start = lo;
+}
+
 // One warp per slot.  The 27 stencil cells (in the reference's order: z, y, x
 // from -1 to +1) are flattened into one candidate sequence that the 32 lanes
 // walk together; the distance test reads the cell-ordered slot coordinates
@@ -343,6 +356,7 @@ __global__ void __launch_bounds__(TPB) k_build_list(Arena a, int g, TermArrays t
                     const int cell = G.cell_off + x + dx_ * (y + dy_ * z);
                     cstart = t.cell_start[cell];
                     ccount = t.cell_count[cell];
+                    if(t.half) {clip_half(cstart, ccount, s);}
                 }
             }
             int incl = ccount;
@@ -480,6 +494,7 @@ __global__ void __launch_bounds__(TPB) k_build_list_sub(Arena a, int g, TermArra
                     const int cell = G.cell_off + x + dx_ * (y + dy_ * z);
                     cs = t.cell_start[cell];
                     cc = t.cell_count[cell];
+                    if(t.half) {clip_half(cs, cc, s);}
                 }
                 c_start[grp][k] = cs;
                 c_excl[grp][k] = cc;

@@ -142,7 +142,8 @@ struct TermDev {
     int unroll_choice = 1;       // partner batch depth of the force launch
     int schedule_choice = 0;     // force launch schedule (0 slot per threads, 1 warp-balanced,
                                  // 2 block-vector, 3 block-vector with length-sorted threads,
-                                 // 4 slot per threads with length-sorted groups)
+                                 // 4 slot per threads with length-sorted groups, 5 slot-major lists)
+    bool half_choice = false;    // half lists (mixed form only)
     int build_lanes_choice = 32; // lanes per slot of the list build (8, 16, 32)
     bool build_lanes_fixed = false;  // ... chosen by the caller (else from the expected candidates)
     TermArrays t{};
@@ -1209,6 +1210,7 @@ void commit(mjg_context* c)
         t.unroll = T.unroll_choice;
         t.schedule = T.schedule_choice;
         t.slot_major = t.schedule == 5 ? 1 : 0;
+        t.half = T.half_choice && c->precision == P_MIXED ? 1 : 0;
         if(!T.build_lanes_fixed)
         {
             // candidates per slot if the participants filled their grids
@@ -2102,7 +2104,8 @@ int mjg_neighbors(mjg_context* c, int sys, int term, int64_t* pairs, int64_t cap
         {
             const int r = all[(size_t)nbr_pos(k, q, t.np, t.tpp, t.cap, t.slot_major)];
             const int64_t i = part[q] - s.off, j = part[r] - s.off;
-            if(i < j) {out.emplace_back(i, j);}
+            if(t.half) {out.emplace_back(std::min(i, j), std::max(i, j));}   // each pair listed once
+            else if(i < j) {out.emplace_back(i, j);}
         }
     }
     std::sort(out.begin(), out.end());
@@ -2275,6 +2278,35 @@ int mjg_set_pair_schedule(mjg_context* c, int term, int schedule)
             }
         }
     }
+    ABI_END(c)
+}
+
+int mjg_set_half_lists(mjg_context* c, int term, int on)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "half lists apply to global terms");}
+    if(on && c->precision != P_MIXED) {throw Error(MJG_EINVAL, "half lists need the mixed form's integer force sums");}
+    TermDev& T = c->term[term - MJG_TERM_EXV];
+    T.half_choice = on != 0;
+    const int half = T.half_choice ? 1 : 0;
+    if(T.t.half != half)
+    {
+        T.t.half = half;
+        release_graph(c);
+        if(T.t.on && c->committed)
+        {
+            rebuild_all(c);             // another list form: rebuild every list
+            CK(cudaStreamSynchronize(c->stream));
+        }
+    }
+    ABI_END(c)
+}
+
+int mjg_get_half_lists(mjg_context* c, int term, int* on)
+{
+    ABI_BEGIN(c)
+    if(term < MJG_TERM_EXV || term > MJG_TERM_LJ || !on) {throw Error(MJG_EINVAL, "bad query");}
+    *on = c->term[term - MJG_TERM_EXV].half_choice ? 1 : 0;
     ABI_END(c)
 }
 

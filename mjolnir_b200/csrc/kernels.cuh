@@ -51,6 +51,9 @@ struct TermArrays {
     int        any_periodic;    // some system with this term has a periodic box
     int        build_lanes;     // lanes per slot of the list build (8, 16 or 32)
     int        slot_major;      // list layout: 0 blocked by tpp (nbr_index), 1 slot-major (nbr_pos)
+    int        half;            // list form: 0 full (a pair in both partners' lists), 1 half (mixed
+                                // form only: a pair in the list of its lower slot alone, and the
+                                // force launch adds the negated pair force to the partner)
     int        fe_energy;       // energy-only launch: sum the energy as calc_force_and_energy does
                                 // (the generic pair loop skips pairs whose force is zero,
                                 // GlobalPairInteraction.hpp:148-213) instead of calc_energy's

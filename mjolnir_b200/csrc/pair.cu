@@ -115,7 +115,10 @@ struct PairEval {
     float eps12f, epsf, coefcf, debf, invdf, crsqf, wif;
     int kind, power;
     bool fe;                    // energy-only: the force-and-energy rule of the generic loop
+    bool half;                  // half lists: the partner's force is added here too
     const double* slot_p1;
+    void* force;
+    const int* slot_particle;
 
     __device__ __forceinline__ PairEval(const Arena& a, const TermArrays& t, long long slot, int sys)
     {
@@ -141,6 +144,30 @@ struct PairEval {
         debf = (float)debye; invdf = (float)inv_debye;
         crsqf = (float)crsq; wif = (float)pi.w;
         fe = !NF && t.fe_energy != 0;
+        half = PREC == P_MIXED && NF && t.half != 0;
+        force = a.force;
+        slot_particle = t.slot_particle;
+    }
+
+    // Half lists (mixed form): the partner's share of the pair, the negated
+    // fixed-point components of c r_ij.  Its own evaluation of the pair would
+    // take r_ji = -r_ij exactly (an FP64 difference; the minimum image is odd
+    // inside the cutoff), the same coefficient (every potential is symmetric
+    // in its two parameters, and FP32 sums and products commute) and the same
+    // rounding to the grid (round to nearest even is odd), so the integer sum
+    // of each particle is the full lists' sum, bit for bit.
+    __device__ __forceinline__ void partner_add(double c, int q, double dx, double dy, double dz) const
+    {
+        if constexpr(PREC == P_MIXED && NF)
+        {
+            if(!half || c == 0.0) {return;}
+            const long long x = fx_from_double(c * dx), y = fx_from_double(c * dy), z = fx_from_double(c * dz);
+            unsigned long long* f =
+                reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(force) + slot_particle[q]);
+            if(x) {atomicAdd(f + 0, (unsigned long long)(-x));}
+            if(y) {atomicAdd(f + 1, (unsigned long long)(-y));}
+            if(z) {atomicAdd(f + 2, (unsigned long long)(-z));}
+        }
     }
 
     // WCA, LennardJonesAttractive and UniformLennardJones through the generic
@@ -206,7 +233,7 @@ struct PairEval {
     }
     __device__ __forceinline__ void family(int k, double sigma, double epsilon, double l2, double dx,
                                            double dy, double dz, bool count_e, Acc<PREC>& acc,
-                                           double& energy, bool& ovf) const
+                                           double& energy, bool& ovf, int q) const
     {
         using T = typename std::conditional<PREC == P_FP64, double, float>::type;
         if(NF || fe)
@@ -215,7 +242,7 @@ struct PairEval {
             const T l  = T(l2) * rl;
             const T f_mag = fam_derivative<T>(k, l, T(sigma), T(epsilon), T(cr));
             if(f_mag == T(0)) {return;}
-            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf);}
+            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf); partner_add((double)(f_mag * rl), q, dx, dy, dz);}
             if(count_e) {energy += (double)fam_potential<T>(k, l, T(sigma), T(epsilon), T(cr), T(coefc));}
         }
         else if(count_e)
@@ -267,7 +294,7 @@ struct PairEval {
     }
     __device__ __forceinline__ void exv_family(double sigma, double radius, double l2, double dx, double dy,
                                                double dz, bool count_e, Acc<PREC>& acc, double& energy,
-                                               bool& ovf) const
+                                               bool& ovf, int q) const
     {
         using T = typename std::conditional<PREC == P_FP64, double, float>::type;
         if(NF || fe)
@@ -276,7 +303,7 @@ struct PairEval {
             const T l  = T(l2) * rl;
             const T f_mag = exv_derivative<T>(l, T(sigma), T(radius));
             if(f_mag == T(0)) {return;}
-            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf);}
+            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf); partner_add((double)(f_mag * rl), q, dx, dy, dz);}
             if(count_e) {energy += (double)exv_potential<T>(l, T(sigma), T(radius));}
         }
         else if(count_e)
@@ -303,7 +330,7 @@ struct PairEval {
             if(kind != EXV_PLAIN)
             {
                 const double radius = kind == EXV_HARD_CORE ? epsi + slot_p1[q] : 0.0;
-                exv_family(pi.w + pj.w, radius, l2, dx, dy, dz, count_e, acc, energy, ovf);
+                exv_family(pi.w + pj.w, radius, l2, dx, dy, dz, count_e, acc, energy, ovf, q);
                 return;
             }
             const double sigma = pi.w + pj.w;
@@ -328,7 +355,11 @@ struct PairEval {
                 const float s2 = sg * sg * rcp;
                 const float s6 = s2 * s2 * s2;
                 const float cf = in ? -eps12f * s6 * s6 * rcp : 0.0f;
-                if constexpr(NF) {acc.add_c(cf, fabsf(cf) * fmaxf(l2f, 1.0f), dx, dy, dz, ovf);}
+                if constexpr(NF)
+                {
+                    acc.add_c(cf, fabsf(cf) * fmaxf(l2f, 1.0f), dx, dy, dz, ovf);
+                    partner_add((double)cf, q, dx, dy, dz);
+                }
                 if(count_e && in) {energy += (double)(epsf * (s6 * s6 - coefcf));}
             }
         }
@@ -361,6 +392,7 @@ struct PairEval {
                 {
                     const float cf = (float)qq * cu;
                     acc.add_c(cf, fabsf(cf) * l, dx, dy, dz, ovf);
+                    partner_add((double)cf, q, dx, dy, dz);
                 }
                 if(count_e && in) {energy += qq * (double)(ex * rl - coefcf);}
             }
@@ -372,7 +404,7 @@ struct PairEval {
             const double epsilon = (epsi == epsj) ? epsi : sqrt(epsi * epsj);
             if(kind != LJ_PLAIN)
             {
-                family(kind, sigma, epsilon, l2, dx, dy, dz, count_e, acc, energy, ovf);
+                family(kind, sigma, epsilon, l2, dx, dy, dz, count_e, acc, energy, ovf, q);
                 return;
             }
             const double sigma_sq = sigma * sigma;
@@ -396,6 +428,7 @@ struct PairEval {
                 {
                     const float cf = 24.0f * ef * (s6 - 2.0f * s6 * s6) * rcp;
                     acc.add_c(cf, fabsf(cf) * fmaxf(l2f, 1.0f), dx, dy, dz, ovf);
+                    partner_add((double)cf, q, dx, dy, dz);
                 }
                 if(count_e) {energy += (double)(4.0f * ef * (s6 * s6 - s6 - coefcf));}
             }

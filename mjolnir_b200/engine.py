@@ -283,6 +283,19 @@ class Engine:
         self._c(self.lib.mjg_get_pair_schedule(self.ctx, t, C.byref(v)))
         return v.value
 
+    def set_half_lists(self, term, on: bool):
+        """Half Verlet lists for the term (mixed form only): each pair in one
+        list, the partner's force added by the same evaluation; identical
+        results, half the list words and pair evaluations."""
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        self._c(self.lib.mjg_set_half_lists(self.ctx, t, int(bool(on))))
+
+    def get_half_lists(self, term) -> bool:
+        t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
+        v = C.c_int()
+        self._c(self.lib.mjg_get_half_lists(self.ctx, t, C.byref(v)))
+        return bool(v.value)
+
     def set_build_lanes(self, term, lanes: int):
         """Lanes per particle of the term's list build (8, 16 or 32)."""
         t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)

@@ -35,6 +35,8 @@ def _shape(e, shapes):
     for t, c in shapes.items():
         if "margin" in c:
             e.set_margin(t, c["margin"])
+        if e.precision == "mixed":
+            e.set_half_lists(t, c.get("half", False))
         e.set_pair_schedule(t, c["schedule"])
         e.set_threads_per_particle(t, c["tpp"])
         e.set_pair_unroll(t, c["unroll"])

@@ -186,6 +186,8 @@ class Server:
                 self.eng.get_threads_per_particle(key)
             except Exception:
                 continue                         # term not in the arena now
+            if self.eng.precision == "mixed" and self.eng.get_half_lists(key) != cfg.get("half_lists", False):
+                self.eng.set_half_lists(key, cfg.get("half_lists", False))
             if self.eng.get_pair_schedule(key) != cfg.get("schedule", 0):
                 self.eng.set_pair_schedule(key, cfg.get("schedule", 0))
             if self.eng.get_threads_per_particle(key) != cfg.get("threads_per_particle", 1):
