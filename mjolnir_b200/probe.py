@@ -5,9 +5,10 @@
     python -m mjolnir_b200.probe lj [--precision fp64]   # the 4,096-particle Lennard-Jones fluid
 
 `batch` builds the benchmark's 256 independent polymer melts with the launch
-shapes the autotuner picks for them (ExcludedVolume: margin 0.3, block-vector
-schedule with length-sorted threads, 2-word blocks; DebyeHuckel: margin 0.2, 2
-threads per slot with length-sorted groups), steps 300 MD steps, then times
+shapes the autotuner picks for them (ExcludedVolume: margin 0.3, half lists,
+block-vector schedule with length-sorted threads, 2-word blocks; DebyeHuckel:
+margin 0.2, full lists, 2 threads per slot with length-sorted groups), steps
+300 MD steps, then times
 each kernel alone.  `fluid` builds the periodic EXV + DebyeHuckel bead fluid
 (0.003 per cubic A, margins 0.3 / 0.1) with its tuned shapes (ExcludedVolume:
 block-vector schedule, 2-word blocks; DebyeHuckel: slot-major lists, 8
@@ -25,7 +26,7 @@ import torch
 from . import systems as S
 from .engine import Engine
 
-BATCH_SHAPES = {"exv": dict(margin=0.3, schedule=3, tpp=2, unroll=1, lanes=8),
+BATCH_SHAPES = {"exv": dict(margin=0.3, schedule=3, tpp=2, unroll=1, lanes=8, half=True),
                 "dh": dict(margin=0.2, schedule=4, tpp=2, unroll=1, lanes=16)}
 FLUID_SHAPES = {"exv": dict(schedule=2, tpp=2, unroll=1),
                 "dh": dict(schedule=5, tpp=8, unroll=1)}
