@@ -6,6 +6,7 @@ The library is rebuilt only when a source is newer than it.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -55,6 +56,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) \
         + glob.glob(os.path.join(INCLUDE, "*.h"))
     newest_header = max((os.path.getmtime(h) for h in headers), default=0.0)
+    cmds = []
     for src in sources():
         obj = os.path.join(build_dir, os.path.basename(src) + ".o")
         objs.append(obj)
@@ -62,10 +64,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if not force and not ptxas_info and os.path.exists(obj) and \
                 os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_header):
             continue
-        cmd = [nvcc(), *ARCH, *NVFLAGS, *extra, "-I", INCLUDE, "-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True, env=env)
+        cmds.append([nvcc(), *ARCH, *NVFLAGS, *extra, "-I", INCLUDE, "-c", src, "-o", obj])
+    # the translation units compile side by side (the pair kernels' unit
+    # alone takes minutes)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+        for f in [ex.submit(subprocess.run, cmd, check=True, env=env) for cmd in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     subprocess.run(cmd, check=True, env=env)

@@ -105,7 +105,7 @@ template<> struct Acc<P_MIXED>
 // (slot s, partner q).  PER: some system of the arena is periodic (the
 // minimum image is applied where the system asks for it); without it the
 // image code is compiled out.
-template<int PREC, int G, bool NF, bool NE, bool PER>
+template<int PREC, int G, bool NF, bool NE, bool PER, bool HALF = false>
 struct PairEval {
     const SysDev* S;
     double4 pi;
@@ -115,7 +115,6 @@ struct PairEval {
     float eps12f, epsf, coefcf, debf, invdf, crsqf, wif;
     int kind, power;
     bool fe;                    // energy-only: the force-and-energy rule of the generic loop
-    bool half;                  // half lists: the partner's force is added here too
     const double* slot_p1;
     void* force;
     const int* slot_particle;
@@ -144,7 +143,6 @@ struct PairEval {
         debf = (float)debye; invdf = (float)inv_debye;
         crsqf = (float)crsq; wif = (float)pi.w;
         fe = !NF && t.fe_energy != 0;
-        half = PREC == P_MIXED && NF && t.half != 0;
         force = a.force;
         slot_particle = t.slot_particle;
     }
@@ -158,9 +156,9 @@ struct PairEval {
     // of each particle is the full lists' sum, bit for bit.
     __device__ __forceinline__ void partner_add(double c, int q, double dx, double dy, double dz) const
     {
-        if constexpr(PREC == P_MIXED && NF)
+        if constexpr(PREC == P_MIXED && NF && HALF)
         {
-            if(!half || c == 0.0) {return;}
+            if(c == 0.0) {return;}
             const long long x = fx_from_double(c * dx), y = fx_from_double(c * dy), z = fx_from_double(c * dz);
             unsigned long long* f =
                 reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(force) + slot_particle[q]);
@@ -517,7 +515,7 @@ __device__ __forceinline__ int sorted_group(const Arena& a, const TermArrays& t,
 // Both pair kernels are held to 64 registers (four 256-thread blocks per SM):
 // they wait on memory, and the occupancy is worth more than the few words
 // spilled in the widest variants.
-template<int PREC, int G, bool NF, bool NE, int TPP, bool PER, int UNR, bool SORT = false>
+template<int PREC, int G, bool NF, bool NE, int TPP, bool PER, int UNR, bool SORT = false, bool HALF = false>
 __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
 {
     // TPP consecutive threads share one slot; lane lg walks partners lg,
@@ -540,7 +538,7 @@ __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
     Acc<PREC> acc;
     if(active)
     {
-        const PairEval<PREC, G, NF, NE, PER> eval(a, t, s, sys);
+        const PairEval<PREC, G, NF, NE, PER, HALF> eval(a, t, s, sys);
         const long long np = t.np;
         const int n = head.n;
         // word k = lg + r TPP of the slot's list: blocked layout, rows np TPP
@@ -655,7 +653,7 @@ __device__ __forceinline__ void load_block(const int* __restrict__ p, int (&q)[L
 // list blocks (a counting sort in shared memory), so that the lanes of a warp
 // walk lists of about the same length; the slots themselves, and with them
 // the spatial order of the partners, stay where they are.
-template<int PREC, int G, bool PER, int L, bool SORT>
+template<int PREC, int G, bool PER, int L, bool SORT, bool HALF>
 __global__ void __launch_bounds__(TPB, 4) k_pair_vec(Arena a, TermArrays t)
 {
     long long s = (long long)blockIdx.x * TPB + threadIdx.x;
@@ -671,7 +669,7 @@ __global__ void __launch_bounds__(TPB, 4) k_pair_vec(Arena a, TermArrays t)
     double energy = 0.0;
     bool ovf = false;
     Acc<PREC> acc;
-    const PairEval<PREC, G, true, false, PER> eval(a, t, s, sys);
+    const PairEval<PREC, G, true, false, PER, HALF> eval(a, t, s, sys);
     const long long np = t.np;
     const int n = head.n;
     const double4* __restrict__ pd = t.slot_pd;
@@ -712,7 +710,7 @@ __global__ void __launch_bounds__(TPB, 4) k_pair_vec(Arena a, TermArrays t)
 // the sum to the particle's fixed-point force with integer atomics when its
 // chunk leaves that slot; integer sums are exact, so the result does not
 // depend on where the chunks start.
-template<int G, bool PER, int UNR>
+template<int G, bool PER, int UNR, bool HALF>
 __global__ void __launch_bounds__(TPB) k_pair_warp(Arena a, TermArrays t)
 {
     __shared__ int seg[TPB / 32][33];
@@ -756,7 +754,7 @@ __global__ void __launch_bounds__(TPB) k_pair_warp(Arena a, TermArrays t)
         const int b = seg[wl][j];
         const int kend = min(seg[wl][j + 1], e_end) - b;
         const int sys = t.slot_sys[s];
-        const PairEval<P_MIXED, G, true, false, PER> eval(a, t, s, sys);
+        const PairEval<P_MIXED, G, true, false, PER, HALF> eval(a, t, s, sys);
         Acc<P_MIXED> acc;
         double energy = 0.0;
         bool ovf = false;
@@ -832,7 +830,7 @@ __global__ void k_count_cut(Arena a, TermArrays t, int sys_filter, unsigned long
     if((threadIdx.x & 31) == 0 && cnt) {atomicAdd(out, cnt);}
 }
 
-template<int PREC, int G, int TPP, bool PER>
+template<int PREC, int G, int TPP, bool PER, bool HALF>
 void dispatch_per(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
 {
     const unsigned nb = (unsigned)((t.np * TPP + TPB - 1) / TPB);
@@ -845,48 +843,51 @@ void dispatch_per(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t 
             if(t.schedule == 2 || t.schedule == 3)
             {
                 const unsigned nv = (unsigned)((t.np + TPB - 1) / TPB);
-                if(t.schedule == 3) {k_pair_vec<PREC, G, PER, TPP, true ><<<nv, TPB, 0, s>>>(a, t);}
-                else                {k_pair_vec<PREC, G, PER, TPP, false><<<nv, TPB, 0, s>>>(a, t);}
+                if(t.schedule == 3) {k_pair_vec<PREC, G, PER, TPP, true,  HALF><<<nv, TPB, 0, s>>>(a, t);}
+                else                {k_pair_vec<PREC, G, PER, TPP, false, HALF><<<nv, TPB, 0, s>>>(a, t);}
                 return;
             }
         }
         if(PREC == P_MIXED && t.schedule == 1)
         {
             const unsigned nw = (unsigned)((t.np + TPB - 1) / TPB);
-            if(t.unroll == 4)      {k_pair_warp<G, PER, 4><<<nw, TPB, 0, s>>>(a, t);}
-            else if(t.unroll == 2) {k_pair_warp<G, PER, 2><<<nw, TPB, 0, s>>>(a, t);}
-            else                   {k_pair_warp<G, PER, 1><<<nw, TPB, 0, s>>>(a, t);}
+            if(t.unroll == 4)      {k_pair_warp<G, PER, 4, HALF><<<nw, TPB, 0, s>>>(a, t);}
+            else if(t.unroll == 2) {k_pair_warp<G, PER, 2, HALF><<<nw, TPB, 0, s>>>(a, t);}
+            else                   {k_pair_warp<G, PER, 1, HALF><<<nw, TPB, 0, s>>>(a, t);}
         }
         else if(t.schedule == 4)
         {
-            if(t.unroll == 4)      {k_pair<PREC, G, true, false, TPP, PER, 4, true><<<nb, TPB, 0, s>>>(a, t);}
-            else if(t.unroll == 2) {k_pair<PREC, G, true, false, TPP, PER, 2, true><<<nb, TPB, 0, s>>>(a, t);}
-            else                   {k_pair<PREC, G, true, false, TPP, PER, 1, true><<<nb, TPB, 0, s>>>(a, t);}
+            if(t.unroll == 4)      {k_pair<PREC, G, true, false, TPP, PER, 4, true, HALF><<<nb, TPB, 0, s>>>(a, t);}
+            else if(t.unroll == 2) {k_pair<PREC, G, true, false, TPP, PER, 2, true, HALF><<<nb, TPB, 0, s>>>(a, t);}
+            else                   {k_pair<PREC, G, true, false, TPP, PER, 1, true, HALF><<<nb, TPB, 0, s>>>(a, t);}
         }
-        else if(t.unroll == 4) {k_pair<PREC, G, true, false, TPP, PER, 4><<<nb, TPB, 0, s>>>(a, t);}
-        else if(t.unroll == 2) {k_pair<PREC, G, true, false, TPP, PER, 2><<<nb, TPB, 0, s>>>(a, t);}
-        else                   {k_pair<PREC, G, true, false, TPP, PER, 1><<<nb, TPB, 0, s>>>(a, t);}
+        else if(t.unroll == 4) {k_pair<PREC, G, true, false, TPP, PER, 4, false, HALF><<<nb, TPB, 0, s>>>(a, t);}
+        else if(t.unroll == 2) {k_pair<PREC, G, true, false, TPP, PER, 2, false, HALF><<<nb, TPB, 0, s>>>(a, t);}
+        else                   {k_pair<PREC, G, true, false, TPP, PER, 1, false, HALF><<<nb, TPB, 0, s>>>(a, t);}
     }
     else if(ne)   {k_pair<PREC, G, false, true,  TPP, PER, 1><<<nb, TPB, 0, s>>>(a, t);}
 }
 
-template<int PREC, int G, int TPP>
+template<int PREC, int G, int TPP, bool HALF>
 void dispatch_tpp(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
 {
-    if(t.any_periodic) {dispatch_per<PREC, G, TPP, true >(a, t, nf, ne, s);}
-    else               {dispatch_per<PREC, G, TPP, false>(a, t, nf, ne, s);}
+    if(t.any_periodic) {dispatch_per<PREC, G, TPP, true,  HALF>(a, t, nf, ne, s);}
+    else               {dispatch_per<PREC, G, TPP, false, HALF>(a, t, nf, ne, s);}
 }
 
-template<int PREC, int G>
+// HALF: the mixed form's force launch on half lists (the partner's share
+// added by the same evaluation); a template argument, so that the full-list
+// kernels carry none of its code
+template<int PREC, int G, bool HALF = false>
 void dispatch(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
 {
     switch(t.tpp)
     {
-        case 1:  dispatch_tpp<PREC, G, 1 >(a, t, nf, ne, s); break;
-        case 2:  dispatch_tpp<PREC, G, 2 >(a, t, nf, ne, s); break;
-        case 4:  dispatch_tpp<PREC, G, 4 >(a, t, nf, ne, s); break;
-        case 8:  dispatch_tpp<PREC, G, 8 >(a, t, nf, ne, s); break;
-        default: dispatch_tpp<PREC, G, 16>(a, t, nf, ne, s); break;
+        case 1:  dispatch_tpp<PREC, G, 1 , HALF>(a, t, nf, ne, s); break;
+        case 2:  dispatch_tpp<PREC, G, 2 , HALF>(a, t, nf, ne, s); break;
+        case 4:  dispatch_tpp<PREC, G, 4 , HALF>(a, t, nf, ne, s); break;
+        case 8:  dispatch_tpp<PREC, G, 8 , HALF>(a, t, nf, ne, s); break;
+        default: dispatch_tpp<PREC, G, 16, HALF>(a, t, nf, ne, s); break;
     }
 }
 
@@ -918,9 +919,18 @@ void launch_pair(const Arena& a, int g, TermArrays& t, bool need_force, bool nee
         // reference's FP64 arithmetic
         if(need_force)
         {
-            if(g == G_EXV)     {dispatch<P_MIXED, G_EXV>(a, t, true, false, s);}
-            else if(g == G_DH) {dispatch<P_MIXED, G_DH >(a, t, true, false, s);}
-            else               {dispatch<P_MIXED, G_LJ >(a, t, true, false, s);}
+            if(t.half)
+            {
+                if(g == G_EXV)     {dispatch<P_MIXED, G_EXV, true>(a, t, true, false, s);}
+                else if(g == G_DH) {dispatch<P_MIXED, G_DH,  true>(a, t, true, false, s);}
+                else               {dispatch<P_MIXED, G_LJ,  true>(a, t, true, false, s);}
+            }
+            else
+            {
+                if(g == G_EXV)     {dispatch<P_MIXED, G_EXV>(a, t, true, false, s);}
+                else if(g == G_DH) {dispatch<P_MIXED, G_DH >(a, t, true, false, s);}
+                else               {dispatch<P_MIXED, G_LJ >(a, t, true, false, s);}
+            }
         }
         if(need_energy)
         {
