@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
     double energy = 0.0;
     bool ovf = false;
     Acc<PREC> acc;
-    if(active)
+    if(active && head.n > 0)         // the group's slot; an empty list reads nothing
     {
         const PairEval<PREC, G, NF, NE, PER, HALF> eval(a, t, s, sys);
         const long long np = t.np;
@@ -665,6 +665,7 @@ __global__ void __launch_bounds__(TPB, 4) k_pair_vec(Arena a, TermArrays t)
     }
     if(s >= t.np) {return;}
     if(!SORT) {head = slot_head(a, t, s);}
+    if(head.n == 0) {return;}        // an empty list (frequent in half lists): nothing to add
     const int sys = head.sys;
     double energy = 0.0;
     bool ovf = false;
