@@ -440,20 +440,30 @@ void alloc_lists(mjg_context* c, int g, int cap)
 // forced rebuild of every list; grows capacities until nothing overflows
 void rebuild_all(mjg_context* c)
 {
+    // every term's first attempt, then one synchronisation; a term whose
+    // lists overflowed grows them and is rebuilt alone (up to three times)
+    int mx[NGLOBAL] = {};
+    auto attempt = [&](int g) {
+        TermDev& T = c->term[g];
+        CK(cudaMemsetAsync(T.t.max_count, 0, sizeof(int), c->stream));
+        launch_rebuild(c->arena, g, T.t, 1, c->stream);
+        CK(cudaMemcpyAsync(&mx[g], T.t.max_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    };
+    for(int g = 0; g < NGLOBAL; ++g)
+    {
+        if(c->term[g].t.on && c->term[g].t.np > 0) {attempt(g);}
+    }
+    CK(cudaStreamSynchronize(c->stream));
     for(int g = 0; g < NGLOBAL; ++g)
     {
         TermDev& T = c->term[g];
         if(!T.t.on || T.t.np == 0) {continue;}
-        for(int attempt = 0; attempt < 4; ++attempt)
+        for(int k = 0; k < 3 && mx[g] > T.t.cap; ++k)
         {
-            CK(cudaMemsetAsync(T.t.max_count, 0, sizeof(int), c->stream));
-            launch_rebuild(c->arena, g, T.t, 1, c->stream);
-            int mx = 0;
-            CK(cudaMemcpyAsync(&mx, T.t.max_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            if(!T.tpp_fixed) {T.t.tpp = default_tpp(mx[g], T.t.np);}
+            alloc_lists(c, g, list_capacity(mx[g]));
+            attempt(g);
             CK(cudaStreamSynchronize(c->stream));
-            if(mx <= T.t.cap) {break;}
-            if(!T.tpp_fixed) {T.t.tpp = default_tpp(mx, T.t.np);}
-            alloc_lists(c, g, list_capacity(mx));
         }
     }
     // rebuild_all may have raised ST_LIST_OVERFLOW on the way; clear it
@@ -1085,7 +1095,8 @@ void commit(mjg_context* c)
     const bool any_aux = any_underdamped || any_gjf;
     if(any_aux) {c->d_accel.ensure(32 * (size_t)std::max<long long>(n_tot, 1));}
     else        {c->d_accel.release();}
-    c->d_staging.ensure(sizeof(double) * 3 * (size_t)std::max<long long>(n_tot, 1));
+    // room for positions and velocities side by side (bulk state copies)
+    c->d_staging.ensure(sizeof(double) * 6 * (size_t)std::max<long long>(n_tot, 1));
     if(c->rollback)
     {
         c->b_sys.ensure(c->d_sys.bytes);
@@ -2002,17 +2013,11 @@ int mjg_get_state_all(mjg_context* c, double* pos, double* vel)
     ABI_BEGIN(c)
     if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
     double* stg = c->d_staging.as<double>();
-    if(pos)
-    {
-        launch_pack_state(c->arena, stg, 0, 0, c->n_tot, c->stream);
-        CK(cudaMemcpyAsync(pos, stg, sizeof(double) * 3 * c->n_tot, cudaMemcpyDeviceToHost, c->stream));
-    }
-    if(vel)
-    {
-        CK(cudaStreamSynchronize(c->stream));
-        launch_pack_state(c->arena, stg, 1, 0, c->n_tot, c->stream);
-        CK(cudaMemcpyAsync(vel, stg, sizeof(double) * 3 * c->n_tot, cudaMemcpyDeviceToHost, c->stream));
-    }
+    double* stg_vel = stg + 3 * c->n_tot;          // the staging holds both arrays side by side
+    if(pos) {launch_pack_state(c->arena, stg, 0, 0, c->n_tot, c->stream);}
+    if(vel) {launch_pack_state(c->arena, stg_vel, 1, 0, c->n_tot, c->stream);}
+    if(pos) {CK(cudaMemcpyAsync(pos, stg, sizeof(double) * 3 * c->n_tot, cudaMemcpyDeviceToHost, c->stream));}
+    if(vel) {CK(cudaMemcpyAsync(vel, stg_vel, sizeof(double) * 3 * c->n_tot, cudaMemcpyDeviceToHost, c->stream));}
     CK(cudaStreamSynchronize(c->stream));
     ABI_END(c)
 }
@@ -2022,16 +2027,13 @@ int mjg_set_state_all(mjg_context* c, const double* pos, const double* vel)
     ABI_BEGIN(c)
     if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
     double* stg = c->d_staging.as<double>();
-    if(vel)
-    {
-        CK(cudaMemcpyAsync(stg, vel, sizeof(double) * 3 * c->n_tot, cudaMemcpyHostToDevice, c->stream));
-        launch_unpack_state(c->arena, nullptr, stg, 0, c->n_tot, c->stream);
-    }
+    double* stg_vel = stg + 3 * c->n_tot;          // both arrays side by side: one unpack launch
+    if(vel) {CK(cudaMemcpyAsync(stg_vel, vel, sizeof(double) * 3 * c->n_tot, cudaMemcpyHostToDevice, c->stream));}
+    if(pos) {CK(cudaMemcpyAsync(stg, pos, sizeof(double) * 3 * c->n_tot, cudaMemcpyHostToDevice, c->stream));}
+    // positions are taken as given (already inside their boxes)
+    if(pos || vel) {launch_unpack_state(c->arena, pos ? stg : nullptr, vel ? stg_vel : nullptr, 0, c->n_tot, c->stream);}
     if(pos)
     {
-        // positions are taken as given (already inside their boxes)
-        CK(cudaMemcpyAsync(stg, pos, sizeof(double) * 3 * c->n_tot, cudaMemcpyHostToDevice, c->stream));
-        launch_unpack_state(c->arena, stg, nullptr, 0, c->n_tot, c->stream);
         rebuild_all(c);
         compute_initial_forces(c);
         launch_init_accel(c->arena, 0, c->n_tot, c->stream);   // new positions: Integrator::initialize
