@@ -265,8 +265,9 @@ MJG_API int mjg_context_get_stream(mjg_context* ctx, void** stream);
 MJG_API int mjg_time_kernel(mjg_context* ctx, int term, int reps, double* ms_per_launch);
 /* Performance knobs of a global term (they change no result in the mixed
  * form, whose force sums are exact and order independent):
- * threads cooperating on one particle's list in the pair kernel (1, 2, 4, 8
- * or 16; re-lays out and rebuilds the lists), and the relative Verlet margin
+ * threads cooperating on one particle's list in the pair kernel (1, 2, 4, 8,
+ * 16 or 32; re-lays out and rebuilds the lists; schedules 2 and 3 run as
+ * schedule 0 at 32), and the relative Verlet margin
  * of every system that has the term (re-commits: new cell grids, new lists,
  * state kept).  The reference fixes the margin in its input
  * (input/read_spatial_partition.hpp:62-76). */

@@ -10,7 +10,7 @@ For every global term of an :class:`~mjolnir_b200.engine.Engine` it picks
     its list in blocks with vector loads; the first and last optionally with
     each block's threads ordered by list length; or the first on lists stored
     slot by slot, each brought to L2 by one bulk prefetch), the threads per
-    particle / list block (1, 2, 4, 8, 16), the partners each thread
+    particle / list block (1, 2, 4, 8, 16, 32), the partners each thread
     requests per batch (1, 2, 4) and, in the mixed form, full or half lists;
   * the lanes per particle of the list build (8, 16, 32), by timing whole
     steps at the chosen margin and shape.
@@ -35,7 +35,7 @@ def _time_steps(eng, nsteps: int) -> float:
 
 
 def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
-         tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4), schedules=(0, 1, 2, 3, 4, 5), steps: int = 60,
+         tpps=(1, 2, 4, 8, 16, 32), unrolls=(1, 2, 4), schedules=(0, 1, 2, 3, 4, 5), steps: int = 60,
          warm: int = 20, log=None, build_lanes=(8, 16, 32)) -> dict:
     present = []
     for t in terms:
@@ -97,7 +97,7 @@ def _tune_shape(eng, term, tpps, unrolls, schedules):
         for sch in schedules:
             eng.set_pair_schedule(term, sch)
             for p in tpps:
-                if sch in (2, 3) and p == 1:
+                if sch in (2, 3) and p in (1, 32):
                     continue                  # the same launch as schedule 0
                 if sch == 5 and p < 8:
                     continue                  # slot-major lists want whole 32-byte sectors per group
@@ -110,7 +110,7 @@ def _tune_shape(eng, term, tpps, unrolls, schedules):
     return best[1]
 
 
-def tune_shapes(eng, terms=("exv", "dh", "lj"), tpps=(1, 2, 4, 8, 16), unrolls=(1, 2, 4),
+def tune_shapes(eng, terms=("exv", "dh", "lj"), tpps=(1, 2, 4, 8, 16, 32), unrolls=(1, 2, 4),
                 schedules=(0, 1, 2, 3, 4, 5)) -> dict:
     """Launch shape only (margins as committed): for a single large system,
     where the margin is fixed by the input."""

@@ -407,7 +407,7 @@ void upload_sys(mjg_context* c)
 
 // room for growth; a multiple of 16 so that every threads-per-slot choice
 // tiles the blocked layout
-int list_capacity(int max_count) {return ((max_count + max_count / 4 + 16) + 15) / 16 * 16;}
+int list_capacity(int max_count) {return ((max_count + max_count / 4 + 16) + 31) / 32 * 32;}
 
 // threads per slot of the pair kernel from the longest list, widened for
 // arenas with few slots until the launch fills the GPU (about 148 SMs x 1,024
@@ -417,14 +417,15 @@ int list_capacity(int max_count) {return ((max_count + max_count / 4 + 16) + 15)
 int default_tpp(int max_count, long long slots)
 {
     int tpp = max_count >= 192 ? 8 : (max_count >= 48 ? 4 : (max_count >= 12 ? 2 : 1));
-    while(tpp < 16 && tpp < max_count && slots * tpp < 148LL * 1024) {tpp *= 2;}
+    while(tpp < 32 && tpp < max_count && slots * tpp < 148LL * 1024) {tpp *= 2;}
     return tpp;
 }
 
-// words per slot the neighbour buffer holds for capacity cap: at least 16
-// (the widest block of the blocked layout), because the force launches read
-// a slot's first block before they know its length
-size_t list_words(int cap) {return (size_t)std::max(cap, 16);}
+// words per slot the neighbour buffer holds for capacity cap: a multiple of
+// 32 and at least 32 (the widest group of the blocked layout), because the
+// force launches read a slot's first block before they know its length and
+// a blocked row holds tpp words of every slot
+size_t list_words(int cap) {return (size_t)std::max((cap + 31) / 32 * 32, 32);}
 
 // sizes the neighbour arrays of term g for capacity cap (the buffer only grows)
 void alloc_lists(mjg_context* c, int g, int cap)
@@ -2094,7 +2095,7 @@ int mjg_neighbors(mjg_context* c, int sys, int term, int64_t* pairs, int64_t cap
     std::vector<int> nnb(t.np), part(t.np);
     CK(cudaMemcpy(nnb.data(), t.nnb, sizeof(int) * t.np, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(part.data(), t.slot_particle, sizeof(int) * t.np, cudaMemcpyDeviceToHost));
-    std::vector<int> all((size_t)t.cap * (size_t)t.np);
+    std::vector<int> all(list_words(t.cap) * (size_t)t.np);
     if(!all.empty())
     {
         CK(cudaMemcpy(all.data(), t.nbr, sizeof(int) * all.size(), cudaMemcpyDeviceToHost));
@@ -2228,7 +2229,10 @@ int mjg_set_threads_per_particle(mjg_context* c, int term, int tpp)
     ABI_BEGIN(c)
     if(!c->committed) {throw Error(MJG_ESTATE, "mjg_commit first");}
     if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "threads per slot apply to global terms");}
-    if(tpp != 1 && tpp != 2 && tpp != 4 && tpp != 8 && tpp != 16) {throw Error(MJG_EINVAL, "tpp must be 1, 2, 4, 8 or 16");}
+    if(tpp != 1 && tpp != 2 && tpp != 4 && tpp != 8 && tpp != 16 && tpp != 32)
+    {
+        throw Error(MJG_EINVAL, "tpp must be 1, 2, 4, 8, 16 or 32");
+    }
     TermDev& T = c->term[term - MJG_TERM_EXV];
     if(!T.t.on) {throw Error(MJG_EINVAL, "term not present");}
     T.tpp_fixed = true;

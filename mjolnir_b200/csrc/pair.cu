@@ -839,7 +839,7 @@ void dispatch_per(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t 
     else if(nf)
     {
         // the per-step force launch: schedule and partner batch depth are tunable
-        if constexpr(TPP > 1)
+        if constexpr(TPP > 1 && TPP <= 16)   // 32-word blocks: the slot-per-group kernel instead
         {
             if(t.schedule == 2 || t.schedule == 3)
             {
@@ -888,7 +888,8 @@ void dispatch(const Arena& a, TermArrays& t, bool nf, bool ne, cudaStream_t s)
         case 2:  dispatch_tpp<PREC, G, 2 , HALF>(a, t, nf, ne, s); break;
         case 4:  dispatch_tpp<PREC, G, 4 , HALF>(a, t, nf, ne, s); break;
         case 8:  dispatch_tpp<PREC, G, 8 , HALF>(a, t, nf, ne, s); break;
-        default: dispatch_tpp<PREC, G, 16, HALF>(a, t, nf, ne, s); break;
+        case 16: dispatch_tpp<PREC, G, 16, HALF>(a, t, nf, ne, s); break;
+        default: dispatch_tpp<PREC, G, 32, HALF>(a, t, nf, ne, s); break;
     }
 }
 

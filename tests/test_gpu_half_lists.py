@@ -71,8 +71,8 @@ MIXED = [S.polymer_melt(nchains=4, nbeads=60, radius=45.0, seed=41),
          S.lj_fluid(n=512, seed=43)]
 
 
-@pytest.mark.parametrize("schedule,tpp", [(0, 1), (0, 4), (1, 1), (1, 16), (2, 2), (3, 4), (4, 2),
-                                          (4, 16), (5, 8)])
+@pytest.mark.parametrize("schedule,tpp", [(0, 1), (0, 4), (0, 32), (1, 1), (1, 16), (2, 2), (3, 4),
+                                          (4, 2), (4, 16), (4, 32), (5, 8), (5, 32)])
 def test_half_lists_equal_full_lists_every_schedule(schedule, tpp):
     ref = run(MIXED, False, 0, 1)
     got = run(MIXED, True, schedule, tpp)

@@ -236,12 +236,13 @@ def test_launch_shapes_give_the_same_trajectory(precision):
              S.bead_fluid(n=3000, density=0.003, seed=42, dt=0.3),
              S.lj_fluid(n=512, seed=43)]
     ref = None
-    shapes = [(0, tpp, unr) for tpp in (1, 2, 4, 8, 16) for unr in (1, 2, 4)]
+    shapes = [(0, tpp, unr) for tpp in (1, 2, 4, 8, 16, 32) for unr in (1, 2, 4)]
     shapes += [(sch, tpp, 1) for sch in (2, 3) for tpp in (2, 4, 8, 16)]
-    shapes += [(4, tpp, unr) for tpp in (1, 4, 16) for unr in (1, 2)]
-    shapes += [(5, tpp, unr) for tpp in (1, 8, 16) for unr in (1, 2, 4)]      # slot-major lists
+    shapes += [(4, tpp, unr) for tpp in (1, 4, 16, 32) for unr in (1, 2)]
+    shapes += [(5, tpp, unr) for tpp in (1, 8, 16, 32) for unr in (1, 2, 4)]      # slot-major lists
+    shapes += [(2, 32, 1), (3, 32, 1)]                                            # run as schedule 0
     if precision == "mixed":
-        shapes += [(1, tpp, unr) for tpp in (1, 16) for unr in (1, 2, 4)]
+        shapes += [(1, tpp, unr) for tpp in (1, 16, 32) for unr in (1, 2, 4)]
     for sch, tpp, unr in shapes:
         e = Engine(precision)
         ids = [e.add_system(d) for d in descs]
