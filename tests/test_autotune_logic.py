@@ -66,3 +66,32 @@ def test_the_fastest_measured_shape_is_applied(best):
     assert shape == best
     autotune._apply(e, "exv", shape)
     assert (e.state["schedule"], e.state["tpp"], e.state["unroll"], e.state["half"]) == best
+
+
+def test_margin_choice_prefers_the_narrowest_within_one_percent(monkeypatch):
+    """Whole-step times per margin (a fake clock): the fastest is 0.5, but
+    0.3 is within 1 % of it and narrower, so 0.3 is kept; the build lanes
+    are then chosen at that margin."""
+    step_ms = {0.1: 1.0, 0.2: 0.8, 0.3: 0.795, 0.5: 0.79}
+    lanes_ms = {8: 0.70, 16: 0.69, 32: 0.72}
+
+    class Eng(FakeEngine):
+        def __init__(self):
+            super().__init__("mixed", lambda k: 1.0)
+            self.margin, self.lanes, self.timing_lanes = None, None, False
+
+        def set_margin(self, term, m):
+            self.margin = m
+
+        def set_build_lanes(self, term, lanes):
+            self.lanes, self.timing_lanes = lanes, True
+
+        def step(self, n):
+            pass
+
+    e = Eng()
+    monkeypatch.setattr(autotune, "_time_steps",
+                        lambda eng, n: lanes_ms[eng.lanes] if eng.timing_lanes else step_ms[eng.margin])
+    choice = autotune.tune(e, terms=("exv",))
+    assert choice["exv"]["margin"] == 0.3 and e.margin == 0.3
+    assert choice["exv"]["build_lanes"] == 16 and e.lanes == 16
