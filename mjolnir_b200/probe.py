@@ -7,7 +7,7 @@
 `batch` builds the benchmark's 256 independent polymer melts with the launch
 shapes the autotuner picks for them (ExcludedVolume: margin 0.3, half lists,
 block-vector schedule with length-sorted threads, 2-word blocks; DebyeHuckel:
-margin 0.2, full lists, 2 threads per slot with length-sorted groups), steps
+margin 0.1, full lists, 2 threads per slot with length-sorted groups), steps
 300 MD steps, then times
 each kernel alone.  `fluid` builds the periodic EXV + DebyeHuckel bead fluid
 (0.003 per cubic A, margins 0.3 / 0.1) with its tuned shapes (ExcludedVolume:
@@ -27,7 +27,7 @@ from . import systems as S
 from .engine import Engine
 
 BATCH_SHAPES = {"exv": dict(margin=0.3, schedule=3, tpp=2, unroll=1, lanes=8, half=True),
-                "dh": dict(margin=0.2, schedule=4, tpp=2, unroll=1, lanes=16)}
+                "dh": dict(margin=0.1, schedule=4, tpp=2, unroll=1, lanes=16)}
 FLUID_SHAPES = {"exv": dict(schedule=2, tpp=2, unroll=1),
                 "dh": dict(schedule=5, tpp=8, unroll=1)}
 
