@@ -364,7 +364,7 @@ def fluid_pair_roofline(local, peak, steps=200):
         e.add_system(d)
         e.commit()
         e.step(2)
-        tuned = autotune.tune(e, terms=("exv", "dh"), margins=(0.05, 0.1, 0.2, 0.3), steps=40, warm=10)
+        tuned = autotune.tune(e, terms=("exv", "dh"), margins=(0.05, 0.1, 0.2, 0.3), steps=100, warm=100)
         stream = torch.cuda.ExternalStream(e.stream_handle(), device=local)
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
