@@ -34,7 +34,7 @@ def _time_steps(eng, nsteps: int) -> float:
     return a.elapsed_time(b) / nsteps
 
 
-def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.2, 0.3, 0.5),
+def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.15, 0.2, 0.25, 0.3, 0.4, 0.5),
          tpps=(1, 2, 4, 8, 16, 32), unrolls=(1, 2, 4), schedules=(0, 1, 2, 3, 4, 5), steps: int = 200,
          warm: int = 300, log=None, build_lanes=(8, 16, 32)) -> dict:
     """`warm` steps after each change before `steps` timed ones: a new margin

@@ -92,6 +92,6 @@ def test_margin_choice_prefers_the_narrowest_within_one_percent(monkeypatch):
     e = Eng()
     monkeypatch.setattr(autotune, "_time_steps",
                         lambda eng, n: lanes_ms[eng.lanes] if eng.timing_lanes else step_ms[eng.margin])
-    choice = autotune.tune(e, terms=("exv",))
+    choice = autotune.tune(e, terms=("exv",), margins=tuple(step_ms))
     assert choice["exv"]["margin"] == 0.3 and e.margin == 0.3
     assert choice["exv"]["build_lanes"] == 16 and e.lanes == 16
