@@ -5,7 +5,7 @@
     python -m mjolnir_b200.probe lj [--precision fp64]   # the 4,096-particle Lennard-Jones fluid
 
 `batch` builds the benchmark's 256 independent polymer melts with the launch
-shapes the autotuner picks for them (ExcludedVolume: margin 0.3, half lists,
+shapes the autotuner picks for them (ExcludedVolume: margin 0.25, half lists,
 block-vector schedule with length-sorted threads, 2-word blocks; DebyeHuckel:
 margin 0.1, full lists, 2 threads per slot with length-sorted groups), steps
 300 MD steps, then times
@@ -26,7 +26,7 @@ import torch
 from . import systems as S
 from .engine import Engine
 
-BATCH_SHAPES = {"exv": dict(margin=0.3, schedule=3, tpp=2, unroll=1, lanes=8, half=True),
+BATCH_SHAPES = {"exv": dict(margin=0.25, schedule=3, tpp=2, unroll=1, lanes=8, half=True),
                 "dh": dict(margin=0.1, schedule=4, tpp=2, unroll=1, lanes=16)}
 FLUID_SHAPES = {"exv": dict(schedule=2, tpp=2, unroll=1),
                 "dh": dict(schedule=5, tpp=8, unroll=1)}
