@@ -306,7 +306,7 @@ MJG_API int mjg_get_pair_schedule(mjg_context* ctx, int term, int* schedule);
  * (GlobalPairInteraction.hpp:148-213). */
 MJG_API int mjg_set_half_lists(mjg_context* ctx, int term, int on);
 MJG_API int mjg_get_half_lists(mjg_context* ctx, int term, int* on);
-/* Lanes per particle of a global term's list build (8, 16 or 32): fewer
+/* Lanes per particle of a global term's list build (4, 8, 16 or 32): fewer
  * lanes build several lists per warp at once, which pays when a particle has
  * few candidates in its 27 neighbouring cells.  Unless set here, each commit
  * picks it from the candidates an even filling of the grids would give

@@ -12,7 +12,7 @@ For every global term of an :class:`~mjolnir_b200.engine.Engine` it picks
     slot by slot, each brought to L2 by one bulk prefetch), the threads per
     particle / list block (1, 2, 4, 8, 16, 32), the partners each thread
     requests per batch (1, 2, 4) and, in the mixed form, full or half lists;
-  * the lanes per particle of the list build (8, 16, 32), by timing whole
+  * the lanes per particle of the list build (4, 8, 16, 32), by timing whole
     steps at the chosen margin and shape.
 In the mixed form none of the choices changes a result: the fixed-point force
 sums do not depend on list order or length, and the lists are the same.  The engine's systems keep stepping
@@ -36,7 +36,7 @@ def _time_steps(eng, nsteps: int) -> float:
 
 def tune(eng, terms=("exv", "dh", "lj"), margins=(0.1, 0.15, 0.2, 0.25, 0.3, 0.4, 0.5),
          tpps=(1, 2, 4, 8, 16, 32), unrolls=(1, 2, 4), schedules=(0, 1, 2, 3, 4, 5), steps: int = 200,
-         warm: int = 300, log=None, build_lanes=(8, 16, 32)) -> dict:
+         warm: int = 300, log=None, build_lanes=(4, 8, 16, 32)) -> dict:
     """`warm` steps after each change before `steps` timed ones: a new margin
     rebuilds every list at once, and the rebuilds only spread out to their
     steady rate after a few rebuild intervals -- a short window after the

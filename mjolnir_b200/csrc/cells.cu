@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(TPB) k_build_list(Arena a, int g, TermArrays t
     }
 }
 
-// The same list build with LPS lanes per slot (8 or 16): a warp builds 32 /
+// The same list build with LPS lanes per slot (4, 8 or 16): a warp builds 32 /
 // LPS lists at once, so that short candidate sequences (a few partners per
 // stencil) do not leave most of a warp idle while it waits on memory.  A
 // group's 27 stencil ranges go through shared memory; candidate k of the
@@ -629,7 +629,8 @@ void launch_rebuild(const Arena& a, int g, TermArrays& t, int force_all, cudaStr
     k_cells_scatter<<<GRID, TPB, 0, s>>>(t, t.slot_particle);
     k_cells_sort  <<<GRID, TPB, 0, s>>>(t, t.slot_particle);
     k_slots_setup <<<GRID, TPB, 0, s>>>(a, t);
-    if(t.build_lanes == 8)       {k_build_list_sub<8> <<<GRID, TPB, 0, s>>>(a, g, t);}
+    if(t.build_lanes == 4)       {k_build_list_sub<4> <<<GRID, TPB, 0, s>>>(a, g, t);}
+    else if(t.build_lanes == 8)  {k_build_list_sub<8> <<<GRID, TPB, 0, s>>>(a, g, t);}
     else if(t.build_lanes == 16) {k_build_list_sub<16><<<GRID, TPB, 0, s>>>(a, g, t);}
     else                         {k_build_list        <<<GRID, TPB, 0, s>>>(a, g, t);}
     k_rebuild_done<<<blocks(a.nsys, 128), 128, 0, s>>>(a, g, t, force_all);

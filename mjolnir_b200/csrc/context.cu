@@ -144,7 +144,7 @@ struct TermDev {
                                  // 2 block-vector, 3 block-vector with length-sorted threads,
                                  // 4 slot per threads with length-sorted groups, 5 slot-major lists)
     bool half_choice = false;    // half lists (mixed form only)
-    int build_lanes_choice = 32; // lanes per slot of the list build (8, 16, 32)
+    int build_lanes_choice = 32; // lanes per slot of the list build (4, 8, 16, 32)
     bool build_lanes_fixed = false;  // ... chosen by the caller (else from the expected candidates)
     TermArrays t{};
 };
@@ -2320,7 +2320,7 @@ int mjg_set_build_lanes(mjg_context* c, int term, int lanes)
 {
     ABI_BEGIN(c)
     if(term < MJG_TERM_EXV || term > MJG_TERM_LJ) {throw Error(MJG_EINVAL, "build lanes apply to global terms");}
-    if(lanes != 8 && lanes != 16 && lanes != 32) {throw Error(MJG_EINVAL, "lanes must be 8, 16 or 32");}
+    if(lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) {throw Error(MJG_EINVAL, "lanes must be 4, 8, 16 or 32");}
     TermDev& T = c->term[term - MJG_TERM_EXV];
     T.build_lanes_fixed = true;
     T.build_lanes_choice = lanes;

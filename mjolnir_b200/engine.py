@@ -297,7 +297,7 @@ class Engine:
         return bool(v.value)
 
     def set_build_lanes(self, term, lanes: int):
-        """Lanes per particle of the term's list build (8, 16 or 32)."""
+        """Lanes per particle of the term's list build (4, 8, 16 or 32)."""
         t = A.TERM_NAMES.index(term) if isinstance(term, str) else int(term)
         self._c(self.lib.mjg_set_build_lanes(self.ctx, t, int(lanes)))
 

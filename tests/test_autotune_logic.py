@@ -73,7 +73,7 @@ def test_margin_choice_prefers_the_narrowest_within_one_percent(monkeypatch):
     0.3 is within 1 % of it and narrower, so 0.3 is kept; the build lanes
     are then chosen at that margin."""
     step_ms = {0.1: 1.0, 0.2: 0.8, 0.3: 0.795, 0.5: 0.79}
-    lanes_ms = {8: 0.70, 16: 0.69, 32: 0.72}
+    lanes_ms = {4: 0.71, 8: 0.70, 16: 0.69, 32: 0.72}
 
     class Eng(FakeEngine):
         def __init__(self):

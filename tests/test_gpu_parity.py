@@ -288,7 +288,7 @@ def test_simulated_annealing_matches_oracle():
     e.close()
 
 
-@pytest.mark.parametrize("lanes", [8, 16, 32])
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
 @pytest.mark.parametrize("case", ["melt", "fluid"])
 def test_build_lanes_give_the_same_lists(case, lanes):
     """Every lanes-per-particle choice of the list build gives the reference's
