@@ -98,12 +98,13 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.span = [0, None]          # lines that arrived between mark_start and mark_end
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -114,6 +115,20 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_first(self, seconds=3.0):
+        """Until the first sample arrives (nvidia-smi takes a moment to start)."""
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < seconds:
+            time.sleep(0.02)
+
+    def mark_start(self):
+        self.span[0] = len(self.lines)
+
+    def mark_end(self):
+        # the sample in flight when the region ends still saw it
+        time.sleep(0.11)
+        self.span[1] = len(self.lines)
 
     def __exit__(self, *exc):
         if self.proc:
@@ -126,7 +141,8 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines[self.span[0]:self.span[1]] or self.lines[self.span[0]:] or self.lines
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -486,16 +502,19 @@ def run_b200(args, ws, rank, local, pg):
         from mjolnir_b200 import autotune
         tuned = autotune.tune(eng, log=lambda m: print(m, file=sys.stderr))
 
-    # ---- device-resident throughput
-    for _ in range(args.warmup):
-        eng.step(CHUNK)
-    eng.synchronize()
-    barrier(pg)
-    l0 = eng.launch_count()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    # ---- device-resident throughput (the clock samples kept are those taken
+    # during the timed steps; the sampler starts before the warm-up)
     with ClockSampler(local) as clocks:
+        clocks.wait_first()
+        for _ in range(args.warmup):
+            eng.step(CHUNK)
+        eng.synchronize()
+        barrier(pg)
+        l0 = eng.launch_count()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        clocks.mark_start()
         torch.cuda.nvtx.range_push("timed")     # profilers select the timed launches by this range
         e0.record(stream)
         for _ in range(args.steps):
@@ -504,6 +523,7 @@ def run_b200(args, ws, rank, local, pg):
         e1.synchronize()
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
+        clocks.mark_end()
     launches = eng.launch_count() - l0
     t_dev = e0.elapsed_time(e1) / 1e3
     t_dev = max_over_ranks(t_dev, pg)
