@@ -47,3 +47,19 @@ def test_other_schedule_list_form_or_kernel_reports_none(bench, records):
     assert b is None and "lists" in why
     b, why = bench.ncu_traffic("no_such_kernel", 0, 1, False)
     assert b is None
+
+
+def test_clock_summary_keeps_the_timed_span(bench):
+    """The clock summary uses only the samples taken between mark_start and
+    mark_end, and reports any throttle reason seen there."""
+    c = bench.ClockSampler(0)
+    row = "0, {sm}, 1965, 700.0, 0x0, Not Active, Not Active, {therm}, Not Active"
+    c.lines = [row.format(sm=1000, therm="Active")]                     # warm-up, throttled
+    c.span[0] = len(c.lines)
+    c.lines += [row.format(sm=1965, therm="Not Active") for _ in range(5)]
+    c.span[1] = len(c.lines)
+    c.lines += [row.format(sm=900, therm="Active")]                     # after the timed steps
+    s = c.summary()
+    assert s == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 5}
+    c.lines[2] = row.format(sm=1500, therm="Active")
+    assert c.summary()["reasons"] == ["sw_thermal_slowdown"]
