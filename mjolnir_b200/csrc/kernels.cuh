@@ -40,7 +40,7 @@ struct TermArrays {
     long long  np;              // participants (= slots)
     int        ncell;           // total cells over all systems
     int        cap;             // neighbour capacity per slot (a multiple of tpp)
-    int        tpp;             // threads per slot of the pair kernel (1, 2, 4, 8, 16)
+    int        tpp;             // threads per slot of the pair kernel (1, 2, 4, 8, 16, 32)
     int        unroll;          // partners requested per batch by the force launch (1, 2, 4)
     int        schedule;        // force launch: 0 = slot per tpp threads, 1 = warp-balanced (mixed),
                                 // 2 = one thread per slot reading tpp-word blocks of its list,

@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(TPB, 4) k_pair(Arena a, TermArrays t)
         // word k = lg + r TPP of the slot's list: blocked layout, rows np TPP
         // words apart; slot-major layout, the slot's cap words in a row, the
         // whole list requested into L2 (16-byte aligned: cap is a multiple of
-        // 16 words) before the walk starts
+        // 32 words) before the walk starts
         const bool sm = t.slot_major != 0;
         const long long rs = sm ? TPP : np * TPP;
         const int* __restrict__ nbr = t.nbr + (sm ? s * t.cap : s * TPP) + lg;
