@@ -154,14 +154,15 @@ struct PairEval {
     // in its two parameters, and FP32 sums and products commute) and the same
     // rounding to the grid (round to nearest even is odd), so the integer sum
     // of each particle is the full lists' sum, bit for bit.
-    __device__ __forceinline__ void partner_add(double c, int q, double dx, double dy, double dz) const
+    // jp: the partner's particle when the caller has read it with its coordinates
+    __device__ __forceinline__ void partner_add(double c, int q, double dx, double dy, double dz, int jp = -1) const
     {
         if constexpr(PREC == P_MIXED && NF && HALF)
         {
             if(c == 0.0) {return;}
             const long long x = fx_from_double(c * dx), y = fx_from_double(c * dy), z = fx_from_double(c * dz);
             unsigned long long* f =
-                reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(force) + slot_particle[q]);
+                reinterpret_cast<unsigned long long*>(static_cast<longlong4*>(force) + (jp >= 0 ? jp : slot_particle[q]));
             if(x) {atomicAdd(f + 0, (unsigned long long)(-x));}
             if(y) {atomicAdd(f + 1, (unsigned long long)(-y));}
             if(z) {atomicAdd(f + 2, (unsigned long long)(-z));}
@@ -231,7 +232,7 @@ struct PairEval {
     }
     __device__ __forceinline__ void family(int k, double sigma, double epsilon, double l2, double dx,
                                            double dy, double dz, bool count_e, Acc<PREC>& acc,
-                                           double& energy, bool& ovf, int q) const
+                                           double& energy, bool& ovf, int q, int jp) const
     {
         using T = typename std::conditional<PREC == P_FP64, double, float>::type;
         if(NF || fe)
@@ -240,7 +241,7 @@ struct PairEval {
             const T l  = T(l2) * rl;
             const T f_mag = fam_derivative<T>(k, l, T(sigma), T(epsilon), T(cr));
             if(f_mag == T(0)) {return;}
-            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf); partner_add((double)(f_mag * rl), q, dx, dy, dz);}
+            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf); partner_add((double)(f_mag * rl), q, dx, dy, dz, jp);}
             if(count_e) {energy += (double)fam_potential<T>(k, l, T(sigma), T(epsilon), T(cr), T(coefc));}
         }
         else if(count_e)
@@ -292,7 +293,7 @@ struct PairEval {
     }
     __device__ __forceinline__ void exv_family(double sigma, double radius, double l2, double dx, double dy,
                                                double dz, bool count_e, Acc<PREC>& acc, double& energy,
-                                               bool& ovf, int q) const
+                                               bool& ovf, int q, int jp) const
     {
         using T = typename std::conditional<PREC == P_FP64, double, float>::type;
         if(NF || fe)
@@ -301,7 +302,7 @@ struct PairEval {
             const T l  = T(l2) * rl;
             const T f_mag = exv_derivative<T>(l, T(sigma), T(radius));
             if(f_mag == T(0)) {return;}
-            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf); partner_add((double)(f_mag * rl), q, dx, dy, dz);}
+            if(NF) {acc.add((double)(f_mag * rl), dx, dy, dz, ovf); partner_add((double)(f_mag * rl), q, dx, dy, dz, jp);}
             if(count_e) {energy += (double)exv_potential<T>(l, T(sigma), T(radius));}
         }
         else if(count_e)
@@ -312,7 +313,7 @@ struct PairEval {
     }
 
     __device__ __forceinline__ void operator()(const double4& pj, const int q, Acc<PREC>& acc,
-                                               double& energy, bool& ovf) const
+                                               double& energy, bool& ovf, int jp = -1) const
     {
         double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
         if(PER && periodic)
@@ -328,7 +329,7 @@ struct PairEval {
             if(kind != EXV_PLAIN)
             {
                 const double radius = kind == EXV_HARD_CORE ? epsi + slot_p1[q] : 0.0;
-                exv_family(pi.w + pj.w, radius, l2, dx, dy, dz, count_e, acc, energy, ovf, q);
+                exv_family(pi.w + pj.w, radius, l2, dx, dy, dz, count_e, acc, energy, ovf, q, jp);
                 return;
             }
             const double sigma = pi.w + pj.w;
@@ -356,7 +357,7 @@ struct PairEval {
                 if constexpr(NF)
                 {
                     acc.add_c(cf, fabsf(cf) * fmaxf(l2f, 1.0f), dx, dy, dz, ovf);
-                    partner_add((double)cf, q, dx, dy, dz);
+                    partner_add((double)cf, q, dx, dy, dz, jp);
                 }
                 if(count_e && in) {energy += (double)(epsf * (s6 * s6 - coefcf));}
             }
@@ -390,7 +391,7 @@ struct PairEval {
                 {
                     const float cf = (float)qq * cu;
                     acc.add_c(cf, fabsf(cf) * l, dx, dy, dz, ovf);
-                    partner_add((double)cf, q, dx, dy, dz);
+                    partner_add((double)cf, q, dx, dy, dz, jp);
                 }
                 if(count_e && in) {energy += qq * (double)(ex * rl - coefcf);}
             }
@@ -402,7 +403,7 @@ struct PairEval {
             const double epsilon = (epsi == epsj) ? epsi : sqrt(epsi * epsj);
             if(kind != LJ_PLAIN)
             {
-                family(kind, sigma, epsilon, l2, dx, dy, dz, count_e, acc, energy, ovf, q);
+                family(kind, sigma, epsilon, l2, dx, dy, dz, count_e, acc, energy, ovf, q, jp);
                 return;
             }
             const double sigma_sq = sigma * sigma;
@@ -426,7 +427,7 @@ struct PairEval {
                 {
                     const float cf = 24.0f * ef * (s6 - 2.0f * s6 * s6) * rcp;
                     acc.add_c(cf, fabsf(cf) * fmaxf(l2f, 1.0f), dx, dy, dz, ovf);
-                    partner_add((double)cf, q, dx, dy, dz);
+                    partner_add((double)cf, q, dx, dy, dz, jp);
                 }
                 if(count_e) {energy += (double)(4.0f * ef * (s6 * s6 - s6 - coefcf));}
             }
@@ -690,10 +691,15 @@ __global__ void __launch_bounds__(TPB, 4) k_pair_vec(Arena a, TermArrays t)
         for(int u0 = 0; u0 < L; u0 += W)
         {
             double4 pv[W];
+            int jv[W];                               // half lists: the partners' particles, read beside
+#pragma unroll                                       // their coordinates, so the atomics wait on nothing
+            for(int u = 0; u < W; ++u)
+            {
+                pv[u] = u0 + u < m ? pd[q[u0 + u]] : eval.pi;
+                jv[u] = HALF && u0 + u < m ? t.slot_particle[q[u0 + u]] : -1;
+            }
 #pragma unroll
-            for(int u = 0; u < W; ++u) {pv[u] = u0 + u < m ? pd[q[u0 + u]] : eval.pi;}
-#pragma unroll
-            for(int u = 0; u < W; ++u) {if(u0 + u < m) {eval(pv[u], q[u0 + u], acc, energy, ovf);}}
+            for(int u = 0; u < W; ++u) {if(u0 + u < m) {eval(pv[u], q[u0 + u], acc, energy, ovf, jv[u]);}}
         }
 #pragma unroll
         for(int u = 0; u < L; ++u) {q[u] = qn[u];}

@@ -4,7 +4,7 @@ fixed-point pair force to the partner.  The integer sums are the full lists'
 sums, so every result is the full lists' result bit for bit: forces,
 trajectories through list rebuilds and rollbacks, the exported pairs
 (SpatialPartition::neighbors' half list, core/NeighborList.hpp:151-266) and
-the energies (to FP64 summation order), over every force-launch schedule,
+the energies (to FP64 summation order, 1e-10), over every force-launch schedule,
 every potential of the three global terms and the cell-list edge cases."""
 import numpy as np
 import pytest
@@ -61,9 +61,11 @@ def same(a, b, what):
         assert np.array_equal(x, y), what
     for x, y in zip(a["state"], b["state"]):
         assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1]), what
+    # energies: FP64 sums added with atomics in arrival order (a DebyeHuckel
+    # energy of cancelling charges keeps ~1e-13 of that order)
     for x, y in zip(a["energy"], b["energy"]):
         for k in x:
-            assert abs(x[k] - y[k]) <= 1e-12 * max(abs(y[k]), 1e-12), (what, k, x[k], y[k])
+            assert abs(x[k] - y[k]) <= 1e-10 * max(abs(y[k]), 1e-12), (what, k, x[k], y[k])
 
 
 MIXED = [S.polymer_melt(nchains=4, nbeads=60, radius=45.0, seed=41),

@@ -357,7 +357,9 @@ def test_frozen_system_waits_and_resumes(precision):
 def test_bulk_state_copies_match_per_system_state(precision):
     """mjg_get_state_all returns every system's state in arena order, and
     mjg_set_state_all followed by steps gives the trajectory of per-system
-    mjg_set_state calls with the same arrays, bit for bit."""
+    mjg_set_state calls with the same arrays: bit for bit in the mixed form,
+    to rounding in FP64 (whose bonded sums add in shared memory in the order
+    the threads arrive)."""
     descs = [S.polymer_melt(nchains=3, nbeads=40, radius=35.0, seed=60),
              S.bead_fluid(n=2000, density=0.003, seed=61, dt=0.3),
              S.lj_fluid(n=343, seed=62)]
@@ -390,4 +392,8 @@ def test_bulk_state_copies_match_per_system_state(precision):
     each = [e.state(sid)[:2] for sid in ids]
     e.close()
     for (p0, v0), (p1, v1) in zip(bulk, each):
-        assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+        if precision == "mixed":
+            assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+        else:
+            assert np.abs(p0 - p1).max() <= 1e-9 * max(1.0, np.abs(p1).max())
+            assert np.abs(v0 - v1).max() <= 1e-7 * max(1.0, np.abs(v1).max())
